@@ -1,0 +1,282 @@
+/*
+ * pned_gpu.h -- C ABI of the B200 (sm_100a) implementation of pNED's
+ * matrix-free H.v and the Krylov loops built on it.
+ *
+ * The entry points replace the single-rank (lnp = 1) hot path of pNED's
+ * Fortran code.  Each declaration cites the reference routine it stands in
+ * for (paths relative to the pNED project root; S1/2 = S_one_half/Hybrid_TPS_*,
+ * Sa = S_arbitrary/Hybrid_TPS9_*).
+ *
+ * Conventions kept from the reference:
+ *   - complex numbers are two doubles (re, im), layout-compatible with
+ *     Fortran complex(KIND(0d0)) and C double _Complex;
+ *   - local matrices xlocal are [9][Q][Q] column-major per bond type,
+ *     Q = q_spin^2: element (row = target pair state, col = current pair
+ *     state, type t) at row + Q*col + Q*Q*(t-1), exactly the memory of the
+ *     Fortran array xlocal_Ham(0:Q-1,0:Q-1,9);
+ *   - the pair state of a bond (s1 < s2) is d(s2)*q + d(s1); digit (bit) j
+ *     of the basis index is site j+1;
+ *   - H.v accumulates v0 += X(target, current) v1(partner), i.e. H^T
+ *     (S1/2 parallel.f90:358), and prdct = <v1|H v1>.
+ *   - batched vectors are interleaved: element (state s, vector r) at s*R + r.
+ *
+ * Every function returns PNED_OK (0) or an error code; the message of the
+ * last error of the calling thread is returned by pned_last_error().  No call
+ * exits or stops the process.  Pointer arguments marked "host or device"
+ * are interpreted according to the PNED_PTR_DEVICE flag of the call.
+ */
+#ifndef PNED_GPU_H
+#define PNED_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PNED_ABI_VERSION 1
+
+/* status codes */
+#define PNED_OK 0
+#define PNED_EINVAL 1      /* invalid argument or model                         */
+#define PNED_ENOMEM 2      /* device allocation failed                          */
+#define PNED_EBUDGET 3     /* request exceeds the HBM budget of the context     */
+#define PNED_EBREAKDOWN 4  /* Lanczos beta below 0.5e-30 (S1/2 Lanczos.f90:126) */
+#define PNED_ECUDA 5       /* CUDA runtime error                                */
+#define PNED_ETIMEOUT 6    /* a bounded wait gave up                            */
+#define PNED_ENOTSUP 7     /* combination not supported by this build           */
+
+/* pointer-location flags */
+#define PNED_PTR_HOST 0
+#define PNED_PTR_DEVICE 1
+
+typedef struct { double re, im; } pned_c128;
+
+typedef struct pned_model pned_model;
+typedef struct pned_ctx pned_ctx;
+
+/* ------------------------------------------------------------------------ */
+/* library                                                                   */
+/* ------------------------------------------------------------------------ */
+int pned_abi_version(void);
+const char *pned_last_error(void);
+/* CUDA device used by models/contexts created afterwards on this thread. */
+int pned_set_device(int device);
+
+/* ------------------------------------------------------------------------ */
+/* host-side model input (replaces set_xlocal_Ham / change_to_TPS_hamiltonian) */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Local two-site matrices from the 19 coupling slots of the reference
+ * (order: J1 K1 I11 I12 J1p K1p J1pp K1pp I11p I12p I11pp I12pp J2 K2 I21 I22
+ * J3 K3 ratio_l), for tree 0 (S1/2 params.f90:1388-1563, q must be 2) or
+ * tree 1 (Sa params.f90:1412-1602, any q).  field (may be NULL) adds the
+ * Zeeman term -h.S_i split over the `coord` nearest-neighbour bonds of each
+ * site (an extension: the reference has no field).  Also writes the skip mask
+ * llocal_Ham (1 = skipped) and parity_type (S1/2 params.f90:1565-1595,
+ * Sa params.f90:1604-1655).
+ */
+int pned_build_xlocal(int q_spin, int tree, const double *couplings19, int simple, const double *field3,
+                      double coord, pned_c128 *xlocal_out, uint8_t *skip_out, int *parity_type_out);
+
+/*
+ * TPS Hamiltonian.  mode 0 reproduces change_to_TPS_hamiltonian
+ * (S1/2 params.f90:1600-1623, Sa params.f90:1660-1686) and returns its L in
+ * *L_inout; mode 1 uses the L given in *L_inout: X <- (L/n_bonds) 1 - X.
+ */
+int pned_tps_transform(int q_spin, int tree, int n_bonds, double c_count, int mode, pned_c128 *xlocal_inout,
+                       double *L_inout);
+
+/* Sz-sector basis list and Lin tables (S1/2 parallel.f90:452-578, Sa :366-486).
+   With list1 == NULL only the dimension is returned in *ldim. */
+int pned_mk_list12(int n_sites, int q_spin, int parity_type, int total_sz, int64_t *ldim, int64_t *list1,
+                   int64_t *list3_lo, int64_t *list3_hi);
+
+/* ------------------------------------------------------------------------ */
+/* model                                                                     */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int32_t n_sites;          /* n                                                 */
+    int32_t q_spin;           /* 2S+1                                              */
+    int32_t tree;             /* 0: S1/2 schedule order, 1: Sa schedule order      */
+    int32_t n_bonds;          /* ibond                                             */
+    const int32_t *ipair;     /* [2*n_bonds] 1-based sites (ipair)                 */
+    const int32_t *bond_type; /* [n_bonds] 1..9 (ibond_type)                       */
+    const pned_c128 *xlocal;  /* [9][Q][Q] (xlocal_Ham)                            */
+    const uint8_t *skip;      /* [9][Q][Q] llocal_Ham, 1 = skipped; NULL = none    */
+    int32_t parity_type;      /* 0 = Sz-conserving sector basis, else full basis   */
+    int32_t total_sz;         /* digit sum of the sector when parity_type == 0     */
+} pned_model_desc;
+
+/*
+ * Compiles the bond table into the device term program (flip masks or
+ * mixed-radix offsets with coefficient tables) and uploads it to the current
+ * device.  Replaces set_parallel_bits + make_cpu_list2 + mk_list12
+ * (S1/2 MPIlib.f90:74-84, 104-341; parallel.f90:452-578) for one GPU.
+ * This build runs the full basis (parity_type != 0); parity_type == 0
+ * returns PNED_ENOTSUP.
+ */
+int pned_model_create(const pned_model_desc *desc, pned_model **out);
+int pned_model_destroy(pned_model *m);
+/* dim = q^n; n_terms = off-diagonal gather terms per state in the program. */
+int pned_model_info(const pned_model *m, int64_t *dim, int *n_terms, int *real_coefficients);
+
+/* ------------------------------------------------------------------------ */
+/* context: device vectors for R interleaved vectors                         */
+/* ------------------------------------------------------------------------ */
+/* hbm_budget = 0: no budget check beyond the device's free memory. */
+int pned_ctx_create(pned_model *m, int R, size_t hbm_budget, pned_ctx **out);
+int pned_ctx_destroy(pned_ctx *c);
+/* cudaStream_t used by the context (NULL = the context's own stream). */
+int pned_ctx_set_stream(pned_ctx *c, void *stream);
+int pned_ctx_synchronize(pned_ctx *c);
+/* Device pointer of the context's interleaved vector buffer k (0..3). */
+int pned_ctx_buffer(pned_ctx *c, int k, pned_c128 **dev_ptr);
+/* Bytes of device memory the context holds. */
+int pned_ctx_bytes(const pned_ctx *c, size_t *bytes);
+
+/* ------------------------------------------------------------------------ */
+/* vector kernels                                                            */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * p_mltply_v3 (S1/2 parallel.f90:190-263, Sa parallel.f90:184-261):
+ * v0 += (H - eperbd*n_bonds)^T v1 for each of the R interleaved vectors, and
+ * prdct[r] = <v1_r|(H - eperbd*n_bonds)^T v1_r>.  v1, v0 host or device
+ * ([dim][R]); prdct host, may be NULL.
+ */
+int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double eperbd, pned_c128 *prdct, int ptr_flags);
+
+/* calc_vec_inprdct (S1/2 parallel.f90:104-126): out[r] = sum conj(x1_r) x2_r. */
+int pned_inprdct(pned_ctx *c, const pned_c128 *x1, const pned_c128 *x2, pned_c128 *out, int ptr_flags);
+
+/* calc_beta (S1/2 parallel.f90:161-188): out[r] = sum |v0_r - alpha_r v1_r|^2. */
+int pned_calc_beta(pned_ctx *c, const pned_c128 *alpha, const pned_c128 *v1, const pned_c128 *v0, double *out,
+                   int ptr_flags);
+
+/*
+ * Seeded complex-Gaussian vectors (replaces the compiler-RNG initial vector of
+ * parallelized_set_initial_vec_p, S1/2 parallel.f90:17-102): element g =
+ * s*R + r is sqrt(-ln u1) e^{2 pi i u2} from splitmix64 counters; each vector
+ * is then normalised when normalise != 0.  v_dev is a device pointer.
+ */
+int pned_fill_gaussian(pned_ctx *c, uint64_t seed, int normalise, pned_c128 *v_dev);
+
+/* ------------------------------------------------------------------------ */
+/* Krylov drivers                                                            */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Lanczos (parallelized_lnc1z, S1/2 Lanczos.f90:48-163) on R independent
+ * chains: n_steps values alpha[i*R + r], beta[i*R + r] (i = 0 .. n_steps-1,
+ * the reference's alpha(i+1), beta(i+1)).  v_init ([dim][R], host or
+ * device) must be normalised.  check_conv != 0 applies the nvec = 8
+ * convergence stop of :133-155 (R = 1 only); *steps_done returns the number of
+ * steps.  ene (may be NULL) receives the 8 lowest Ritz values of chain 0
+ * (bisec, S1/2 basic.f90:25-107).
+ */
+int pned_lanczos_run(pned_ctx *c, const pned_c128 *v_init, int n_steps, int check_conv, double *alpha, double *beta,
+                     double *ene, int *steps_done, int ptr_flags);
+
+/*
+ * Diagonal two-bit observable for the TPS step (S1/2 TPS.f90:128-321):
+ * O(s) = sum_t c_t T[bit(s,a_t)][bit(s,b_t)], bit(s,p) = 0 for p >= n.
+ */
+typedef struct {
+    int32_t n_terms;
+    const int32_t *a;   /* [n_terms] bit positions */
+    const int32_t *b;   /* [n_terms] bit positions */
+    const pned_c128 *c; /* [n_terms] weights        */
+    pned_c128 T[4];     /* T[2*i + k]               */
+} pned_observable;
+
+/*
+ * mTPQ / TPS (parallelized_TPSz, S1/2 TPS.f90:325-409) on R interleaved seeds
+ * with a model already transformed to L - H (pned_tps_transform).  Per step i
+ * and seed r: alpha[i*R+r] = L - <k|(L-H)|k>, beta[i*R+r] = ||(L-H)|k>||,
+ * coef[(i*R + r)*ncoef + j] with j = 0..4 as coef(i,1..5) of eval_phys_val
+ * (:83-111) and 2 entries per observable.  ncoef = 5 + 2*n_obs.
+ */
+int pned_tps_run(pned_ctx *c, double L, const pned_c128 *v_init, int n_steps, int n_obs, const pned_observable *obs,
+                 double *alpha, double *beta, double *coef, int ptr_flags);
+
+/*
+ * Dynamical structure factor chains (intalv_zz + parallelized_dsflnc1z,
+ * S1/2 DSF.f90:18-87, 195-261; Sa DSF.f90:18-89): for r = 0..R-1 the start
+ * vector is S^z_q x with phases qr[r*n + j] = q_r.r_j, normalised; cnorm[r] =
+ * ||S^z_q x||^2 / n (sbeta(1)).  salpha[i*R + r] (i < n_steps) and
+ * sbeta[i*R + r] (i <= n_steps, sbeta[0] = cnorm) as the reference's
+ * salpha(i+1), sbeta(i+1).  x is one vector [dim] (host or device).
+ */
+int pned_dsf_run(pned_ctx *c, const pned_c128 *x, const double *qr, int n_steps, double *cnorm, double *salpha,
+                 double *sbeta, int ptr_flags);
+
+/*
+ * Inverse iteration with CG (parallelized_inv1z + parallelized_cg1,
+ * S1/2 cg.f90:18-196) for chain 0: b_init (normalised, [dim]) and E;
+ * x_out receives the normalised eigenvector ([dim], host or device).
+ */
+int pned_cg_run(pned_ctx *c, double E, const pned_c128 *b_init, int inv_max, int cg_max, pned_c128 *x_out,
+                int *n_inv, int *n_cg, int ptr_flags);
+
+/* ------------------------------------------------------------------------ */
+/* Krylov sessions: the same loops, advanced step by step on the device      */
+/* ------------------------------------------------------------------------ */
+/*
+ * A session keeps the Krylov vectors of R chains resident in the context and
+ * advances them in place, so a caller (a serving loop, a benchmark) can run
+ * steps incrementally without host round trips.  pned_lanczos_run,
+ * pned_tps_run and pned_dsf_run are begin + step + read + end.
+ *
+ * kind PNED_SESSION_LANCZOS: parallelized_lnc1z steps (S1/2 Lanczos.f90:97-157)
+ *      from v_init; PNED_SESSION_TPS: parallelized_TPSz steps (S1/2
+ *      TPS.f90:368-404) with total shift L (model already L - H) and optional
+ *      observables; PNED_SESSION_DSF: parallelized_dsflnc1z chains
+ *      (S1/2 DSF.f90:195-261) started from S^z_q x (pned_session_begin_dsf).
+ */
+#define PNED_SESSION_LANCZOS 1
+#define PNED_SESSION_TPS 2
+#define PNED_SESSION_DSF 3
+
+int pned_session_begin(pned_ctx *c, int kind, const pned_c128 *v_init, int max_steps, double L, int n_obs,
+                       const pned_observable *obs, int ptr_flags);
+/* DSF chains: start vectors S^z_q x (intalv_zz, S1/2 DSF.f90:18-87); cnorm[r] = sbeta(1). */
+int pned_session_begin_dsf(pned_ctx *c, const pned_c128 *x, const double *qr, int max_steps, double *cnorm,
+                           int ptr_flags);
+/* Enqueues n_steps steps on the context's stream and returns without waiting. */
+int pned_session_step(pned_ctx *c, int n_steps);
+/*
+ * Waits for the enqueued steps and copies the per-step results of all steps so
+ * far: alpha/beta [steps][R] and, for TPS, coef [steps][R][ncoef] (any may be
+ * NULL).  status_out (may be NULL) is 1 if a Lanczos beta fell below 0.5e-30.
+ */
+int pned_session_read(pned_ctx *c, double *alpha, double *beta, double *coef, int *steps_done, int *status_out);
+/* Device pointer of the current Krylov vector C and its scale (v = scale * C). */
+int pned_session_vector(pned_ctx *c, pned_c128 **dev_ptr, double *scale_out);
+int pned_session_end(pned_ctx *c);
+/*
+ * Measurement hook (no counterpart in the reference): runs n_steps further
+ * session steps one at a time with CUDA events on the context's stream around
+ * the H.v kernel and around the whole step; returns their mean durations.
+ */
+int pned_session_profile(pned_ctx *c, int n_steps, double *hv_ms, double *step_ms);
+
+/* ------------------------------------------------------------------------ */
+/* host tridiagonal / continued-fraction routines                             */
+/* ------------------------------------------------------------------------ */
+/* bisec (S1/2 basic.f90:25-107) */
+int pned_bisec(const double *alpha, const double *beta, int ndim, double *E, int ne, double eps);
+/* vec12 (S1/2 basic.f90:112-213); v is [nvec][ndim] */
+int pned_vec12(const double *alpha, const double *beta, const double *E, int ndim, int nvec, double *v);
+/* exec_renbun (S1/2 DSF.f90:263-334): salpha/sbeta of length s_maxitr (zero padded) */
+int pned_exec_renbun(int i_range, int s_maxitr, double split, double ene, double epsln, const double *salpha,
+                     const double *sbeta, double *w, int *conv, double *dsf);
+/* nomalization_DSF (S1/2 DSF.f90:337-351) */
+int pned_normalize_dsf(int i_range, double split, double sq_re, double *dsf);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PNED_GPU_H */

@@ -1,0 +1,111 @@
+"""ctypes bindings of libpned_gpu.so (the C ABI of include/pned_gpu.h).
+
+The library is built in-tree (pned_b200/build.py).  Loading fails loudly when
+it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpned_gpu.so")
+
+PNED_OK = 0
+ERRORS = {1: "EINVAL", 2: "ENOMEM", 3: "EBUDGET", 4: "EBREAKDOWN", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP"}
+PTR_HOST = 0
+PTR_DEVICE = 1
+
+
+class c128(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [
+        ("n_sites", C.c_int32), ("q_spin", C.c_int32), ("tree", C.c_int32), ("n_bonds", C.c_int32),
+        ("ipair", C.POINTER(C.c_int32)), ("bond_type", C.POINTER(C.c_int32)),
+        ("xlocal", C.c_void_p), ("skip", C.POINTER(C.c_uint8)),
+        ("parity_type", C.c_int32), ("total_sz", C.c_int32),
+    ]
+
+
+class Observable(C.Structure):
+    _fields_ = [
+        ("n_terms", C.c_int32), ("a", C.POINTER(C.c_int32)), ("b", C.POINTER(C.c_int32)),
+        ("c", C.c_void_p), ("T", c128 * 4),
+    ]
+
+
+class PnedError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pned error {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+EXPORTS = [
+    "pned_abi_version", "pned_last_error", "pned_set_device", "pned_build_xlocal", "pned_tps_transform",
+    "pned_mk_list12", "pned_model_create", "pned_model_destroy", "pned_model_info", "pned_ctx_create",
+    "pned_ctx_destroy", "pned_ctx_set_stream", "pned_ctx_synchronize", "pned_ctx_buffer", "pned_ctx_bytes",
+    "pned_hv", "pned_inprdct", "pned_calc_beta", "pned_fill_gaussian", "pned_lanczos_run", "pned_tps_run",
+    "pned_dsf_run", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
+    "pned_session_begin", "pned_session_begin_dsf", "pned_session_step", "pned_session_read", "pned_session_vector",
+    "pned_session_end", "pned_session_profile",
+]
+SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
+
+
+def lib() -> C.CDLL:
+    """The loaded product library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m pned_b200.build` "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int, C.c_int64, C.c_double
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    L.pned_abi_version.restype = i32
+    L.pned_last_error.restype = C.c_char_p
+    L.pned_set_device.argtypes = [i32]
+    L.pned_build_xlocal.argtypes = [i32, i32, dp, i32, dp, dbl, vp, C.POINTER(C.c_uint8), ip]
+    L.pned_tps_transform.argtypes = [i32, i32, i32, dbl, i32, vp, dp]
+    L.pned_mk_list12.argtypes = [i32, i32, i32, i32, C.POINTER(i64), vp, vp, vp]
+    L.pned_model_create.argtypes = [C.POINTER(ModelDesc), C.POINTER(vp)]
+    L.pned_model_destroy.argtypes = [vp]
+    L.pned_model_info.argtypes = [vp, C.POINTER(i64), ip, ip]
+    L.pned_ctx_create.argtypes = [vp, i32, C.c_size_t, C.POINTER(vp)]
+    L.pned_ctx_destroy.argtypes = [vp]
+    L.pned_ctx_set_stream.argtypes = [vp, vp]
+    L.pned_ctx_synchronize.argtypes = [vp]
+    L.pned_ctx_buffer.argtypes = [vp, i32, C.POINTER(vp)]
+    L.pned_ctx_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
+    L.pned_hv.argtypes = [vp, vp, vp, dbl, vp, i32]
+    L.pned_inprdct.argtypes = [vp, vp, vp, vp, i32]
+    L.pned_calc_beta.argtypes = [vp, vp, vp, vp, dp, i32]
+    L.pned_fill_gaussian.argtypes = [vp, C.c_uint64, i32, vp]
+    L.pned_lanczos_run.argtypes = [vp, vp, i32, i32, dp, dp, dp, ip, i32]
+    L.pned_tps_run.argtypes = [vp, dbl, vp, i32, i32, C.POINTER(Observable), dp, dp, dp, i32]
+    L.pned_dsf_run.argtypes = [vp, vp, dp, i32, dp, dp, dp, i32]
+    L.pned_cg_run.argtypes = [vp, dbl, vp, i32, i32, vp, ip, ip, i32]
+    L.pned_bisec.argtypes = [dp, dp, i32, dp, i32, dbl]
+    L.pned_vec12.argtypes = [dp, dp, dp, i32, i32, dp]
+    L.pned_exec_renbun.argtypes = [i32, i32, dbl, dbl, dbl, dp, dp, dp, ip, dp]
+    L.pned_normalize_dsf.argtypes = [i32, dbl, dbl, dp]
+    L.pned_session_begin.argtypes = [vp, i32, vp, i32, dbl, i32, C.POINTER(Observable), i32]
+    L.pned_session_begin_dsf.argtypes = [vp, vp, dp, i32, dp, i32]
+    L.pned_session_step.argtypes = [vp, i32]
+    L.pned_session_read.argtypes = [vp, dp, dp, dp, ip, ip]
+    L.pned_session_vector.argtypes = [vp, C.POINTER(vp), dp]
+    L.pned_session_end.argtypes = [vp]
+    L.pned_session_profile.argtypes = [vp, i32, dp, dp]
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc != PNED_OK:
+        raise PnedError(rc, lib().pned_last_error().decode(errors="replace"))

@@ -1,0 +1,397 @@
+"""Host-side API over the C ABI, named after the reference routines it replaces.
+
+Vectors are complex128 with R interleaved columns ([dim][R] flattened).  Every
+vector argument may be a numpy array (host memory: copied to and from the
+device by the call) or a CUDA torch tensor (device memory: used in place).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi
+from ._capi import PTR_DEVICE, PTR_HOST, check, lib
+from .couplings import NSLOT
+
+try:  # torch is only plumbing here: device memory for callers that keep vectors on the GPU
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _is_dev(x) -> bool:
+    return torch is not None and isinstance(x, torch.Tensor) and x.is_cuda
+
+
+def _ptr(x, writable=False):
+    """(pointer, flag) for a numpy array or a CUDA tensor of complex128."""
+    if _is_dev(x):
+        if x.dtype != torch.complex128 or not x.is_contiguous():
+            raise TypeError("device vectors must be contiguous complex128 CUDA tensors")
+        return C.c_void_p(x.data_ptr()), PTR_DEVICE
+    if not isinstance(x, np.ndarray) or x.dtype != np.complex128 or not x.flags["C_CONTIGUOUS"]:
+        raise TypeError("host vectors must be C-contiguous complex128 numpy arrays")
+    if writable and not x.flags["WRITEABLE"]:
+        raise TypeError("output vector is read-only")
+    return C.c_void_p(x.ctypes.data), PTR_HOST
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _same_flag(*flags):
+    if len(set(flags)) != 1:
+        raise TypeError("mix of host and device vectors in one call")
+    return flags[0]
+
+
+# --------------------------------------------------------------------------- model input
+
+def build_xlocal(q: int, tree: int, couplings, simple: int = 0, field=None, coord: float = 3.0):
+    """set_xlocal_Ham: returns (xlocal (9,Q,Q) [type, col, row], skip (9,Q,Q) uint8, parity_type)."""
+    Q = q * q
+    cpl = np.ascontiguousarray(couplings, dtype=np.float64)
+    if cpl.shape != (NSLOT,):
+        raise ValueError(f"couplings must have {NSLOT} slots")
+    X = np.zeros((9, Q, Q), dtype=np.complex128)
+    skip = np.zeros((9, Q, Q), dtype=np.uint8)
+    pt = C.c_int(0)
+    fld = None if field is None else np.ascontiguousarray(field, dtype=np.float64)
+    check(lib().pned_build_xlocal(q, tree, _dp(cpl), simple, None if fld is None else _dp(fld), coord,
+                                  C.c_void_p(X.ctypes.data), skip.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                  C.byref(pt)))
+    return X, skip, pt.value
+
+
+def tps_transform(q: int, tree: int, n_bonds: int, xlocal, L=None, c_count: float = 3.0):
+    """change_to_TPS_hamiltonian (L=None: the reference's own L) or X <- (L/n_bonds) 1 - X."""
+    X = np.ascontiguousarray(xlocal, dtype=np.complex128).copy()
+    Lc = C.c_double(0.0 if L is None else float(L))
+    check(lib().pned_tps_transform(q, tree, n_bonds, c_count, 0 if L is None else 1, C.c_void_p(X.ctypes.data),
+                                   C.byref(Lc)))
+    return X, Lc.value
+
+
+def mk_list12(n: int, q: int, parity_type: int, total_sz: int):
+    ldim = C.c_int64(0)
+    check(lib().pned_mk_list12(n, q, parity_type, total_sz, C.byref(ldim), None, None, None))
+    nA = q ** ((n + 1) // 2)
+    nB = q ** (n // 2)
+    list1 = np.zeros(ldim.value, dtype=np.int64)
+    lo = np.zeros(max(nA, nB), dtype=np.int64)
+    hi = np.zeros(max(nA, nB), dtype=np.int64)
+    check(lib().pned_mk_list12(n, q, parity_type, total_sz, C.byref(ldim), C.c_void_p(list1.ctypes.data),
+                               C.c_void_p(lo.ctypes.data), C.c_void_p(hi.ctypes.data)))
+    return list1, lo, hi
+
+
+def bisec(alpha, beta, ndim: int, ne: int, eps: float = 1e-25):
+    a = np.ascontiguousarray(alpha, dtype=np.float64)
+    b = np.ascontiguousarray(beta, dtype=np.float64)
+    E = np.zeros(max(1, ne))
+    check(lib().pned_bisec(_dp(a), _dp(b), ndim, _dp(E), ne, eps))
+    return E[:ne]
+
+
+def vec12(alpha, beta, E, ndim: int, nvec: int):
+    a = np.ascontiguousarray(alpha, dtype=np.float64)
+    b = np.ascontiguousarray(np.concatenate([np.asarray(beta, dtype=np.float64), np.zeros(2)]))
+    e = np.ascontiguousarray(E, dtype=np.float64)
+    v = np.zeros((nvec, ndim))
+    check(lib().pned_vec12(_dp(a), _dp(b), _dp(e), ndim, nvec, _dp(v)))
+    return v
+
+
+def exec_renbun(i_range: int, s_maxitr: int, split: float, ene: float, epsln: float, salpha, sbeta):
+    sa = np.zeros(s_maxitr)
+    sb = np.zeros(s_maxitr)
+    na, nb = min(len(salpha), s_maxitr), min(len(sbeta), s_maxitr)
+    sa[:na] = np.asarray(salpha)[:na]
+    sb[:nb] = np.asarray(sbeta)[:nb]
+    w = np.zeros(i_range)
+    conv = np.zeros(i_range, dtype=np.int32)
+    dsf = np.zeros(i_range)
+    check(lib().pned_exec_renbun(i_range, s_maxitr, split, ene, epsln, _dp(sa), _dp(sb), _dp(w),
+                                 conv.ctypes.data_as(C.POINTER(C.c_int)), _dp(dsf)))
+    return w, conv, dsf
+
+
+def normalize_dsf(i_range: int, split: float, sq_re: float, dsf):
+    d = np.ascontiguousarray(dsf, dtype=np.float64).copy()
+    check(lib().pned_normalize_dsf(i_range, split, sq_re, _dp(d)))
+    return d
+
+
+# --------------------------------------------------------------------------- model / context
+
+class Model:
+    """A compiled model on the current device (pned_model_create)."""
+
+    def __init__(self, n, q, tree, ipair, bond_type, xlocal, skip, parity_type, total_sz=None):
+        if total_sz is None:
+            total_sz = n // 2 * (q - 1)
+        self.n, self.q, self.tree = int(n), int(q), int(tree)
+        self._ipair = np.ascontiguousarray(ipair, dtype=np.int32)
+        self._bt = np.ascontiguousarray(bond_type, dtype=np.int32)
+        self._x = np.ascontiguousarray(xlocal, dtype=np.complex128)
+        self._skip = None if skip is None else np.ascontiguousarray(skip, dtype=np.uint8)
+        self.n_bonds = int(self._bt.shape[0])
+        d = _capi.ModelDesc()
+        d.n_sites, d.q_spin, d.tree, d.n_bonds = self.n, self.q, self.tree, self.n_bonds
+        d.ipair = self._ipair.ctypes.data_as(C.POINTER(C.c_int32))
+        d.bond_type = self._bt.ctypes.data_as(C.POINTER(C.c_int32))
+        d.xlocal = C.c_void_p(self._x.ctypes.data)
+        d.skip = None if self._skip is None else self._skip.ctypes.data_as(C.POINTER(C.c_uint8))
+        d.parity_type, d.total_sz = int(parity_type), int(total_sz)
+        h = C.c_void_p()
+        check(lib().pned_model_create(C.byref(d), C.byref(h)))
+        self._h = h
+        dim, nt, rc_ = C.c_int64(0), C.c_int(0), C.c_int(0)
+        check(lib().pned_model_info(h, C.byref(dim), C.byref(nt), C.byref(rc_)))
+        self.dim, self.n_terms, self.real = dim.value, nt.value, bool(rc_.value)
+
+    @classmethod
+    def from_couplings(cls, cluster, couplings, q=2, tree=0, field=None, tps_L=None, simple=0):
+        """Model from a cluster table and coupling slots (+ field, + TPS shift L)."""
+        X, skip, pt = build_xlocal(q, tree, couplings, simple=simple, field=field)
+        if tps_L is not None:
+            X, _ = tps_transform(q, tree, cluster.nbond, X, L=tps_L)
+        return cls(cluster.n, q, tree, cluster.ipair, cluster.ibond_type, X, skip, pt)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pned_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ObservableSpec:
+    """O(s) = sum_t c_t T[bit(s, a_t)][bit(s, b_t)] (see pned_observable)."""
+    a: np.ndarray
+    b: np.ndarray
+    c: np.ndarray
+    T: np.ndarray
+
+
+class Context:
+    """Device vectors and scratch for R interleaved vectors of one model."""
+
+    def __init__(self, model: Model, R: int = 1, hbm_budget: int = 0, stream=None):
+        self.model = model
+        self.R = int(R)
+        h = C.c_void_p()
+        check(lib().pned_ctx_create(model._h, self.R, C.c_size_t(int(hbm_budget)), C.byref(h)))
+        self._h = h
+        if stream is not None:
+            self.set_stream(stream)
+
+    @property
+    def n_elem(self):
+        return self.model.dim * self.R
+
+    def set_stream(self, stream):
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        check(lib().pned_ctx_set_stream(self._h, C.c_void_p(sp)))
+
+    def synchronize(self):
+        check(lib().pned_ctx_synchronize(self._h))
+
+    def bytes(self) -> int:
+        b = C.c_size_t(0)
+        check(lib().pned_ctx_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pned_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check_len(self, *vs):
+        for v in vs:
+            n = v.numel() if _is_dev(v) else v.size
+            if n != self.n_elem:
+                raise ValueError(f"vector has {n} elements, expected dim*R = {self.n_elem}")
+
+    # ----- p_mltply_v3 / calc_vec_inprdct / calc_beta
+    def p_mltply_v3(self, v1, v0, eperbd: float = 0.0):
+        """v0 += (H - eperbd*ibond)^T v1 (in place); returns prdct (R complex)."""
+        self._check_len(v1, v0)
+        p1, f1 = _ptr(v1)
+        p0, f0 = _ptr(v0, writable=True)
+        pr = np.zeros(self.R, dtype=np.complex128)
+        check(lib().pned_hv(self._h, p1, p0, float(eperbd), C.c_void_p(pr.ctypes.data), _same_flag(f1, f0)))
+        return pr
+
+    def calc_vec_inprdct(self, x1, x2):
+        self._check_len(x1, x2)
+        p1, f1 = _ptr(x1)
+        p2, f2 = _ptr(x2)
+        out = np.zeros(self.R, dtype=np.complex128)
+        check(lib().pned_inprdct(self._h, p1, p2, C.c_void_p(out.ctypes.data), _same_flag(f1, f2)))
+        return out
+
+    def calc_beta(self, alpha, v1, v0):
+        self._check_len(v1, v0)
+        al = np.ascontiguousarray(np.broadcast_to(np.asarray(alpha, dtype=np.complex128), (self.R,)))
+        p1, f1 = _ptr(v1)
+        p0, f0 = _ptr(v0)
+        out = np.zeros(self.R)
+        check(lib().pned_calc_beta(self._h, C.c_void_p(al.ctypes.data), p1, p0, _dp(out), _same_flag(f1, f0)))
+        return out
+
+    def fill_gaussian(self, seed: int, out, normalise: bool = True):
+        """Seeded complex-Gaussian vectors into a CUDA tensor (dim*R complex128)."""
+        self._check_len(out)
+        p, f = _ptr(out, writable=True)
+        if f != PTR_DEVICE:
+            raise TypeError("fill_gaussian writes device memory (a CUDA tensor)")
+        check(lib().pned_fill_gaussian(self._h, C.c_uint64(seed), int(normalise), p))
+        return out
+
+    # ----- Krylov drivers
+    def lanczos(self, v_init, n_steps: int, check_conv: bool = False):
+        """parallelized_lnc1z on R chains: alpha/beta [steps][R], Ritz values of chain 0."""
+        self._check_len(v_init)
+        p, f = _ptr(v_init)
+        a = np.zeros(n_steps * self.R)
+        b = np.zeros(n_steps * self.R)
+        ene = np.zeros(8)
+        done = C.c_int(0)
+        rc = lib().pned_lanczos_run(self._h, p, n_steps, int(check_conv), _dp(a), _dp(b), _dp(ene),
+                                    C.byref(done), f)
+        check(rc)
+        k = done.value
+        return dict(alpha=a[:k * self.R].reshape(k, self.R), beta=b[:k * self.R].reshape(k, self.R), ene=ene, itr=k)
+
+    @staticmethod
+    def _obs_array(observables):
+        nobs = len(observables)
+        keep = []
+        arr = (_capi.Observable * max(1, nobs))()
+        for o, spec in enumerate(observables):
+            a_ = np.ascontiguousarray(spec.a, dtype=np.int32)
+            b_ = np.ascontiguousarray(spec.b, dtype=np.int32)
+            c_ = np.ascontiguousarray(spec.c, dtype=np.complex128)
+            keep += [a_, b_, c_]
+            arr[o].n_terms = a_.shape[0]
+            arr[o].a = a_.ctypes.data_as(C.POINTER(C.c_int32))
+            arr[o].b = b_.ctypes.data_as(C.POINTER(C.c_int32))
+            arr[o].c = C.c_void_p(c_.ctypes.data)
+            T = np.asarray(spec.T, dtype=np.complex128).reshape(4)
+            for i in range(4):
+                arr[o].T[i] = _capi.c128(T[i].real, T[i].imag)
+        return arr, keep
+
+    def tps(self, L: float, v_init, n_steps: int, observables=()):
+        """parallelized_TPSz on R seeds with a model built for L - H."""
+        self._check_len(v_init)
+        p, f = _ptr(v_init)
+        nobs = len(observables)
+        arr, keep = self._obs_array(observables)
+        ncoef = 5 + 2 * nobs
+        al = np.zeros(n_steps * self.R)
+        be = np.zeros(n_steps * self.R)
+        co = np.zeros(n_steps * self.R * ncoef)
+        check(lib().pned_tps_run(self._h, float(L), p, n_steps, nobs, arr, _dp(al), _dp(be), _dp(co), f))
+        return dict(alpha=al.reshape(n_steps, self.R), beta=be.reshape(n_steps, self.R),
+                    coef=co.reshape(n_steps, self.R, ncoef))
+
+    def dsf(self, x, qr, n_steps: int):
+        """intalv_zz + parallelized_dsflnc1z for R momenta (qr: [R][n] phases q.r_j)."""
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        if qr.shape != (self.R, self.model.n):
+            raise ValueError("qr must have shape (R, n)")
+        n_x = x.numel() if _is_dev(x) else x.size
+        if n_x != self.model.dim:
+            raise ValueError("x must have dim elements")
+        p, f = _ptr(x)
+        cn = np.zeros(self.R)
+        sa = np.zeros(n_steps * self.R)
+        sb = np.zeros((n_steps + 1) * self.R)
+        rc = lib().pned_dsf_run(self._h, p, _dp(qr), n_steps, _dp(cn), _dp(sa), _dp(sb), f)
+        check(rc)
+        return dict(cnorm=cn, salpha=sa.reshape(n_steps, self.R), sbeta=sb.reshape(n_steps + 1, self.R))
+
+    def cg(self, E: float, b_init, inv_max: int = 5000, cg_max: int = 500, x_out=None):
+        """parallelized_inv1z + cg1 (R = 1): returns (x, n_inv, n_cg)."""
+        self._check_len(b_init)
+        p, f = _ptr(b_init)
+        if x_out is None:
+            x_out = np.zeros(self.model.dim, dtype=np.complex128) if f == PTR_HOST else \
+                torch.zeros(self.model.dim, dtype=torch.complex128, device=b_init.device)
+        px, fx = _ptr(x_out, writable=True)
+        ni, nc = C.c_int(0), C.c_int(0)
+        check(lib().pned_cg_run(self._h, float(E), p, inv_max, cg_max, px, C.byref(ni), C.byref(nc),
+                                _same_flag(f, fx)))
+        return x_out, ni.value, nc.value
+
+    # ----- sessions: the Krylov vectors stay on the device between calls
+    def session_begin(self, kind: str, v_init, max_steps: int, L: float = 0.0, observables=()):
+        """Starts a 'lanczos' or 'tps' session from v_init ([dim][R])."""
+        self._check_len(v_init)
+        p, f = _ptr(v_init)
+        k = {"lanczos": _capi.SESSION_LANCZOS, "tps": _capi.SESSION_TPS}[kind]
+        arr, keep = self._obs_array(observables)
+        self._sess = dict(kind=kind, nobs=len(observables), max_steps=max_steps)
+        check(lib().pned_session_begin(self._h, k, p, int(max_steps), float(L), len(observables), arr, f))
+
+    def session_begin_dsf(self, x, qr, max_steps: int):
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        p, f = _ptr(x)
+        cn = np.zeros(self.R)
+        check(lib().pned_session_begin_dsf(self._h, p, _dp(qr), int(max_steps), _dp(cn), f))
+        self._sess = dict(kind="dsf", nobs=0, max_steps=max_steps)
+        return cn
+
+    def session_step(self, n: int):
+        """Enqueues n steps (asynchronous)."""
+        check(lib().pned_session_step(self._h, int(n)))
+
+    def session_read(self):
+        s = self._sess
+        m = s["max_steps"]
+        a = np.zeros(m * self.R)
+        b = np.zeros(m * self.R)
+        nc = 5 + 2 * s["nobs"]
+        co = np.zeros(m * self.R * nc) if s["kind"] == "tps" else None
+        k, st = C.c_int(0), C.c_int(0)
+        check(lib().pned_session_read(self._h, _dp(a), _dp(b), None if co is None else _dp(co), C.byref(k),
+                                      C.byref(st)))
+        k = k.value
+        out = dict(alpha=a[:k * self.R].reshape(k, self.R), beta=b[:k * self.R].reshape(k, self.R), steps=k,
+                   breakdown=bool(st.value))
+        if co is not None:
+            out["coef"] = co[:k * self.R * nc].reshape(k, self.R, nc)
+        return out
+
+    def session_profile(self, n: int):
+        """Mean (hv_ms, step_ms) over n further steps timed one by one with CUDA events."""
+        a, b = C.c_double(0), C.c_double(0)
+        check(lib().pned_session_profile(self._h, int(n), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def session_vector(self):
+        """(device pointer of the current Krylov vector buffer, scales[R])."""
+        p = C.c_void_p()
+        sc = np.zeros(self.R)
+        check(lib().pned_session_vector(self._h, C.byref(p), _dp(sc)))
+        return p.value, sc
+
+    def session_end(self):
+        check(lib().pned_session_end(self._h))
+        self._sess = None

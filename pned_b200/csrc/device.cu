@@ -1,0 +1,731 @@
+// Device side of libpned_gpu.so: model upload, contexts, H.v kernels,
+// deterministic reductions and the C-ABI vector entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+
+namespace pned {
+
+// ---------------------------------------------------------------------------
+// error helpers
+// ---------------------------------------------------------------------------
+int cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(PNED_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// Diagonal d(s) = sum_b X_b[st_b(s), st_b(s)] over all bonds (set-up, once).
+template <bool RD>
+__global__ void diag_kernel(int64_t dim, int n, int q, int nbond, const int *__restrict__ s1,
+                            const int *__restrict__ s2, const double2 *__restrict__ dtab, void *out)
+{
+    const int Q = q * q;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < dim; s += (int64_t)gridDim.x * blockDim.x) {
+        double2 acc = make_double2(0.0, 0.0);
+        if (q == 2) {
+            for (int b = 0; b < nbond; ++b) {
+                const int st = int((s >> s1[b]) & 1) | (int((s >> s2[b]) & 1) << 1);
+                acc = cadd(acc, dtab[b * Q + st]);
+            }
+        } else {
+            uint64_t digits = pack_digits(s, n, q);
+            for (int b = 0; b < nbond; ++b) {
+                const int st = digit_at(digits, s1[b]) + q * digit_at(digits, s2[b]);
+                acc = cadd(acc, dtab[b * Q + st]);
+            }
+        }
+        if (RD) static_cast<double *>(out)[s] = acc.x;
+        else static_cast<double2 *>(out)[s] = acc;
+    }
+}
+
+// Gathered H.v on the S = 1/2 full basis:
+//   W[s,r] = pc_r P[s,r] + sc_r * ( (d(s) - shift) C[s,r] + sum_t c_t(s) C[s ^ m_t, r] )
+// with fused per-vector sums: alpha = <v|Hv>, ||W||^2, <G|W>, <G|v> (v = sc C).
+template <int VPT, bool RC, bool RD, int K>
+__global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant__ XorProgram prog, const HvArgs a)
+{
+    extern __shared__ double2 s_tab[];
+    for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
+    __syncthreads();
+    const int R = a.R, G = R / VPT;
+    const int64_t nitems = a.dim * G;
+    double2 red[K][VPT];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) red[k][j] = make_double2(0.0, 0.0);
+    const int g = threadIdx.x % G;
+    const int r0 = g * VPT;
+    double scr[VPT], pcr[VPT], gsr[VPT];
+#pragma unroll
+    for (int j = 0; j < VPT; ++j) {
+        scr[j] = a.sc[r0 + j];
+        pcr[j] = a.pc ? a.pc[r0 + j] : 0.0;
+        gsr[j] = a.gsc ? a.gsc[r0 + j] : 0.0;
+    }
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = it / G;
+        const uint32_t su = uint32_t(s);
+        double2 v[VPT], acc[VPT];
+        const double2 *cs = a.C + s * R + r0;
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) v[j] = cs[j];
+        if (RD) {
+            const double dd = static_cast<const double *>(a.diag)[s] - a.shift;
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) acc[j] = cscale(dd, v[j]);
+        } else {
+            double2 dd = static_cast<const double2 *>(a.diag)[s];
+            dd.x -= a.shift;
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) acc[j] = cmul(dd, v[j]);
+        }
+        for (int t = 0; t < prog.nterms; ++t) {
+            const XorTerm T = prog.t[t];
+            uint32_t idx = 0;
+#pragma unroll
+            for (int k = 0; k < kMaxDeps; ++k)
+                if (k < T.nb) idx |= ((su >> ((T.pos4 >> (8 * k)) & 0xffu)) & 1u) << k;
+            const double2 c = s_tab[T.tab + idx];
+            const double2 *ps = a.C + int64_t(su ^ T.xmask) * R + r0;
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) {
+                const double2 w = __ldg(ps + j);
+                if (RC) {
+                    acc[j].x = fma(c.x, w.x, acc[j].x);
+                    acc[j].y = fma(c.x, w.y, acc[j].y);
+                } else {
+                    acc[j] = cfma(c, w, acc[j]);
+                }
+            }
+        }
+        hv_epilogue<K, VPT>(a, s, r0, v, acc, scr, pcr, gsr, red);
+    }
+    block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
+}
+
+// Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by
+// the two bond digits; zero coefficients (target digit out of range) skip the load.
+template <int VPT, bool RC, bool RD, int K>
+__global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constant__ RadixProgram prog, const HvArgs a,
+                                                            int q)
+{
+    extern __shared__ double2 s_tab[];
+    for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
+    __syncthreads();
+    const int R = a.R, G = R / VPT;
+    const int64_t nitems = a.dim * G;
+    double2 red[K][VPT];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) red[k][j] = make_double2(0.0, 0.0);
+    const int g = threadIdx.x % G;
+    const int r0 = g * VPT;
+    double scr[VPT], pcr[VPT], gsr[VPT];
+#pragma unroll
+    for (int j = 0; j < VPT; ++j) {
+        scr[j] = a.sc[r0 + j];
+        pcr[j] = a.pc ? a.pc[r0 + j] : 0.0;
+        gsr[j] = a.gsc ? a.gsc[r0 + j] : 0.0;
+    }
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = it / G;
+        double2 v[VPT], acc[VPT];
+        const double2 *cs = a.C + s * R + r0;
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) v[j] = cs[j];
+        if (RD) {
+            const double dd = static_cast<const double *>(a.diag)[s] - a.shift;
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) acc[j] = cscale(dd, v[j]);
+        } else {
+            double2 dd = static_cast<const double2 *>(a.diag)[s];
+            dd.x -= a.shift;
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) acc[j] = cmul(dd, v[j]);
+        }
+        const uint64_t digits = pack_digits(s, prog.n, q);
+        for (int t = 0; t < prog.nterms; ++t) {
+            const RadixTerm T = prog.t[t];
+            const int idx = digit_at(digits, T.s1) + q * digit_at(digits, T.s2);
+            const double2 c = s_tab[T.tab + idx];
+            if (c.x == 0.0 && c.y == 0.0) continue;
+            const double2 *ps = a.C + (s + T.offset) * R + r0;
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) {
+                const double2 w = __ldg(ps + j);
+                if (RC) {
+                    acc[j].x = fma(c.x, w.x, acc[j].x);
+                    acc[j].y = fma(c.x, w.y, acc[j].y);
+                } else {
+                    acc[j] = cfma(c, w, acc[j]);
+                }
+            }
+        }
+        hv_epilogue<K, VPT>(a, s, r0, v, acc, scr, pcr, gsr, red);
+    }
+    block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
+}
+
+// Sums partials[nb][KR] in a fixed order into out[KR] (one block).
+__global__ void finish_sum_kernel(const double2 *__restrict__ partials, int nb, int KR, double2 *out)
+{
+    __shared__ double2 sm[kThreads];
+    for (int kr = 0; kr < KR; ++kr) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s = cadd(s, partials[(size_t)b * KR + kr]);
+        sm[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sm[threadIdx.x] = cadd(sm[threadIdx.x], sm[threadIdx.x + w]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[kr] = sm[0];
+        __syncthreads();
+    }
+}
+
+// Dot products: MODE 0: sum conj(x1) x2; MODE 1 (calc_beta): sum |x2 - alpha x1|^2.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) dot_kernel(const double2 *__restrict__ x1, const double2 *__restrict__ x2,
+                                                       const double2 *__restrict__ alpha, int64_t dim, int R, int vpt,
+                                                       double2 *partials)
+{
+    double2 red[1][kMaxVPT];
+    for (int j = 0; j < kMaxVPT; ++j) red[0][j] = make_double2(0.0, 0.0);
+    const int G = R / vpt, r0 = (threadIdx.x % G) * vpt;
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * G;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t base = (it / G) * R + r0;
+#pragma unroll
+        for (int j = 0; j < kMaxVPT; ++j) {
+            if (j >= vpt) break;
+            const double2 a1 = x1[base + j], a2 = x2[base + j];
+            if (MODE == 0) {
+                red[0][j] = cadd(red[0][j], cconjmul(a1, a2));
+            } else {
+                const double2 al = alpha[r0 + j];
+                const double2 d = make_double2(a2.x - (al.x * a1.x - al.y * a1.y), a2.y - (al.x * a1.y + al.y * a1.x));
+                red[0][j].x += d.x * d.x + d.y * d.y;
+            }
+        }
+    }
+    block_reduce_store<1, kMaxVPT>(red, G, vpt, R, partials);
+}
+
+// Lanczos residual: Rn = W - Re(alpha) v, beta^2 partial = sum |W - alpha v|^2 (v = sc C).
+__global__ void __launch_bounds__(kThreads) residual_kernel(const double2 *__restrict__ W, const double2 *__restrict__ C,
+                                                            double2 *Rn, const double *__restrict__ sc,
+                                                            const double2 *__restrict__ alpha, int64_t dim, int R,
+                                                            int vpt, double2 *partials)
+{
+    double2 red[1][kMaxVPT];
+    for (int j = 0; j < kMaxVPT; ++j) red[0][j] = make_double2(0.0, 0.0);
+    const int G = R / vpt, r0 = (threadIdx.x % G) * vpt;
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * G;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t base = (it / G) * R + r0;
+#pragma unroll
+        for (int j = 0; j < kMaxVPT; ++j) {
+            if (j >= vpt) break;
+            const double2 al = alpha[r0 + j];
+            const double2 w = W[base + j];
+            const double2 v = cscale(sc[r0 + j], C[base + j]);
+            const double2 d = make_double2(w.x - (al.x * v.x - al.y * v.y), w.y - (al.x * v.y + al.y * v.x));
+            red[0][j].x += d.x * d.x + d.y * d.y;
+            Rn[base + j] = make_double2(w.x - al.x * v.x, w.y - al.x * v.y);
+        }
+    }
+    block_reduce_store<1, kMaxVPT>(red, G, vpt, R, partials);
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__global__ void __launch_bounds__(kThreads) gaussian_kernel(uint64_t key, int64_t dim, double2 *v, int R, int vpt,
+                                                            double2 *partials)
+{
+    double2 red[1][kMaxVPT];
+    for (int j = 0; j < kMaxVPT; ++j) red[0][j] = make_double2(0.0, 0.0);
+    const int G = R / vpt, r0 = (threadIdx.x % G) * vpt;
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * G;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t base = (it / G) * R + r0;
+#pragma unroll
+        for (int j = 0; j < kMaxVPT; ++j) {
+            if (j >= vpt) break;
+            const int64_t g = base + j;
+            const uint64_t h1 = splitmix64(key ^ uint64_t(2 * g));
+            const uint64_t h2 = splitmix64(key ^ uint64_t(2 * g + 1));
+            const double u1 = (double(h1 >> 11) + 0.5) * 0x1.0p-53;
+            const double u2 = double(h2 >> 11) * 0x1.0p-53;
+            const double rad = sqrt(-log(u1));
+            const double ang = 2.0 * 3.14159265358979323846 * u2;
+            const double2 z = make_double2(rad * cos(ang), rad * sin(ang));
+            v[g] = z;
+            red[0][j].x += z.x * z.x + z.y * z.y;
+        }
+    }
+    if (partials) block_reduce_store<1, kMaxVPT>(red, G, vpt, R, partials);
+}
+
+__global__ void scale_kernel(double2 *v, int64_t n, int R, const double2 *sums, int mode)
+{
+    // mode 0: v *= 1/sqrt(sums[r].x)
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+        const int r = int(g % R);
+        const double f = 1.0 / sqrt(sums[r].x);
+        v[g] = cscale(f, v[g]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+// Vectors per thread for R interleaved vectors; the R/vpt threads of a state
+// form a power-of-two group so that reductions can use xor shuffles.
+int pick_vpt(int R)
+{
+    switch (R) {
+    case 1: return 1;
+    case 2: return 2;
+    case 3: return 3;
+    case 4: return 4;
+    case 6: return 3;
+    case 8: return 4;
+    case 12: return 3;
+    case 16: return 4;
+    default: return 0;
+    }
+}
+
+template <int VPT, bool RC, bool RD, int K>
+static cudaError_t launch_hv_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    const size_t smem = sizeof(double2) * std::max(1, m->ntab);
+    if (m->q == 2) {
+        hv_xor_kernel<VPT, RC, RD, K><<<nblocks, kThreads, smem, st>>>(*m->xprog, a);
+    } else {
+        hv_radix_kernel<VPT, RC, RD, K><<<nblocks, kThreads, smem, st>>>(*m->rprog, a, m->q);
+    }
+    return cudaGetLastError();
+}
+
+template <int VPT, int K>
+static cudaError_t launch_hv_v(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    if (m->real_coef && m->real_diag) return launch_hv_t<VPT, true, true, K>(m, a, nblocks, st);
+    if (m->real_diag) return launch_hv_t<VPT, false, true, K>(m, a, nblocks, st);
+    return launch_hv_t<VPT, false, false, K>(m, a, nblocks, st);
+}
+
+template <int K>
+static cudaError_t launch_hv_k(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    switch (pick_vpt(a.R)) {
+    case 4: return launch_hv_v<4, K>(m, a, nblocks, st);
+    case 3: return launch_hv_v<3, K>(m, a, nblocks, st);
+    case 2: return launch_hv_v<2, K>(m, a, nblocks, st);
+    case 1: return launch_hv_v<1, K>(m, a, nblocks, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    switch (a.K) {
+    case 1: return launch_hv_k<1>(m, a, nblocks, st);
+    case 4: return launch_hv_k<4>(m, a, nblocks, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st)
+{
+    finish_sum_kernel<<<1, kThreads, 0, st>>>(partials, nb, KR, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dot(const pned_ctx *c, const double2 *x1, const double2 *x2, const double2 *alpha, int mode,
+                       double2 *out, cudaStream_t st)
+{
+    const int R = c->R;
+    const int vpt = pick_vpt(R);
+    if (mode == 0) dot_kernel<0><<<c->nblocks, kThreads, 0, st>>>(x1, x2, alpha, c->m->dim, R, vpt, c->partials);
+    else dot_kernel<1><<<c->nblocks, kThreads, 0, st>>>(x1, x2, alpha, c->m->dim, R, vpt, c->partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_finish(c->partials, c->nblocks, R, out, st);
+}
+
+cudaError_t launch_residual(const pned_ctx *c, const double2 *W, const double2 *C, double2 *Rn, const double *sc,
+                            const double2 *alpha, cudaStream_t st)
+{
+    residual_kernel<<<c->nblocks, kThreads, 0, st>>>(W, C, Rn, sc, alpha, c->m->dim, c->R, pick_vpt(c->R),
+                                                     c->partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gaussian(const pned_ctx *c, uint64_t seed, bool normalise, double2 *v, cudaStream_t st)
+{
+    uint64_t key = splitmix64_host(seed ^ 0x5DEECE66Dull);
+    const int64_t n = c->m->dim * c->R;
+    gaussian_kernel<<<c->nblocks, kThreads, 0, st>>>(key, c->m->dim, v, c->R, pick_vpt(c->R),
+                                                     normalise ? c->partials : nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !normalise) return e;
+    e = launch_finish(c->partials, c->nblocks, c->R, c->sums, st);
+    if (e != cudaSuccess) return e;
+    scale_kernel<<<c->nblocks, kThreads, 0, st>>>(v, n, c->R, c->sums, 0);
+    return cudaGetLastError();
+}
+
+}  // namespace pned
+
+// ---------------------------------------------------------------------------
+// C ABI: model and context
+// ---------------------------------------------------------------------------
+using namespace pned;
+
+static thread_local int g_device = 0;
+
+extern "C" int pned_set_device(int device)
+{
+    int cnt = 0;
+    cudaError_t e = cudaGetDeviceCount(&cnt);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= cnt) return fail(PNED_EINVAL, "pned_set_device: no such device");
+    g_device = device;
+    return PNED_OK;
+}
+
+extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
+{
+    if (!desc || !out) return fail(PNED_EINVAL, "pned_model_create: null argument");
+    *out = nullptr;
+    std::unique_ptr<pned_model> m(new pned_model());
+    int rc = compile_program(desc, m->hp);
+    if (rc) return rc;
+    cudaError_t e = cudaSetDevice(g_device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    m->device = g_device;
+    const HostProgram &hp = m->hp;
+    m->n = hp.n; m->q = hp.q; m->dim = hp.dim; m->nbond = hp.nbond;
+    m->real_coef = true;
+    for (const cd &z : hp.table) if (z.imag() != 0) m->real_coef = false;
+    m->real_diag = true;
+    for (const cd &z : hp.dtab) if (z.imag() != 0) m->real_diag = false;
+    m->ntab = int(hp.table.size());
+    // program by value
+    if (hp.q == 2) {
+        m->xprog.reset(new XorProgram());
+        m->xprog->nterms = int(hp.xterms.size());
+        m->xprog->ntab = m->ntab;
+        std::copy(hp.xterms.begin(), hp.xterms.end(), m->xprog->t);
+        m->nterms = m->xprog->nterms;
+    } else {
+        m->rprog.reset(new RadixProgram());
+        m->rprog->nterms = int(hp.rterms.size());
+        m->rprog->ntab = m->ntab;
+        m->rprog->n = hp.n;
+        std::copy(hp.rterms.begin(), hp.rterms.end(), m->rprog->t);
+        m->nterms = m->rprog->nterms;
+    }
+    // coefficient table
+    std::vector<double2> tab(std::max<size_t>(1, hp.table.size()));
+    for (size_t i = 0; i < hp.table.size(); ++i) tab[i] = make_double2(hp.table[i].real(), hp.table[i].imag());
+    e = cudaMalloc(&m->d_table, sizeof(double2) * tab.size());
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(table)");
+    e = cudaMemcpy(m->d_table, tab.data(), sizeof(double2) * tab.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy(table)");
+    // diagonal
+    const size_t dbytes = (m->real_diag ? sizeof(double) : sizeof(double2)) * size_t(m->dim);
+    e = cudaMalloc(&m->d_diag, dbytes);
+    if (e != cudaSuccess) return fail(PNED_ENOMEM, "pned_model_create: cannot allocate the diagonal");
+    int *ds1 = nullptr, *ds2 = nullptr;
+    double2 *dt = nullptr;
+    const int Q = hp.q * hp.q;
+    std::vector<double2> dtab(hp.dtab.size());
+    for (size_t i = 0; i < dtab.size(); ++i) dtab[i] = make_double2(hp.dtab[i].real(), hp.dtab[i].imag());
+    e = cudaMalloc(&ds1, sizeof(int) * hp.nbond);
+    if (e == cudaSuccess) e = cudaMalloc(&ds2, sizeof(int) * hp.nbond);
+    if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(double2) * dtab.size());
+    if (e == cudaSuccess) e = cudaMemcpy(ds1, hp.dsite1.data(), sizeof(int) * hp.nbond, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ds2, hp.dsite2.data(), sizeof(int) * hp.nbond, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dt, dtab.data(), sizeof(double2) * dtab.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+        if (m->real_diag) diag_kernel<true><<<nsm * 8, kThreads>>>(m->dim, hp.n, hp.q, hp.nbond, ds1, ds2, dt, m->d_diag);
+        else diag_kernel<false><<<nsm * 8, kThreads>>>(m->dim, hp.n, hp.q, hp.nbond, ds1, ds2, dt, m->d_diag);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    cudaFree(ds1); cudaFree(ds2); cudaFree(dt);
+    (void)Q;
+    if (e != cudaSuccess) return cuda_fail(e, "pned_model_create: diagonal");
+    *out = m.release();
+    return PNED_OK;
+}
+
+extern "C" int pned_model_destroy(pned_model *m)
+{
+    if (!m) return PNED_OK;
+    cudaSetDevice(m->device);
+    cudaFree(m->d_table);
+    cudaFree(m->d_diag);
+    delete m;
+    return PNED_OK;
+}
+
+extern "C" int pned_model_info(const pned_model *m, int64_t *dim, int *n_terms, int *real_coef)
+{
+    if (!m) return fail(PNED_EINVAL, "pned_model_info: null model");
+    if (dim) *dim = m->dim;
+    if (n_terms) *n_terms = m->nterms;
+    if (real_coef) *real_coef = (m->real_coef && m->real_diag) ? 1 : 0;
+    return PNED_OK;
+}
+
+namespace pned {
+
+int ctx_alloc_buffer(pned_ctx *c, int k)
+{
+    if (k < 0 || k >= kMaxBuffers) return fail(PNED_EINVAL, "context buffer index out of range");
+    if (c->buf[k]) return PNED_OK;
+    const size_t bytes = sizeof(double2) * size_t(c->m->dim) * c->R;
+    if (c->budget && c->bytes + bytes > c->budget)
+        return fail(PNED_EBUDGET, "context HBM budget exceeded by vector buffer " + std::to_string(k));
+    cudaError_t e = cudaMalloc(&c->buf[k], bytes);
+    if (e != cudaSuccess) {
+        c->buf[k] = nullptr;
+        cudaGetLastError();
+        return fail(PNED_ENOMEM, "cudaMalloc of a vector buffer failed (" + std::to_string(bytes) + " bytes)");
+    }
+    c->bytes += bytes;
+    return PNED_OK;
+}
+
+}  // namespace pned
+
+extern "C" int pned_ctx_create(pned_model *m, int R, size_t budget, pned_ctx **out)
+{
+    if (!m || !out || pick_vpt(R) == 0)
+        return fail(PNED_EINVAL, "pned_ctx_create: R must be one of 1, 2, 3, 4, 6, 8, 12, 16");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(m->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    std::unique_ptr<pned_ctx> c(new pned_ctx());
+    c->m = m;
+    c->R = R;
+    c->budget = budget;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    c->nsm = nsm;
+    // fixed grid: the reduction order (and so the result) does not depend on timing
+    const int64_t items = m->dim * (R / pick_vpt(R));
+    c->nblocks = int(std::min<int64_t>(int64_t(nsm) * 8, (items + kThreads - 1) / kThreads));
+    c->nblocks = std::max(1, c->nblocks);
+    e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    c->stream = c->own_stream;
+    const size_t pbytes = sizeof(double2) * size_t(c->nblocks) * kMaxK * kMaxR;
+    e = cudaMalloc(&c->partials, pbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->sums, sizeof(double2) * kMaxK * kMaxR * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(double) * kScalSlots * kMaxR);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_sums, sizeof(double2) * kMaxK * kMaxR * 4);
+    if (e != cudaSuccess) {
+        pned_ctx_destroy(c.release());
+        return cuda_fail(e, "pned_ctx_create: scratch");
+    }
+    c->bytes = pbytes;
+    if (c->budget && c->bytes > c->budget) {
+        pned_ctx_destroy(c.release());
+        return fail(PNED_EBUDGET, "pned_ctx_create: budget below the context's scratch size");
+    }
+    *out = c.release();
+    return PNED_OK;
+}
+
+extern "C" int pned_ctx_destroy(pned_ctx *c)
+{
+    if (!c) return PNED_OK;
+    cudaSetDevice(c->m->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    session_release(c);
+    for (int k = 0; k < kMaxBuffers; ++k) cudaFree(c->buf[k]);
+    cudaFree(c->partials);
+    cudaFree(c->sums);
+    cudaFree(c->scal);
+    cudaFree(c->flag);
+    cudaFreeHost(c->h_sums);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return PNED_OK;
+}
+
+extern "C" int pned_ctx_set_stream(pned_ctx *c, void *stream)
+{
+    if (!c) return fail(PNED_EINVAL, "pned_ctx_set_stream: null context");
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    return PNED_OK;
+}
+
+extern "C" int pned_ctx_synchronize(pned_ctx *c)
+{
+    if (!c) return fail(PNED_EINVAL, "pned_ctx_synchronize: null context");
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "cudaStreamSynchronize");
+}
+
+extern "C" int pned_ctx_buffer(pned_ctx *c, int k, pned_c128 **p)
+{
+    if (!c || !p) return fail(PNED_EINVAL, "pned_ctx_buffer: null argument");
+    int rc = ctx_alloc_buffer(c, k);
+    if (rc) return rc;
+    *p = reinterpret_cast<pned_c128 *>(c->buf[k]);
+    return PNED_OK;
+}
+
+extern "C" int pned_ctx_bytes(const pned_ctx *c, size_t *bytes)
+{
+    if (!c || !bytes) return fail(PNED_EINVAL, "pned_ctx_bytes: null argument");
+    *bytes = c->bytes + 0;
+    return PNED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: vector kernels
+// ---------------------------------------------------------------------------
+namespace pned {
+
+// Copies [dim][R] host data into buffer k (or returns the device pointer).
+int stage_in(pned_ctx *c, const pned_c128 *src, int flags, int k, const double2 **dev)
+{
+    if (!src) return fail(PNED_EINVAL, "null vector argument");
+    if (flags & PNED_PTR_DEVICE) { *dev = reinterpret_cast<const double2 *>(src); return PNED_OK; }
+    int rc = ctx_alloc_buffer(c, k);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(c->buf[k], src, sizeof(double2) * size_t(c->m->dim) * c->R,
+                                    cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync H2D");
+    *dev = c->buf[k];
+    return PNED_OK;
+}
+
+int sums_to_host(pned_ctx *c, int KR)
+{
+    cudaError_t e = cudaMemcpyAsync(c->h_sums, c->sums, sizeof(double2) * KR, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "reading reduction results");
+}
+
+// scal slot pointer
+double *slot(pned_ctx *c, int s) { return c->scal + s * kMaxR; }
+
+int set_slot(pned_ctx *c, int s, double value)
+{
+    std::vector<double> h(kMaxR, value);
+    cudaError_t e = cudaMemcpyAsync(slot(c, s), h.data(), sizeof(double) * kMaxR, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "setting device scalars");
+}
+
+}  // namespace pned
+
+extern "C" int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double eperbd, pned_c128 *prdct, int flags)
+{
+    if (!c || !v1 || !v0) return fail(PNED_EINVAL, "pned_hv: null argument");
+    cudaSetDevice(c->m->device);
+    const double2 *dv1;
+    int rc = stage_in(c, v1, flags, 0, &dv1);
+    if (rc) return rc;
+    const double2 *dv0c;
+    rc = stage_in(c, v0, flags, 1, &dv0c);
+    if (rc) return rc;
+    double2 *dv0 = const_cast<double2 *>(dv0c);
+    rc = set_slot(c, kSlotOne, 1.0);
+    if (rc) return rc;
+    HvArgs a{};
+    a.C = dv1; a.P = dv0; a.W = dv0;
+    a.sc = slot(c, kSlotOne); a.pc = slot(c, kSlotOne);
+    a.diag = c->m->d_diag; a.shift = eperbd * c->m->nbond;
+    a.table = c->m->d_table; a.partials = c->partials;
+    a.dim = c->m->dim; a.R = c->R; a.K = 1;
+    cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
+    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, c->R, c->sums, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_hv launch");
+    if (!(flags & PNED_PTR_DEVICE)) {
+        e = cudaMemcpyAsync(v0, dv0, sizeof(double2) * size_t(c->m->dim) * c->R, cudaMemcpyDeviceToHost, c->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "pned_hv D2H");
+    }
+    rc = sums_to_host(c, c->R);
+    if (rc) return rc;
+    if (prdct)
+        for (int r = 0; r < c->R; ++r) prdct[r] = pned_c128{c->h_sums[r].x, c->h_sums[r].y};
+    return PNED_OK;
+}
+
+extern "C" int pned_inprdct(pned_ctx *c, const pned_c128 *x1, const pned_c128 *x2, pned_c128 *out, int flags)
+{
+    if (!c || !out) return fail(PNED_EINVAL, "pned_inprdct: null argument");
+    cudaSetDevice(c->m->device);
+    const double2 *a, *b;
+    int rc = stage_in(c, x1, flags, 0, &a);
+    if (!rc) rc = stage_in(c, x2, flags, 1, &b);
+    if (rc) return rc;
+    cudaError_t e = launch_dot(c, a, b, nullptr, 0, c->sums, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_inprdct");
+    rc = sums_to_host(c, c->R);
+    if (rc) return rc;
+    for (int r = 0; r < c->R; ++r) out[r] = pned_c128{c->h_sums[r].x, c->h_sums[r].y};
+    return PNED_OK;
+}
+
+extern "C" int pned_calc_beta(pned_ctx *c, const pned_c128 *alpha, const pned_c128 *v1, const pned_c128 *v0,
+                              double *out, int flags)
+{
+    if (!c || !alpha || !out) return fail(PNED_EINVAL, "pned_calc_beta: null argument");
+    cudaSetDevice(c->m->device);
+    const double2 *a, *b;
+    int rc = stage_in(c, v1, flags, 0, &a);
+    if (!rc) rc = stage_in(c, v0, flags, 1, &b);
+    if (rc) return rc;
+    double2 *dal = c->sums + kMaxK * kMaxR;   // alpha staged after the result slots
+    cudaError_t e = cudaMemcpyAsync(dal, alpha, sizeof(double2) * c->R, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_dot(c, a, b, dal, 1, c->sums, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_calc_beta");
+    rc = sums_to_host(c, c->R);
+    if (rc) return rc;
+    for (int r = 0; r < c->R; ++r) out[r] = c->h_sums[r].x;
+    return PNED_OK;
+}
+
+extern "C" int pned_fill_gaussian(pned_ctx *c, uint64_t seed, int normalise, pned_c128 *v_dev)
+{
+    if (!c || !v_dev) return fail(PNED_EINVAL, "pned_fill_gaussian: null argument");
+    cudaSetDevice(c->m->device);
+    cudaError_t e = launch_gaussian(c, seed, normalise != 0, reinterpret_cast<double2 *>(v_dev), c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_fill_gaussian");
+}

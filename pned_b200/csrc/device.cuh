@@ -1,0 +1,189 @@
+// Device-side declarations shared by device.cu and krylov.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "kernels.cuh"
+
+struct pned_model {
+    pned::HostProgram hp;
+    int device = 0;
+    int n = 0, q = 2, nbond = 0;
+    int64_t dim = 0;
+    bool real_coef = true, real_diag = true;
+    int ntab = 0, nterms = 0;
+    std::unique_ptr<pned::XorProgram> xprog;
+    std::unique_ptr<pned::RadixProgram> rprog;
+    double2 *d_table = nullptr;
+    void *d_diag = nullptr;
+};
+
+namespace pned {
+constexpr int kMaxBuffers = 6;
+// device scalar slots, kMaxR doubles each
+enum : int {
+    kSlotOne = 0,   // all ones
+    kSlotSc,        // scale of the current vector C
+    kSlotPc,        // coefficient of the previous vector P in W
+    kSlotGsc,       // scale of the vector G (TPS: previous vector)
+    kSlotTmp,
+    kScalSlots
+};
+
+struct DevObs {
+    int n = 0;
+    int *a = nullptr, *b = nullptr;
+    double2 *c = nullptr, *T = nullptr;
+};
+
+// State of a Krylov session (see pned_session_begin).
+struct Session {
+    int kind = 0;              // 0: none; PNED_SESSION_*
+    int max_steps = 0;
+    int enqueued = 0;          // steps enqueued so far
+    double L = 0.0;
+    int b0 = 2, b1 = 3, b2 = 4;  // Lanczos: C, P, W;  TPS: C, W, G
+    int nobs = 0, ncoef = 0;
+    double *d_alpha = nullptr, *d_beta = nullptr, *d_coef = nullptr;
+    int *d_counter = nullptr, *d_flag = nullptr;
+    double2 *d_osum = nullptr;
+    std::vector<DevObs> obs;
+    std::vector<void *> allocs;
+    cudaGraphExec_t graph = nullptr;
+    int g0 = -1, g1 = -1, g2 = -1;  // buffer roles when the graph was captured
+    int period = 2;
+    cudaEvent_t ev_hv0 = nullptr, ev_hv1 = nullptr;  // set while profiling: events around the H.v kernel
+};
+}  // namespace pned
+
+struct pned_ctx {
+    pned_model *m = nullptr;
+    int R = 1;
+    size_t budget = 0, bytes = 0;
+    int nsm = 148, nblocks = 1;
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+    double2 *buf[pned::kMaxBuffers] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double2 *partials = nullptr;   // [nblocks][kMaxK][kMaxR]
+    double2 *sums = nullptr;       // [4][kMaxK*kMaxR]
+    double *scal = nullptr;        // [kScalSlots][kMaxR]
+    int *flag = nullptr;
+    double2 *h_sums = nullptr;     // pinned mirror of sums
+    pned::Session sess;
+};
+
+namespace pned {
+
+int cuda_fail(cudaError_t e, const char *what);
+int ctx_alloc_buffer(pned_ctx *c, int k);
+int stage_in(pned_ctx *c, const pned_c128 *src, int flags, int k, const double2 **dev);
+int sums_to_host(pned_ctx *c, int KR);
+double *slot(pned_ctx *c, int s);
+int set_slot(pned_ctx *c, int s, double value);
+int pick_vpt(int R);
+void session_release(pned_ctx *c);
+
+cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
+cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);
+cudaError_t launch_dot(const pned_ctx *c, const double2 *x1, const double2 *x2, const double2 *alpha, int mode,
+                       double2 *out, cudaStream_t st);
+cudaError_t launch_residual(const pned_ctx *c, const double2 *W, const double2 *C, double2 *Rn, const double *sc,
+                            const double2 *alpha, cudaStream_t st);
+cudaError_t launch_gaussian(const pned_ctx *c, uint64_t seed, bool normalise, double2 *v, cudaStream_t st);
+
+inline uint64_t splitmix64_host(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// 2 bits per base-q digit (q <= 4), digit j at bits 2j..2j+1.
+__device__ __forceinline__ uint64_t pack_digits(int64_t s, int n, int q)
+{
+    uint64_t r = 0;
+    uint64_t x = uint64_t(s);
+    if (q == 3) {
+        for (int j = 0; j < n; ++j) {
+            const uint64_t y = x / 3u;
+            r |= (x - 3u * y) << (2 * j);
+            x = y;
+        }
+    } else {
+        for (int j = 0; j < n; ++j) {
+            const uint64_t y = x / uint64_t(q);
+            r |= (x - uint64_t(q) * y) << (2 * j);
+            x = y;
+        }
+    }
+    return r;
+}
+__device__ __forceinline__ int digit_at(uint64_t digits, int j) { return int((digits >> (2 * j)) & 3u); }
+
+// Block-level reduction of red[K][VPT] (vector r = g*vpt + j, g = lane % G,
+// G a power of two dividing 32) into partials[blockIdx.x][K][R].
+template <int K, int VPT>
+__device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G, int vpt, int R, double2 *partials)
+{
+    __shared__ double2 sm[kThreads / 32][kMaxK][kMaxR];
+    for (int off = 16; off >= G; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int j = 0; j < VPT; ++j) {
+                red[k][j].x += __shfl_xor_sync(0xffffffffu, red[k][j].x, off);
+                red[k][j].y += __shfl_xor_sync(0xffffffffu, red[k][j].y, off);
+            }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane < G)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int j = 0; j < VPT; ++j)
+                if (j < vpt) sm[warp][k][lane * vpt + j] = red[k][j];
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    for (int idx = threadIdx.x; idx < K * R; idx += blockDim.x) {
+        const int k = idx / R, r = idx - k * R;
+        double2 s = make_double2(0.0, 0.0);
+        for (int w = 0; w < nw; ++w) s = cadd(s, sm[w][k][r]);
+        partials[((size_t)blockIdx.x * K + k) * R + r] = s;
+    }
+}
+
+// Common epilogue of the H.v kernels: writes W and accumulates the fused sums.
+template <int K, int VPT>
+__device__ __forceinline__ void hv_epilogue(const HvArgs &a, int64_t s, int r0, const double2 (&v)[VPT],
+                                            const double2 (&acc)[VPT], const double (&scr)[VPT],
+                                            const double (&pcr)[VPT], const double (&gsr)[VPT],
+                                            double2 (&red)[K][VPT])
+{
+    const int R = a.R;
+#pragma unroll
+    for (int j = 0; j < VPT; ++j) {
+        const int64_t e = s * R + r0 + j;
+        const double2 hv = cscale(scr[j], acc[j]);
+        double2 out = hv;
+        if (a.P) {
+            const double2 p = a.P[e];
+            out.x = fma(pcr[j], p.x, out.x);
+            out.y = fma(pcr[j], p.y, out.y);
+        }
+        a.W[e] = out;
+        const double2 vv = cscale(scr[j], v[j]);
+        red[0][j] = cadd(red[0][j], cconjmul(vv, hv));
+        if (K >= 2) red[1][j].x += out.x * out.x + out.y * out.y;
+        if (K >= 4) {
+            if (a.G) {
+                const double2 gv = cscale(gsr[j], a.G[e]);
+                red[2][j] = cadd(red[2][j], cconjmul(gv, out));
+                red[3][j] = cadd(red[3][j], cconjmul(gv, vv));
+            }
+        }
+    }
+}
+
+}  // namespace pned

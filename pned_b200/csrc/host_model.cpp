@@ -1,0 +1,580 @@
+// Host-side parts of libpned_gpu.so: model input (local matrices, TPS shift,
+// Sz-sector lists), the term-program compiler, and the small tridiagonal /
+// continued-fraction routines that run on the CPU in the reference too.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+
+#include "pned_internal.h"
+
+namespace pned {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+int fail(int code, const std::string &msg)
+{
+    set_error(msg);
+    return code;
+}
+
+// ---------------------------------------------------------------------------
+// Local two-site matrices
+// ---------------------------------------------------------------------------
+namespace {
+
+// Spin-component matrices S^a (a = x, y, z) on one site, q x q, row-major.
+// tree 0: S = 1/2 with digit 0 = up (S1/2 params.f90:1434-1439);
+// tree 1: digit d <-> m = d - S, S^+/S^- from sqrt((S -+ m)(S +- m + 1)),
+//         S^y = -(i/2)(su - sd) (Sa params.f90:1479-1494).
+std::vector<cd> single_site_ops(int q, int tree)
+{
+    std::vector<cd> s(3 * q * q, cd(0, 0));
+    auto at = [&](int a, int i, int j) -> cd & { return s[(a * q + i) * q + j]; };
+    if (tree == 0) {
+        at(0, 0, 1) = 0.5; at(0, 1, 0) = 0.5;
+        at(1, 0, 1) = cd(0, -0.5); at(1, 1, 0) = cd(0, 0.5);
+        at(2, 0, 0) = 0.5; at(2, 1, 1) = -0.5;
+        return s;
+    }
+    const double S = 0.5 * (q - 1);
+    for (int i = 0; i < q; ++i) {
+        const double m = i - S;
+        cd up = (i + 1 < q) ? cd(std::sqrt((S - m) * (S + m + 1.0)), 0) : cd(0, 0);  // row i, col i+1
+        cd dn = (i > 0) ? cd(std::sqrt((S + m) * (S - m + 1.0)), 0) : cd(0, 0);      // row i, col i-1
+        if (i + 1 < q) {
+            at(0, i, i + 1) += 0.5 * up;
+            at(1, i, i + 1) += cd(0, -0.5) * up;
+        }
+        if (i > 0) {
+            at(0, i, i - 1) += 0.5 * dn;
+            at(1, i, i - 1) -= cd(0, -0.5) * dn;
+        }
+        at(2, i, i) = m;
+    }
+    return s;
+}
+
+// The seven 3x3 exchange matrices J1x, J1y, J1z, J2x, J2y, J2z, J3z built from
+// the coupling slots; ratio_l multiplies the non-Kitaev entries, with the
+// tree-1 placement of params.f90:1497-1521.
+void exchange_matrices(const double *c, int tree, cd J[7][3][3])
+{
+    enum { J1, K1, I11, I12, J1p, K1p, J1pp, K1pp, I11p, I12p, I11pp, I12pp, J2, K2, I21, I22, J3, K3, RL };
+    const double rl = c[RL];
+    const double j13 = tree ? c[J1pp] : c[J1pp] * rl, j12 = tree ? c[J1p] : c[J1p] * rl;
+    const double j11 = tree ? c[J1] : c[J1] * rl;
+    const double z[3][3] = {{j11, c[I11] * rl, c[I12] * rl}, {c[I11] * rl, j11, c[I12] * rl},
+                            {c[I12] * rl, c[I12] * rl, c[K1]}};
+    const double x[3][3] = {{c[K1p], c[I12pp] * rl, c[I12p] * rl}, {c[I12pp] * rl, j13, c[I11p] * rl},
+                            {c[I12p] * rl, c[I11p] * rl, j12}};
+    const double y[3][3] = {{j13, c[I12pp] * rl, c[I11p] * rl}, {c[I12pp] * rl, c[K1p], c[I12p] * rl},
+                            {c[I11p] * rl, c[I12p] * rl, j12}};
+    const double a2 = c[J2] * rl, k2 = c[K2] * rl, g1 = c[I21] * rl, g2 = c[I22] * rl;
+    const double x2[3][3] = {{k2, g1, g2}, {g1, a2, g2}, {g2, g2, a2}};
+    const double y2[3][3] = {{a2, g1, g2}, {g1, k2, g2}, {g2, g2, a2}};
+    const double z2[3][3] = {{a2, g1, g2}, {g1, a2, g2}, {g2, g2, k2}};
+    const double j3 = c[J3] * rl;
+    const double z3[3][3] = {{j3, 0, 0}, {0, j3, 0}, {0, 0, j3}};
+    const double (*mats[7])[3] = {x, y, z, x2, y2, z2, z3};
+    for (int t = 0; t < 7; ++t)
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) J[t][a][b] = mats[t][a][b];
+}
+
+}  // namespace
+
+}  // namespace pned
+
+using namespace pned;
+
+extern "C" int pned_build_xlocal(int q, int tree, const double *cpl, int simple, const double *field, double coord,
+                                 pned_c128 *xout, uint8_t *skip_out, int *parity_out)
+{
+    if (q < 2 || q > 8 || (tree == 0 && q != 2) || (tree != 0 && tree != 1) || !cpl || !xout)
+        return fail(PNED_EINVAL, "pned_build_xlocal: bad q_spin/tree/pointers");
+    const int Q = q * q;
+    std::vector<cd> s = single_site_ops(q, tree);
+    cd J[7][3][3];
+    exchange_matrices(cpl, tree, J);
+    // two-site operators P_ab(row = q*j1 + i1, col = q*j2 + i2) = S^a(i1,i2) S^b(j1,j2)
+    std::vector<cd> P(9 * Q * Q);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            for (int j1 = 0; j1 < q; ++j1)
+                for (int i1 = 0; i1 < q; ++i1)
+                    for (int j2 = 0; j2 < q; ++j2)
+                        for (int i2 = 0; i2 < q; ++i2)
+                            P[(3 * a + b) * Q * Q + (q * j1 + i1) * Q + (q * j2 + i2)] =
+                                s[(a * q + i1) * q + i2] * s[(b * q + j1) * q + j2];
+    std::vector<cd> X(9 * Q * Q, cd(0, 0));
+    for (int row = 0; row < Q; ++row)
+        for (int col = 0; col < Q; ++col) {
+            cd v[7];
+            for (int t = 0; t < 7; ++t) {
+                // same term order as the reference: xx xy xz yx yy yz zx zy zz
+                cd acc = J[t][0][0] * P[row * Q + col];
+                for (int ab = 1; ab < 9; ++ab) acc = acc + J[t][ab / 3][ab % 3] * P[ab * Q * Q + row * Q + col];
+                v[t] = acc;
+            }
+            cd x2x = v[3], x2y = v[4];
+            const bool keep_second = tree == 0 || simple == 3 || simple == 4;
+            if (simple == 3) { x2x = v[5]; x2y = v[5]; }
+            if (!keep_second) { x2x = 0; x2y = 0; }
+            const cd out[9] = {v[0], v[1], v[2], x2x, x2y, v[5], v[6], v[6], v[6]};
+            for (int t = 0; t < 9; ++t) X[t * Q * Q + row + Q * col] += out[t];
+        }
+    if (field) {
+        for (int t = 0; t < 3; ++t)
+            for (int j1 = 0; j1 < q; ++j1)
+                for (int i1 = 0; i1 < q; ++i1)
+                    for (int j2 = 0; j2 < q; ++j2)
+                        for (int i2 = 0; i2 < q; ++i2) {
+                            cd acc = 0;
+                            for (int a = 0; a < 3; ++a) {
+                                if (j1 == j2) acc += field[a] * s[(a * q + i1) * q + i2];
+                                if (i1 == i2) acc += field[a] * s[(a * q + j1) * q + j2];
+                            }
+                            X[t * Q * Q + (q * j1 + i1) + Q * (q * j2 + i2)] -= acc / coord;
+                        }
+    }
+    // parity type and skip mask
+    const double eps = .5e-28;
+    auto mag2 = [](cd z) { return std::fabs((std::conj(z) * z).real()); };
+    auto XA = [&](int r, int c, int t) { return X[t * Q * Q + r + Q * c]; };
+    int pt = 0;
+    std::vector<uint8_t> skip(9 * Q * Q, 1);
+    if (tree == 0) {
+        for (int t = 0; t < 9; ++t) {
+            if (mag2(XA(1, 0, t)) > eps || mag2(XA(2, 0, t)) > eps) pt |= 2;
+            if (mag2(XA(3, 0, t)) > eps) pt |= 1;
+        }
+        for (int t = 0; t < 9; ++t)
+            for (int c = 0; c < Q; ++c)
+                for (int r = 0; r < Q; ++r) {
+                    bool keep;
+                    if (pt == 0)
+                        keep = (r == c) || (r == 1 && c == 2) || (r == 2 && c == 1);
+                    else
+                        keep = (r == c) || mag2(XA(r, c, t)) > eps;
+                    skip[t * Q * Q + r + Q * c] = keep ? 0 : 1;
+                }
+    } else {
+        auto dsum = [&](int st) { return st % q + st / q; };
+        for (int t = 0; t < 9; ++t)
+            for (int j = 0; j < Q; ++j)
+                for (int i = j; i < Q; ++i)
+                    if (dsum(j) != dsum(i) && mag2(XA(i, j, t)) > eps) pt |= 1;
+        for (int t = 0; t < 9; ++t)
+            for (int j = 0; j < Q; ++j)
+                for (int i = 0; i < Q; ++i) {
+                    bool keep = (i == j) || (pt == 0 ? dsum(i) == dsum(j) : mag2(XA(i, j, t)) > eps);
+                    skip[t * Q * Q + i + Q * j] = keep ? 0 : 1;
+                }
+    }
+    for (int k = 0; k < 9 * Q * Q; ++k) xout[k] = pned_c128{X[k].real(), X[k].imag()};
+    if (skip_out) std::memcpy(skip_out, skip.data(), skip.size());
+    if (parity_out) *parity_out = pt;
+    return PNED_OK;
+}
+
+extern "C" int pned_tps_transform(int q, int tree, int nbond, double c_count, int mode, pned_c128 *x, double *L)
+{
+    if (q < 2 || !x || !L || nbond <= 0) return fail(PNED_EINVAL, "pned_tps_transform: bad arguments");
+    const int Q = q * q;
+    auto at = [&](int r, int c, int t) -> pned_c128 & { return x[t * Q * Q + r + Q * c]; };
+    double lb;
+    int ndiag = Q;
+    if (mode == 0) {
+        // reference: l_b from the diagonal entries 0..3 of all nine types
+        double acc = 0;
+        for (int t = 0; t < 9; ++t)
+            for (int i = 0; i < 4 && i < Q; ++i) {
+                const pned_c128 z = at(i, i, t);
+                const double m2 = std::fabs(z.re * z.re + z.im * z.im);
+                acc += tree == 0 ? m2 : 0.25 * double((q - 1) * (q - 1)) * std::sqrt(m2);
+            }
+        lb = tree == 0 ? acc / c_count : 2.0 * acc / c_count / double(Q);
+        ndiag = std::min(4, Q);   // the reference shifts entries 0..3 only
+        *L = lb * double(nbond);
+    } else if (mode == 1) {
+        lb = *L / double(nbond);
+    } else {
+        return fail(PNED_EINVAL, "pned_tps_transform: mode must be 0 or 1");
+    }
+    for (int k = 0; k < 9 * Q * Q; ++k) { x[k].re = -x[k].re; x[k].im = -x[k].im; }
+    for (int t = 0; t < 9; ++t)
+        for (int i = 0; i < ndiag; ++i) at(i, i, t).re = lb + at(i, i, t).re;
+    return PNED_OK;
+}
+
+extern "C" int pned_mk_list12(int n, int q, int parity_type, int total_sz, int64_t *ldim, int64_t *list1,
+                              int64_t *l3lo, int64_t *l3hi)
+{
+    if (n < 1 || q < 2 || !ldim) return fail(PNED_EINVAL, "pned_mk_list12: bad arguments");
+    const int ihf0 = n / 2, ihf = (n + 1) / 2;
+    int64_t nA = 1, nB = 1;
+    for (int i = 0; i < ihf; ++i) nA *= q;
+    for (int i = 0; i < ihf0; ++i) nB *= q;
+    std::vector<int> dsum(nA);
+    for (int64_t j = 0; j < nA; ++j) {
+        int64_t x = j;
+        int s = 0;
+        for (int i = 0; i < ihf; ++i) { s += int(x % q); x /= q; }
+        dsum[j] = s;
+    }
+    int64_t cnt = 0;
+    int64_t ja = 0, jb = 0, ibpat = 0;
+    const int64_t nmax = std::max(nA, nB);
+    if (l3lo) std::fill(l3lo, l3lo + nmax, int64_t(-1));
+    if (l3hi) std::fill(l3hi, l3hi + nmax, int64_t(-1));
+    for (int64_t i2 = 0; i2 < nB; ++i2)
+        for (int64_t i1 = 0; i1 < nA; ++i1) {
+            if (parity_type == 0 && dsum[i1] + dsum[i2] != total_sz) continue;
+            ++cnt;
+            if (!list1) continue;
+            if (i2 == ibpat) ++ja;
+            else { ibpat = i2; ja = 1; jb = cnt - 1; }
+            list1[cnt - 1] = i2 * nA + i1;
+            if (l3lo) l3lo[i1] = ja;
+            if (l3hi) l3hi[i2] = jb;
+        }
+    *ldim = cnt;
+    return PNED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Term-program compiler
+// ---------------------------------------------------------------------------
+namespace pned {
+
+namespace {
+
+struct Bond { int s1, s2, t; };
+
+// Bonds in schedule order: tree 0 keeps ipair order (sort_list of
+// S1/2 MPIlib.f90:344-392 is stable when every item is local); tree 1 reorders
+// by the larger site with the exchange sort of Sa MPIlib.f90:398-425.
+std::vector<Bond> schedule_bonds(const pned_model_desc *d)
+{
+    std::vector<Bond> b(d->n_bonds);
+    for (int i = 0; i < d->n_bonds; ++i) {
+        int a = d->ipair[2 * i] - 1, c = d->ipair[2 * i + 1] - 1;
+        b[i] = Bond{std::min(a, c), std::max(a, c), d->bond_type[i]};
+    }
+    if (d->tree == 1) {
+        std::vector<int> key(b.size()), idx(b.size());
+        for (size_t i = 0; i < b.size(); ++i) { key[i] = b[i].s2; idx[i] = int(i); }
+        for (size_t i = 0; i + 1 < b.size(); ++i)
+            for (size_t j = i + 1; j < b.size(); ++j)
+                if (key[i] > key[j]) { std::swap(key[i], key[j]); std::swap(idx[i], idx[j]); }
+        std::vector<Bond> o(b.size());
+        for (size_t i = 0; i < b.size(); ++i) o[i] = b[idx[i]];
+        b.swap(o);
+    }
+    return b;
+}
+
+}  // namespace
+
+int compile_program(const pned_model_desc *d, HostProgram &P)
+{
+    const int n = d->n_sites, q = d->q_spin, Q = q * q;
+    if (n < 2 || q < 2 || d->n_bonds < 1 || !d->ipair || !d->bond_type || !d->xlocal)
+        return fail(PNED_EINVAL, "pned_model_create: incomplete description");
+    if (q == 2 && n > 32) return fail(PNED_EINVAL, "pned_model_create: n_sites > 32 for S = 1/2");
+    double dimd = std::pow(double(q), n);
+    if (dimd > 9.0e18) return fail(PNED_EINVAL, "pned_model_create: basis too large");
+    if (q > 2 && (q > 4 || n > 32)) return fail(PNED_ENOTSUP, "pned_model_create: mixed radix needs q <= 4, n <= 32");
+    for (int i = 0; i < 2 * d->n_bonds; ++i)
+        if (d->ipair[i] < 1 || d->ipair[i] > n) return fail(PNED_EINVAL, "pned_model_create: ipair out of range");
+    for (int i = 0; i < d->n_bonds; ++i) {
+        if (d->bond_type[i] < 1 || d->bond_type[i] > 9) return fail(PNED_EINVAL, "pned_model_create: bond type");
+        if (d->ipair[2 * i] == d->ipair[2 * i + 1]) return fail(PNED_EINVAL, "pned_model_create: bond on one site");
+    }
+    if (d->parity_type == 0)
+        return fail(PNED_ENOTSUP, "pned_model_create: the Sz-sector basis (parity_type == 0) is not built yet");
+    P = HostProgram{};
+    P.n = n; P.q = q; P.nbond = d->n_bonds;
+    P.dim = 1;
+    for (int i = 0; i < n; ++i) P.dim *= q;
+    std::vector<Bond> bonds = schedule_bonds(d);
+    auto elem = [&](int t, int row, int col) -> cd {
+        const size_t k = size_t(t - 1) * Q * Q + row + size_t(Q) * col;
+        if (d->skip && d->skip[k]) return cd(0, 0);
+        return cd(d->xlocal[k].re, d->xlocal[k].im);
+    };
+    // diagonal tables
+    for (const Bond &b : bonds) {
+        P.dsite1.push_back(b.s1);
+        P.dsite2.push_back(b.s2);
+        for (int st = 0; st < Q; ++st) {
+            cd v = elem(b.t, st, st);
+            if (v.imag() != 0) P.real = false;
+            P.dtab.push_back(v);
+        }
+    }
+    if (q == 2) {
+        // group off-diagonal contributions by flip mask (first-appearance order)
+        struct Contrib { int bond; int f; };
+        std::vector<uint32_t> order;
+        std::map<uint32_t, std::vector<Contrib>> groups;
+        for (size_t bi = 0; bi < bonds.size(); ++bi) {
+            const Bond &b = bonds[bi];
+            for (int f = 1; f < 4; ++f) {
+                bool any = false;
+                for (int st = 0; st < 4; ++st)
+                    if (elem(b.t, st ^ f, st) != cd(0, 0)) any = true;
+                if (!any) continue;
+                uint32_t mask = ((f & 1) ? (1u << b.s1) : 0u) | ((f & 2) ? (1u << b.s2) : 0u);
+                if (!groups.count(mask)) order.push_back(mask);
+                groups[mask].push_back(Contrib{int(bi), f});
+            }
+        }
+        for (uint32_t mask : order) {
+            const auto &cs = groups[mask];
+            // split into pieces whose dependency sites number at most kMaxDeps
+            size_t i = 0;
+            while (i < cs.size()) {
+                std::vector<int> deps;
+                size_t j = i;
+                for (; j < cs.size(); ++j) {
+                    std::vector<int> nd = deps;
+                    for (int s : {bonds[cs[j].bond].s1, bonds[cs[j].bond].s2})
+                        if (std::find(nd.begin(), nd.end(), s) == nd.end()) nd.push_back(s);
+                    if (int(nd.size()) > kMaxDeps) break;
+                    deps = nd;
+                }
+                std::sort(deps.begin(), deps.end());
+                XorTerm term{};
+                term.xmask = mask;
+                term.nb = uint8_t(deps.size());
+                term.pos4 = 0;
+                for (size_t k = 0; k < deps.size(); ++k) term.pos4 |= uint32_t(deps[k]) << (8 * k);
+                term.tab = uint16_t(P.table.size());
+                for (int idx = 0; idx < (1 << deps.size()); ++idx) {
+                    auto bit = [&](int site) {
+                        for (size_t k = 0; k < deps.size(); ++k)
+                            if (deps[k] == site) return (idx >> k) & 1;
+                        return 0;
+                    };
+                    cd c = 0;
+                    for (size_t k = i; k < j; ++k) {
+                        const Bond &b = bonds[cs[k].bond];
+                        const int st = 2 * bit(b.s2) + bit(b.s1);
+                        c += elem(b.t, st ^ cs[k].f, st);
+                    }
+                    if (c.imag() != 0) P.real = false;
+                    P.table.push_back(c);
+                }
+                P.xterms.push_back(term);
+                i = j;
+            }
+        }
+        if (P.xterms.size() > size_t(kMaxTerms)) return fail(PNED_ENOTSUP, "pned_model_create: too many terms");
+    } else {
+        int64_t pw[33];
+        pw[0] = 1;
+        for (int i = 1; i <= n; ++i) pw[i] = pw[i - 1] * q;
+        for (const Bond &b : bonds) {
+            for (int d2 = -(q - 1); d2 <= q - 1; ++d2)
+                for (int d1 = -(q - 1); d1 <= q - 1; ++d1) {
+                    if (d1 == 0 && d2 == 0) continue;
+                    std::vector<cd> tab(Q, cd(0, 0));
+                    bool any = false;
+                    for (int st = 0; st < Q; ++st) {
+                        const int a = st % q, c = st / q;
+                        const int e1 = a + d1, e2 = c + d2;
+                        if (e1 < 0 || e1 >= q || e2 < 0 || e2 >= q) continue;
+                        cd v = elem(b.t, e1 + q * e2, st);
+                        if (v != cd(0, 0)) { any = true; tab[st] = v; }
+                    }
+                    if (!any) continue;
+                    RadixTerm t{};
+                    t.offset = d1 * pw[b.s1] + d2 * pw[b.s2];
+                    t.s1 = uint8_t(b.s1);
+                    t.s2 = uint8_t(b.s2);
+                    t.tab = uint16_t(P.table.size());
+                    for (cd v : tab) {
+                        if (v.imag() != 0) P.real = false;
+                        P.table.push_back(v);
+                    }
+                    P.rterms.push_back(t);
+                }
+        }
+        if (P.rterms.size() > size_t(kMaxTerms)) return fail(PNED_ENOTSUP, "pned_model_create: too many terms");
+    }
+    // the coefficient table is staged into 48 KB of shared memory per block
+    if (P.table.size() > size_t(kMaxTable))
+        return fail(PNED_ENOTSUP, "pned_model_create: coefficient table above 3072 complex entries");
+    return PNED_OK;
+}
+
+}  // namespace pned
+
+// ---------------------------------------------------------------------------
+// Tridiagonal routines (CPU, as in the reference)
+// ---------------------------------------------------------------------------
+extern "C" int pned_bisec(const double *alpha, const double *beta, int ndim, double *E, int ne, double eps)
+{
+    // Sturm-sequence bisection, S1/2 basic.f90:25-107
+    if (ndim > 8000 || ndim < 1) return fail(PNED_EINVAL, "pned_bisec: ndim must be 1..8000");
+    if (ne > ndim || ne < 0) return fail(PNED_EINVAL, "pned_bisec: ne out of range");
+    double range = std::fabs(alpha[0]) + std::fabs(beta[0]);
+    for (int k = 2; k <= ndim - 1; ++k)
+        range = std::max(range, std::fabs(beta[k - 2]) + std::fabs(alpha[k - 1]) + std::fabs(beta[k - 1]));
+    if (ndim >= 2) range = std::max(range, std::fabs(beta[ndim - 2]) + std::fabs(alpha[ndim - 1]));
+    range = -range;
+    std::vector<double> b2(ndim + 1, 0.0);
+    for (int i = 2; i <= ndim; ++i) b2[i - 1] = beta[i - 2] * beta[i - 2];
+    const double epsabs = std::fabs(range) * eps;
+    for (int i = 0; i < ne; ++i) E[i] = -range;
+    double b = range;
+    for (int k = 1; k <= ne; ++k) {
+        double a = E[k - 1];
+        for (int it = 0; it < 100; ++it) {
+            const double c = (a + b) / 2.0;
+            if (std::fabs(a - b) < epsabs) continue;
+            int numneg = 0, ipass = 0;
+            double g = 1.0;
+            for (int i = 1; i <= ndim; ++i) {
+                if (ipass == 0) g = c - alpha[i - 1] - b2[i - 1] / g;
+                else if (ipass == 1) ipass = 2;
+                else { g = c - alpha[i - 1]; ipass = 0; }
+                if (ipass == 0) {
+                    if (g < 0.0) ++numneg;
+                    if (std::fabs(g) < std::fabs(b2[i - 1] * epsabs * eps)) ipass = 1;
+                }
+            }
+            numneg = ndim - numneg;
+            if (numneg < k) b = c;
+            else {
+                a = c;
+                for (int i = k; i <= std::min(numneg, ne); ++i) E[i - 1] = c;
+            }
+        }
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_vec12(const double *alpha, const double *beta, const double *E, int ndim, int nvec, double *v)
+{
+    // inverse iteration on the tridiagonal matrix, S1/2 basic.f90:112-213
+    if (ndim < 1 || nvec < 1 || !v) return fail(PNED_EINVAL, "pned_vec12: bad arguments");
+    std::vector<double> di(ndim + 3), bl(ndim + 3), bu(ndim + 3), bv(ndim + 3), cm(ndim + 3);
+    std::vector<int> lex(ndim + 3);
+    auto V = [&](int j, int k) -> double & { return v[size_t(k - 1) * ndim + j - 1]; };
+    int km = 1;
+    for (int k = 1; k <= nvec; ++k) {
+        for (int j = 1; j <= ndim; ++j) {
+            di[j] = E[k - 1] - alpha[j - 1];
+            bl[j] = -beta[j - 1];
+            bu[j] = -beta[j - 1];
+        }
+        bu[ndim + 1] = 0.0;
+        for (int j = 1; j <= ndim - 1; ++j) {
+            if (std::fabs(di[j]) > std::fabs(bl[j])) {
+                lex[j] = 0;
+                if (std::fabs(di[j]) < 1.e-13) di[j] = 1.e-13;
+                cm[j + 1] = bl[j] / di[j];
+                di[j + 1] = di[j + 1] - cm[j + 1] * bu[j];
+                bv[j] = 0.0;
+            } else {
+                lex[j] = 1;
+                cm[j + 1] = di[j] / bl[j];
+                di[j] = bl[j];
+                const double s = bu[j];
+                bu[j] = di[j + 1];
+                bv[j] = bu[j + 1];
+                di[j + 1] = s - cm[j + 1] * bu[j];
+                bu[j + 1] = -cm[j + 1] * bv[j];
+            }
+        }
+        if (std::fabs(di[ndim]) < 1.e-13) di[ndim] = 1.e-13;
+        for (int j = 1; j <= ndim; ++j) V(j, k) = 1.0 / (double(j) * 5.0);
+        if (k == 1) km = k;
+        else if (std::fabs(E[k - 1] - E[km - 1]) > 1.e-13) km = k;
+        else
+            for (int i = km; i <= k - 1; ++i) {
+                double prd = 0.0;
+                for (int j = 1; j <= ndim; ++j) prd += V(j, i) * V(j, k);
+                for (int j = 1; j <= ndim; ++j) V(j, k) -= prd * V(j, i);
+            }
+        for (int l = 1; l <= k - km + 3; ++l) {
+            if (l != 1 || k != km)
+                for (int j = 1; j <= ndim - 1; ++j) {
+                    if (lex[j] == 0) V(j + 1, k) -= cm[j + 1] * V(j, k);
+                    else {
+                        const double s = V(j, k);
+                        V(j, k) = V(j + 1, k);
+                        V(j + 1, k) = s - cm[j + 1] * V(j, k);
+                    }
+                }
+            for (int j = ndim; j >= 1; --j) {
+                double s = V(j, k);
+                if (j <= ndim - 1) s -= bu[j] * V(j + 1, k);
+                if (j <= ndim - 2) s -= bv[j] * V(j + 2, k);
+                V(j, k) = s / di[j];
+            }
+            double dn = 0.0;
+            for (int j = 1; j <= ndim; ++j) dn += V(j, k) * V(j, k);
+            if (dn > 1.e-13) dn = 1.0 / std::sqrt(dn);
+            for (int j = 1; j <= ndim; ++j) V(j, k) *= dn;
+        }
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_exec_renbun(int i_range, int s_maxitr, double split, double ene, double epsln,
+                                const double *salpha, const double *sbeta, double *w, int *conv, double *dsf)
+{
+    // modified-Lentz continued fraction per omega, S1/2 DSF.f90:263-334
+    if (i_range < 1 || s_maxitr < 2) return fail(PNED_EINVAL, "pned_exec_renbun: bad sizes");
+#pragma omp parallel for schedule(static, 1)
+    for (int j = 1; j <= i_range; ++j) {
+        const double omega = double(j - 1) * split;
+        w[j - 1] = omega;
+        int ic = 0;
+        double xr = 1.0e-10, xi = 1.0e-10, cr = xr, ci = xi, dr = 0.0, di = 0.0;
+        for (int m = 1; m <= s_maxitr - 1; ++m) {
+            const double f1 = omega + ene - salpha[m - 1];
+            const double f2 = -std::pow(sbeta[m - 1], 2.0);
+            const double xr1 = xr, xi1 = xi;
+            dr = dr * f2 + f1;
+            di = di * f2 + epsln;
+            double dd = dr * dr + di * di;
+            if (dd == 0.0) { dr = 0.5e-28; di = 0.5e-28; }
+            double c = cr * cr + ci * ci;
+            cr = cr * f2 / c + f1;
+            ci = -ci * f2 / c + epsln;
+            c = cr * cr + ci * ci;
+            if (c == 0.0) { cr = 0.5e-28; ci = 0.5e-28; }
+            dd = dr * dr + di * di;
+            dr = dr / dd;
+            di = -di / dd;
+            const double dlr = cr * dr - ci * di, dli = ci * dr + cr * di;
+            xr = xr1 * dlr - xi1 * dli;
+            xi = xr1 * dli + xi1 * dlr;
+            if ((dlr - 1.0) * (dlr - 1.0) + dli * dli < 0.5e-28) { ic = m; break; }
+        }
+        if (conv) conv[j - 1] = ic;
+        dsf[j - 1] = xi;
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_normalize_dsf(int i_range, double split, double sq_re, double *dsf)
+{
+    // trapezoid normalisation to S(q), S1/2 DSF.f90:337-351
+    if (i_range < 2 || !dsf) return fail(PNED_EINVAL, "pned_normalize_dsf: bad arguments");
+    double sum = 0.0;
+    for (int i = 2; i <= i_range; ++i) sum += 0.5 * split * (dsf[i - 1] + dsf[i - 2]);
+    for (int i = 0; i < i_range; ++i) dsf[i] = sq_re / sum * dsf[i];
+    return PNED_OK;
+}
+
+extern "C" const char *pned_last_error(void) { return pned::g_err.c_str(); }
+extern "C" int pned_abi_version(void) { return PNED_ABI_VERSION; }

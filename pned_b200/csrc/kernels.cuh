@@ -1,0 +1,71 @@
+// Device kernels of libpned_gpu.so (sm_100a).  FP64 complex throughout.
+//
+// Vectors are interleaved [dim][R]: element (state s, vector r) at s*R + r.
+// A thread owns one state and VPT consecutive vectors of it; G = R/VPT
+// threads share a state.  All reductions are deterministic: a fixed grid
+// writes per-block partial sums in a fixed order and one block finishes them.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pned_internal.h"
+
+namespace pned {
+
+constexpr int kThreads = 256;
+constexpr int kMaxR = 16;
+constexpr int kMaxK = 4;          // reduction quantities per vector in one pass
+constexpr int kMaxVPT = 4;
+
+struct __align__(16) dcplx { double x, y; };
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c)
+{   // a*b + c
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 cconjmul(double2 a, double2 b)
+{   // conj(a) * b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+
+// Term program passed by value as a kernel parameter (constant bank, uniform
+// loads).  Coefficient tables live in global memory and are staged into
+// shared memory per block.
+struct XorProgram {
+    int nterms;
+    int ntab;
+    XorTerm t[kMaxTerms];
+};
+struct RadixProgram {
+    int nterms;
+    int ntab;
+    int n;
+    RadixTerm t[kMaxTerms];
+};
+
+// Per-call scalars: W = pc_r * P + sc_r * (H - shift) (sc_r * C); all from device memory.
+struct HvArgs {
+    const double2 *C;       // input vectors (scaled by sc)
+    const double2 *P;       // optional added vector (may alias W), scaled by pc
+    double2 *W;             // output
+    const double *sc;       // [R] scale of C
+    const double *pc;       // [R] coefficient of P (nullptr: no P term)
+    const void *diag;       // diagonal (double or double2 per state)
+    double shift;           // eperbd * n_bonds subtracted from the diagonal
+    const double2 *table;   // coefficient table (global)
+    double2 *partials;      // [nblocks][K][R]
+    const double2 *G;       // optional previous vector (TPS: vg) scaled by gsc
+    const double *gsc;      // [R]
+    int64_t dim;
+    int R;
+    int K;                  // 1: alpha; 2: alpha, ||W||^2; 4: + <G|W>, <G|C>
+};
+
+}  // namespace pned

@@ -1,0 +1,700 @@
+// Krylov drivers of libpned_gpu.so: Lanczos, mTPQ (TPS), DSF chains and CG
+// inverse iteration.  Scalars (alpha, beta, scales) stay on the device between
+// kernels, so a run of steps needs no host round trip and is replayed as a
+// CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "device.cuh"
+
+namespace pned {
+
+// ---------------------------------------------------------------------------
+// step epilogues (one block, one thread per vector)
+// ---------------------------------------------------------------------------
+
+// Lanczos: alpha = Re(sum0), beta = sqrt(sum1); record; next scales.
+__global__ void lanczos_epilogue(const double2 *__restrict__ sa, const double2 *__restrict__ sb, int R,
+                                 double *sc, double *pc, double *d_alpha, double *d_beta, int *counter,
+                                 int *flag)
+{
+    __shared__ int k;
+    if (threadIdx.x == 0) k = *counter;
+    __syncthreads();
+    const int r = threadIdx.x;
+    if (r < R) {
+        const double al = sa[r].x;
+        const double be = sqrt(sb[r].x);
+        d_alpha[(size_t)k * R + r] = al;
+        d_beta[(size_t)k * R + r] = be;
+        if (!(be >= 0.5e-30)) atomicOr(flag, 1);
+        const double old = sc[r];
+        sc[r] = 1.0 / be;
+        pc[r] = -be * old;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = k + 1;
+}
+
+// TPS: alpha1 = Re<v|(L-H)v>, beta = ||(L-H)v||, coef as eval_phys_val.
+__global__ void tps_epilogue(const double2 *__restrict__ s, int R, int nobs, const double2 *__restrict__ so, double L,
+                             double *sc, double *gsc, double *d_alpha, double *d_beta, double *d_coef, int ncoef,
+                             int *counter)
+{
+    __shared__ int k;
+    if (threadIdx.x == 0) k = *counter;
+    __syncthreads();
+    const int r = threadIdx.x;
+    if (r < R) {
+        const double a1 = s[0 * R + r].x;
+        const double be = sqrt(s[1 * R + r].x);
+        const double2 gw = s[2 * R + r], gv = s[3 * R + r];
+        d_alpha[(size_t)k * R + r] = L - a1;
+        d_beta[(size_t)k * R + r] = be;
+        double *cf = d_coef + ((size_t)k * R + r) * ncoef;
+        cf[0] = double(2 * (k + 1)) / a1;
+        cf[1] = L;
+        cf[2] = be;
+        cf[3] = L - a1;
+        cf[4] = L * gv.x - gw.x;   // Re(L <vg|v1> - <vg|v0>)
+        for (int o = 0; o < nobs; ++o) {
+            cf[5 + 2 * o] = so[(2 * o) * R + r].x;
+            cf[6 + 2 * o] = so[(2 * o + 1) * R + r].x;
+        }
+        gsc[r] = sc[r];
+        sc[r] = 1.0 / be;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = k + 1;
+}
+
+// Diagonal observables: <v|O v> and <g|O v>, v = sc C, g = gsc G.
+__global__ void __launch_bounds__(kThreads) obs_kernel(const double2 *__restrict__ C, const double2 *__restrict__ G,
+                                                       const double *__restrict__ sc, const double *__restrict__ gsc,
+                                                       int64_t dim, int R, int vpt, int n, int nterm,
+                                                       const int *__restrict__ ta, const int *__restrict__ tb,
+                                                       const double2 *__restrict__ tc, const double2 *__restrict__ T,
+                                                       double2 *partials)
+{
+    double2 red[2][kMaxVPT];
+    for (int k = 0; k < 2; ++k)
+        for (int j = 0; j < kMaxVPT; ++j) red[k][j] = make_double2(0.0, 0.0);
+    const int Gs = R / vpt, r0 = (threadIdx.x % Gs) * vpt;
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * Gs;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t st = it / Gs;
+        double2 w = make_double2(0.0, 0.0);
+        for (int t = 0; t < nterm; ++t) {
+            const int i = ta[t] >= n ? 0 : int((st >> ta[t]) & 1);
+            const int k = tb[t] >= n ? 0 : int((st >> tb[t]) & 1);
+            w = cfma(tc[t], T[2 * i + k], w);
+        }
+        const int64_t base = st * R + r0;
+#pragma unroll
+        for (int j = 0; j < kMaxVPT; ++j) {
+            if (j >= vpt) break;
+            const double2 v = cscale(sc[r0 + j], C[base + j]);
+            const double2 ov = cmul(w, v);
+            red[0][j] = cadd(red[0][j], cconjmul(v, ov));
+            if (G) red[1][j] = cadd(red[1][j], cconjmul(cscale(gsc[r0 + j], G[base + j]), ov));
+        }
+    }
+    block_reduce_store<2, kMaxVPT>(red, Gs, vpt, R, partials);
+}
+
+// S^z_q start vectors: C[s, r] = sum_j (d_j(s) - S) e^{i qr[r, j]} x[s].
+__global__ void __launch_bounds__(kThreads) szq_kernel(const double2 *__restrict__ x, const double2 *__restrict__ ph,
+                                                       int64_t dim, int R, int vpt, int n, int q, double2 *C,
+                                                       double2 *partials)
+{
+    double2 red[1][kMaxVPT];
+    for (int j = 0; j < kMaxVPT; ++j) red[0][j] = make_double2(0.0, 0.0);
+    const int Gs = R / vpt, r0 = (threadIdx.x % Gs) * vpt;
+    const double S = 0.5 * (q - 1);
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * Gs;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t st = it / Gs;
+        double2 w[kMaxVPT];
+        for (int j = 0; j < kMaxVPT; ++j) w[j] = make_double2(0.0, 0.0);
+        int64_t y = st;
+        for (int site = 0; site < n; ++site) {
+            int64_t dj;
+            if (q == 2) { dj = y & 1; y >>= 1; }
+            else { const int64_t z = y / q; dj = y - z * q; y = z; }
+            const double f = double(dj) - S;
+#pragma unroll
+            for (int j = 0; j < kMaxVPT; ++j) {
+                if (j >= vpt) break;
+                const double2 p = ph[(r0 + j) * n + site];
+                w[j].x = fma(f, p.x, w[j].x);
+                w[j].y = fma(f, p.y, w[j].y);
+            }
+        }
+        const double2 xs = x[st];
+#pragma unroll
+        for (int j = 0; j < kMaxVPT; ++j) {
+            if (j >= vpt) break;
+            const double2 v = cmul(w[j], xs);
+            C[st * R + r0 + j] = v;
+            red[0][j].x += v.x * v.x + v.y * v.y;
+        }
+    }
+    block_reduce_store<1, kMaxVPT>(red, Gs, vpt, R, partials);
+}
+
+__global__ void dsf_start_epilogue(const double2 *__restrict__ s, int R, int n, double *sc, double *cnorm)
+{
+    const int r = threadIdx.x;
+    if (r < R) {
+        double raw = s[r].x;
+        if (raw < 1e-25) raw = 1e-25;
+        cnorm[r] = raw / double(n);
+        sc[r] = 1.0 / sqrt(raw);
+    }
+}
+
+// x += a p ; r -= a y    (complex a, one vector)
+__global__ void cg_update_xr(double2 *x, double2 *r, const double2 *__restrict__ p, const double2 *__restrict__ y,
+                             double2 a, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] = cfma(a, p[i], x[i]);
+        const double2 ay = cmul(a, y[i]);
+        r[i] = make_double2(r[i].x - ay.x, r[i].y - ay.y);
+    }
+}
+
+// p = r + b p
+__global__ void cg_update_p(double2 *p, const double2 *__restrict__ r, double b, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = make_double2(r[i].x + b * p[i].x, r[i].y + b * p[i].y);
+}
+
+__global__ void scale_real_kernel(double2 *v, double f, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = cscale(f, v[i]);
+}
+
+// ---------------------------------------------------------------------------
+// one step of each kind; buffer roles live in the session
+// ---------------------------------------------------------------------------
+
+// Lanczos (b0 = C, b1 = P, b2 = W):
+//   W = -beta_{i-1} v_{i-1} + H v_i,  alpha_i = <v_i|H v_i>     (hv kernel)
+//   R = W - alpha_i v_i, beta_i = ||W - alpha_i v_i||           (residual kernel)
+// written into the old P buffer, which becomes C (v_{i+1} = R / beta_i).
+static cudaError_t lanczos_step(pned_ctx *c, Session &S, bool first)
+{
+    const int R = c->R;
+    HvArgs a{};
+    a.C = c->buf[S.b0];
+    a.P = first ? nullptr : c->buf[S.b1];
+    a.W = c->buf[S.b2];
+    a.sc = slot(c, kSlotSc);
+    a.pc = first ? nullptr : slot(c, kSlotPc);
+    a.diag = c->m->d_diag;
+    a.shift = 0.0;
+    a.table = c->m->d_table;
+    a.partials = c->partials;
+    a.dim = c->m->dim;
+    a.R = R;
+    a.K = 1;
+    double2 *sa = c->sums, *sb = c->sums + kMaxK * kMaxR;
+    if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
+    cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
+    if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
+    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, sa, c->stream);
+    if (e == cudaSuccess)
+        e = launch_residual(c, c->buf[S.b2], c->buf[S.b0], c->buf[S.b1], slot(c, kSlotSc), sa, c->stream);
+    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, sb, c->stream);
+    if (e == cudaSuccess) {
+        lanczos_epilogue<<<1, 32 * ((R + 31) / 32), 0, c->stream>>>(sa, sb, R, slot(c, kSlotSc), slot(c, kSlotPc),
+                                                                   S.d_alpha, S.d_beta, S.d_counter, S.d_flag);
+        e = cudaGetLastError();
+    }
+    std::swap(S.b0, S.b1);
+    return e;
+}
+
+// TPS (b0 = C = |k> scaled, b1 = W, b2 = G = |k-1> scaled):
+//   W = (L - H)^T v, alpha1 = <v|W>, beta = ||W||, <vg|W>, <vg|v>  (one fused kernel)
+// then G <- C, C <- W (scale 1/beta), W <- old G.
+static cudaError_t tps_step(pned_ctx *c, Session &S, bool first)
+{
+    const int R = c->R;
+    HvArgs a{};
+    a.C = c->buf[S.b0]; a.P = nullptr; a.W = c->buf[S.b1];
+    a.sc = slot(c, kSlotSc); a.pc = nullptr;
+    a.diag = c->m->d_diag; a.shift = 0.0;
+    a.table = c->m->d_table; a.partials = c->partials;
+    a.G = first ? nullptr : c->buf[S.b2]; a.gsc = slot(c, kSlotGsc);
+    a.dim = c->m->dim; a.R = R; a.K = 4;
+    if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
+    cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
+    if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
+    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, 4 * R, c->sums, c->stream);
+    if (first && e == cudaSuccess) e = cudaMemsetAsync(c->sums + 2 * R, 0, sizeof(double2) * 2 * R, c->stream);
+    for (int o = 0; o < S.nobs && e == cudaSuccess; ++o) {
+        const DevObs &ob = S.obs[o];
+        obs_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(c->buf[S.b0], first ? nullptr : c->buf[S.b2],
+                                                          slot(c, kSlotSc), slot(c, kSlotGsc), c->m->dim, R,
+                                                          pick_vpt(R), c->m->n, ob.n, ob.a, ob.b, ob.c, ob.T,
+                                                          c->partials);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, 2 * R, S.d_osum + 2 * o * R, c->stream);
+    }
+    if (e == cudaSuccess) {
+        tps_epilogue<<<1, 32 * ((R + 31) / 32), 0, c->stream>>>(c->sums, R, S.nobs, S.d_osum, S.L, slot(c, kSlotSc),
+                                                               slot(c, kSlotGsc), S.d_alpha, S.d_beta, S.d_coef,
+                                                               S.ncoef, S.d_counter);
+        e = cudaGetLastError();
+    }
+    const int og = S.b2;
+    S.b2 = S.b0; S.b0 = S.b1; S.b1 = og;
+    return e;
+}
+
+static cudaError_t one_step(pned_ctx *c, Session &S, bool first)
+{
+    return S.kind == PNED_SESSION_TPS ? tps_step(c, S, first) : lanczos_step(c, S, first);
+}
+
+template <class T> static T *sess_alloc(Session &S, size_t n)
+{
+    void *q = nullptr;
+    if (cudaMalloc(&q, sizeof(T) * std::max<size_t>(1, n)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    S.allocs.push_back(q);
+    return static_cast<T *>(q);
+}
+
+void session_release(pned_ctx *c)
+{
+    Session &S = c->sess;
+    if (S.graph) cudaGraphExecDestroy(S.graph);
+    for (void *q : S.allocs) cudaFree(q);
+    c->sess = Session{};
+}
+
+static int session_common_begin(pned_ctx *c, int kind, int max_steps)
+{
+    if (c->sess.kind) {
+        cudaStreamSynchronize(c->stream);
+        session_release(c);
+    }
+    Session &S = c->sess;
+    S.kind = kind;
+    S.max_steps = max_steps;
+    S.period = kind == PNED_SESSION_TPS ? 3 : 2;
+    S.b0 = 2; S.b1 = 3; S.b2 = 4;
+    int rc = 0;
+    for (int k : {2, 3, 4})
+        if ((rc = ctx_alloc_buffer(c, k))) { session_release(c); return rc; }
+    const int R = c->R;
+    S.d_alpha = sess_alloc<double>(S, size_t(max_steps) * R);
+    S.d_beta = sess_alloc<double>(S, size_t(max_steps) * R);
+    S.d_counter = sess_alloc<int>(S, 2);
+    if (!S.d_alpha || !S.d_beta || !S.d_counter) { session_release(c); return fail(PNED_ENOMEM, "session scratch"); }
+    S.d_flag = S.d_counter + 1;
+    cudaError_t e = cudaMemsetAsync(S.d_counter, 0, 2 * sizeof(int), c->stream);
+    if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "session memset"); }
+    return PNED_OK;
+}
+
+}  // namespace pned
+
+using namespace pned;
+
+extern "C" int pned_session_begin(pned_ctx *c, int kind, const pned_c128 *v_init, int max_steps, double L, int n_obs,
+                                  const pned_observable *obs, int flags)
+{
+    if (!c || !v_init || max_steps < 1 || n_obs < 0 || (n_obs && !obs) || n_obs > 6)
+        return fail(PNED_EINVAL, "pned_session_begin: bad arguments");
+    if (kind != PNED_SESSION_LANCZOS && kind != PNED_SESSION_TPS)
+        return fail(PNED_EINVAL, "pned_session_begin: kind must be LANCZOS or TPS (DSF: pned_session_begin_dsf)");
+    if (kind == PNED_SESSION_LANCZOS && n_obs) return fail(PNED_EINVAL, "observables belong to TPS sessions");
+    cudaSetDevice(c->m->device);
+    int rc = session_common_begin(c, kind, max_steps);
+    if (rc) return rc;
+    Session &S = c->sess;
+    const int R = c->R;
+    const size_t bytes = sizeof(double2) * size_t(c->m->dim) * R;
+    cudaError_t e = cudaMemcpyAsync(c->buf[S.b0], v_init, bytes,
+                                    (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "pned_session_begin: staging v_init"); }
+    if (kind == PNED_SESSION_TPS) {
+        S.L = L;
+        S.nobs = n_obs;
+        S.ncoef = 5 + 2 * n_obs;
+        S.d_coef = sess_alloc<double>(S, size_t(max_steps) * R * S.ncoef);
+        S.d_osum = sess_alloc<double2>(S, size_t(2 * std::max(1, n_obs)) * R);
+        if (!S.d_coef || !S.d_osum) { session_release(c); return fail(PNED_ENOMEM, "session scratch"); }
+        for (int o = 0; o < n_obs; ++o) {
+            DevObs d;
+            d.n = obs[o].n_terms;
+            d.a = sess_alloc<int>(S, d.n);
+            d.b = sess_alloc<int>(S, d.n);
+            d.c = sess_alloc<double2>(S, d.n);
+            d.T = sess_alloc<double2>(S, 4);
+            if (!d.a || !d.b || !d.c || !d.T) { session_release(c); return fail(PNED_ENOMEM, "observables"); }
+            if (d.n) {
+                e = cudaMemcpyAsync(d.a, obs[o].a, sizeof(int) * d.n, cudaMemcpyHostToDevice, c->stream);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(d.b, obs[o].b, sizeof(int) * d.n, cudaMemcpyHostToDevice, c->stream);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(d.c, obs[o].c, sizeof(double2) * d.n, cudaMemcpyHostToDevice, c->stream);
+            }
+            if (e == cudaSuccess) e = cudaMemcpyAsync(d.T, obs[o].T, sizeof(double2) * 4, cudaMemcpyHostToDevice, c->stream);
+            if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "observables"); }
+            S.obs.push_back(d);
+        }
+        // observable uploads read host memory that may go away after this call
+        e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "observables"); }
+        if ((rc = set_slot(c, kSlotGsc, 0.0))) { session_release(c); return rc; }
+    }
+    if ((rc = set_slot(c, kSlotSc, 1.0))) { session_release(c); return rc; }
+    return PNED_OK;
+}
+
+extern "C" int pned_session_begin_dsf(pned_ctx *c, const pned_c128 *x, const double *qr, int max_steps, double *cnorm,
+                                      int flags)
+{
+    if (!c || !x || !qr || max_steps < 1) return fail(PNED_EINVAL, "pned_session_begin_dsf: bad arguments");
+    cudaSetDevice(c->m->device);
+    int rc = session_common_begin(c, PNED_SESSION_DSF, max_steps);
+    if (rc) return rc;
+    Session &S = c->sess;
+    const int R = c->R, n = c->m->n;
+    const size_t dim = size_t(c->m->dim);
+    const double2 *dx = reinterpret_cast<const double2 *>(x);
+    cudaError_t e = cudaSuccess;
+    if (!(flags & PNED_PTR_DEVICE)) {
+        double2 *tmp = sess_alloc<double2>(S, dim);
+        if (!tmp) { session_release(c); return fail(PNED_ENOMEM, "pned_session_begin_dsf: staging x"); }
+        e = cudaMemcpyAsync(tmp, x, sizeof(double2) * dim, cudaMemcpyHostToDevice, c->stream);
+        dx = tmp;
+    }
+    std::vector<double2> ph(size_t(R) * n);
+    for (int r = 0; r < R; ++r)
+        for (int j = 0; j < n; ++j) ph[size_t(r) * n + j] = make_double2(std::cos(qr[r * n + j]), std::sin(qr[r * n + j]));
+    double2 *dph = sess_alloc<double2>(S, ph.size());
+    double *dcn = sess_alloc<double>(S, R);
+    if (!dph || !dcn) { session_release(c); return fail(PNED_ENOMEM, "pned_session_begin_dsf: scratch"); }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dph, ph.data(), sizeof(double2) * ph.size(), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        szq_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(dx, dph, c->m->dim, R, pick_vpt(R), n, c->m->q,
+                                                          c->buf[S.b0], c->partials);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, c->sums, c->stream);
+    if (e == cudaSuccess) {
+        dsf_start_epilogue<<<1, 32 * ((R + 31) / 32), 0, c->stream>>>(c->sums, R, n, slot(c, kSlotSc), dcn);
+        e = cudaGetLastError();
+    }
+    std::vector<double> hc(R);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hc.data(), dcn, sizeof(double) * R, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "pned_session_begin_dsf: S^z_q"); }
+    if (cnorm) std::copy(hc.begin(), hc.end(), cnorm);
+    return PNED_OK;
+}
+
+extern "C" int pned_session_step(pned_ctx *c, int n_steps)
+{
+    if (!c || n_steps < 0) return fail(PNED_EINVAL, "pned_session_step: bad arguments");
+    Session &S = c->sess;
+    if (!S.kind) return fail(PNED_EINVAL, "pned_session_step: no session");
+    if (S.enqueued + n_steps > S.max_steps)
+        return fail(PNED_EINVAL, "pned_session_step: more steps than max_steps of the session");
+    cudaSetDevice(c->m->device);
+    cudaError_t e = cudaSuccess;
+    while (n_steps > 0) {
+        if (S.enqueued == 0) {
+            e = one_step(c, S, true);
+            if (e != cudaSuccess) return cuda_fail(e, "first Krylov step");
+            ++S.enqueued; --n_steps;
+            continue;
+        }
+        const bool roles_match = S.graph && S.b0 == S.g0 && S.b1 == S.g1 && S.b2 == S.g2;
+        if (roles_match && n_steps >= S.period) {
+            e = cudaGraphLaunch(S.graph, c->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+            S.enqueued += S.period; n_steps -= S.period;
+            continue;
+        }
+        if (!S.graph && n_steps >= 2 * S.period) {
+            // capture `period` steps: the buffer roles come back to where they started
+            cudaGraph_t graph;
+            e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+            const int s0 = S.b0, s1 = S.b1, s2 = S.b2;
+            cudaError_t ek = cudaSuccess;
+            for (int k = 0; k < S.period; ++k) {
+                cudaError_t q = one_step(c, S, false);
+                if (q != cudaSuccess) ek = q;
+            }
+            e = cudaStreamEndCapture(c->stream, &graph);
+            if (e == cudaSuccess && ek != cudaSuccess) e = ek;
+            if (e == cudaSuccess) {
+                e = cudaGraphInstantiate(&S.graph, graph, 0);
+                cudaGraphDestroy(graph);
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "capturing the Krylov step graph");
+            S.g0 = s0; S.g1 = s1; S.g2 = s2;
+            S.b0 = s0; S.b1 = s1; S.b2 = s2;
+            continue;
+        }
+        e = one_step(c, S, false);
+        if (e != cudaSuccess) return cuda_fail(e, "Krylov step");
+        ++S.enqueued; --n_steps;
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_session_read(pned_ctx *c, double *alpha, double *beta, double *coef, int *steps_done,
+                                 int *status_out)
+{
+    if (!c) return fail(PNED_EINVAL, "pned_session_read: null context");
+    Session &S = c->sess;
+    if (!S.kind) return fail(PNED_EINVAL, "pned_session_read: no session");
+    cudaSetDevice(c->m->device);
+    const int R = c->R, k = S.enqueued;
+    cudaError_t e = cudaSuccess;
+    if (alpha && k) e = cudaMemcpyAsync(alpha, S.d_alpha, sizeof(double) * size_t(k) * R, cudaMemcpyDeviceToHost, c->stream);
+    if (beta && k && e == cudaSuccess)
+        e = cudaMemcpyAsync(beta, S.d_beta, sizeof(double) * size_t(k) * R, cudaMemcpyDeviceToHost, c->stream);
+    if (coef && k && S.kind == PNED_SESSION_TPS && e == cudaSuccess)
+        e = cudaMemcpyAsync(coef, S.d_coef, sizeof(double) * size_t(k) * R * S.ncoef, cudaMemcpyDeviceToHost, c->stream);
+    int flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, S.d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_read");
+    if (steps_done) *steps_done = k;
+    if (status_out) *status_out = flag;
+    return PNED_OK;
+}
+
+extern "C" int pned_session_vector(pned_ctx *c, pned_c128 **dev_ptr, double *scale_out)
+{
+    if (!c || !dev_ptr) return fail(PNED_EINVAL, "pned_session_vector: bad arguments");
+    Session &S = c->sess;
+    if (!S.kind) return fail(PNED_EINVAL, "pned_session_vector: no session");
+    *dev_ptr = reinterpret_cast<pned_c128 *>(c->buf[S.b0]);
+    if (scale_out) {
+        double h[kMaxR];
+        cudaError_t e = cudaMemcpyAsync(h, slot(c, kSlotSc), sizeof(double) * kMaxR, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "pned_session_vector");
+        for (int r = 0; r < c->R; ++r) scale_out[r] = h[r];
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_session_profile(pned_ctx *c, int n_steps, double *hv_ms, double *step_ms)
+{
+    if (!c || n_steps < 1 || !hv_ms || !step_ms) return fail(PNED_EINVAL, "pned_session_profile: bad arguments");
+    Session &S = c->sess;
+    if (!S.kind || S.enqueued < 1) return fail(PNED_EINVAL, "pned_session_profile: needs a started session");
+    if (S.enqueued + n_steps > S.max_steps) return fail(PNED_EINVAL, "pned_session_profile: beyond max_steps");
+    cudaSetDevice(c->m->device);
+    cudaEvent_t e0, e1, s0, s1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&s0); cudaEventCreate(&s1);
+    double thv = 0, tst = 0;
+    cudaError_t e = cudaSuccess;
+    S.ev_hv0 = e0; S.ev_hv1 = e1;
+    for (int k = 0; k < n_steps && e == cudaSuccess; ++k) {
+        cudaEventRecord(s0, c->stream);
+        e = one_step(c, S, false);
+        cudaEventRecord(s1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(s1);
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, s0, s1);
+        thv += a; tst += b;
+        ++S.enqueued;
+    }
+    S.ev_hv0 = S.ev_hv1 = nullptr;
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(s0); cudaEventDestroy(s1);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_profile");
+    *hv_ms = thv / n_steps;
+    *step_ms = tst / n_steps;
+    return PNED_OK;
+}
+
+extern "C" int pned_session_end(pned_ctx *c)
+{
+    if (!c) return fail(PNED_EINVAL, "pned_session_end: null context");
+    cudaSetDevice(c->m->device);
+    cudaStreamSynchronize(c->stream);
+    session_release(c);
+    return PNED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// whole-run drivers
+// ---------------------------------------------------------------------------
+extern "C" int pned_lanczos_run(pned_ctx *c, const pned_c128 *v_init, int n_steps, int check_conv, double *alpha,
+                                double *beta, double *ene, int *steps_done, int flags)
+{
+    if (!c || !v_init || !alpha || !beta || n_steps < 1) return fail(PNED_EINVAL, "pned_lanczos_run: bad arguments");
+    if (check_conv && c->R != 1) return fail(PNED_EINVAL, "pned_lanczos_run: check_conv needs R = 1");
+    int rc = pned_session_begin(c, PNED_SESSION_LANCZOS, v_init, n_steps, 0.0, 0, nullptr, flags);
+    if (rc) return rc;
+    const int R = c->R;
+    int done = 0;
+    if (!check_conv) {
+        rc = pned_session_step(c, n_steps);
+        done = n_steps;
+    } else {
+        // the nvec = 8 stop of S1/2 Lanczos.f90:133-155: bisec at i = 32 and every
+        // 5th step after it, stop when ene(8) changes by less than 1e-13 relative
+        const int nvec2 = 8;
+        double ebefor = 0.0;
+        std::vector<double> a, b;
+        while (done < n_steps && !rc) {
+            int next = done < 4 * nvec2 ? std::min(4 * nvec2, n_steps) : std::min((done / 5 + 1) * 5, n_steps);
+            if ((rc = pned_session_step(c, next - done))) break;
+            done = next;
+            if (done < 4 * nvec2 || (done > 4 * nvec2 && done % 5)) continue;
+            a.resize(done); b.resize(done);
+            if ((rc = pned_session_read(c, a.data(), b.data(), nullptr, nullptr, nullptr))) break;
+            double E[8];
+            pned_bisec(a.data(), b.data(), done, E, nvec2, 1e-25);
+            if (done == 4 * nvec2) { ebefor = E[nvec2 - 1]; continue; }
+            if (std::fabs((ebefor - E[nvec2 - 1]) / E[nvec2 - 1]) < 1e-13) break;
+            ebefor = E[nvec2 - 1];
+        }
+    }
+    int status = 0, k = 0;
+    if (!rc) rc = pned_session_read(c, alpha, beta, nullptr, &k, &status);
+    pned_session_end(c);
+    if (rc) return rc;
+    if (steps_done) *steps_done = k;
+    if (ene) {
+        std::vector<double> a0(k), b0(k);
+        for (int i = 0; i < k; ++i) { a0[i] = alpha[size_t(i) * R]; b0[i] = beta[size_t(i) * R]; }
+        for (int i = 0; i < 8; ++i) ene[i] = 0.0;
+        pned_bisec(a0.data(), b0.data(), k, ene, std::min(k, 8), 1e-25);
+    }
+    if (status) return fail(PNED_EBREAKDOWN, "Lanczos beta below 0.5e-30 (tridiagonalisation unsuccessful)");
+    return PNED_OK;
+}
+
+extern "C" int pned_tps_run(pned_ctx *c, double L, const pned_c128 *v_init, int n_steps, int n_obs,
+                            const pned_observable *obs, double *alpha, double *beta, double *coef, int flags)
+{
+    if (!c || !v_init || !alpha || !beta || !coef || n_steps < 1)
+        return fail(PNED_EINVAL, "pned_tps_run: bad arguments");
+    int rc = pned_session_begin(c, PNED_SESSION_TPS, v_init, n_steps, L, n_obs, obs, flags);
+    if (rc) return rc;
+    rc = pned_session_step(c, n_steps);
+    if (!rc) rc = pned_session_read(c, alpha, beta, coef, nullptr, nullptr);
+    pned_session_end(c);
+    return rc;
+}
+
+extern "C" int pned_dsf_run(pned_ctx *c, const pned_c128 *x, const double *qr, int n_steps, double *cnorm,
+                            double *salpha, double *sbeta, int flags)
+{
+    if (!c || !x || !qr || !cnorm || !salpha || !sbeta || n_steps < 1)
+        return fail(PNED_EINVAL, "pned_dsf_run: bad arguments");
+    int rc = pned_session_begin_dsf(c, x, qr, n_steps, cnorm, flags);
+    if (rc) return rc;
+    const int R = c->R;
+    std::vector<double> b(size_t(n_steps) * R);
+    rc = pned_session_step(c, n_steps);
+    int status = 0;
+    if (!rc) rc = pned_session_read(c, salpha, b.data(), nullptr, nullptr, &status);
+    pned_session_end(c);
+    if (rc) return rc;
+    for (int r = 0; r < R; ++r) sbeta[r] = cnorm[r];
+    for (size_t i = 0; i < b.size(); ++i) sbeta[R + i] = b[i];
+    return PNED_OK;
+}
+
+extern "C" int pned_cg_run(pned_ctx *c, double E, const pned_c128 *b_init, int inv_max, int cg_max, pned_c128 *x_out,
+                           int *n_inv, int *n_cg, int flags)
+{
+    if (!c || !b_init || !x_out || inv_max < 1 || cg_max < 1) return fail(PNED_EINVAL, "pned_cg_run: bad arguments");
+    if (c->R != 1) return fail(PNED_EINVAL, "pned_cg_run: needs a context with R = 1");
+    cudaSetDevice(c->m->device);
+    int rc = 0;
+    for (int k = 0; k < 5; ++k)
+        if ((rc = ctx_alloc_buffer(c, k))) return rc;
+    double2 *x = c->buf[0], *b = c->buf[1], *p = c->buf[2], *r = c->buf[3], *y = c->buf[4];
+    const int64_t n = c->m->dim;
+    const size_t bytes = sizeof(double2) * size_t(n);
+    cudaError_t e = cudaMemcpyAsync(b, b_init, bytes,
+                                    (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_cg_run: staging b");
+    if ((rc = set_slot(c, kSlotOne, 1.0))) return rc;
+    const int nb = c->nblocks;
+    auto dot = [&](const double2 *u, const double2 *v, double2 &out) -> int {
+        cudaError_t err = launch_dot(c, u, v, nullptr, 0, c->sums, c->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "cg dot");
+        int q = sums_to_host(c, 1);
+        out = c->h_sums[0];
+        return q;
+    };
+    bool cg_loop_saved = false;   // the SAVEd `loop` flag of cg1 (S1/2 cg.f90:118)
+    int total_cg = 0, itr_inv = 0;
+    for (int it = 1; it <= inv_max; ++it) {
+        itr_inv = it;
+        // ---- cg1: solve (H - E) x = b
+        double2 bc;
+        if ((rc = dot(b, b, bc))) return rc;
+        e = cudaMemcpyAsync(r, b, bytes, cudaMemcpyDeviceToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p, b, bytes, cudaMemcpyDeviceToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, bytes, c->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cg init");
+        for (int k = 1; k <= cg_max; ++k) {
+            ++total_cg;
+            HvArgs a{};
+            a.C = p; a.P = nullptr; a.W = y;
+            a.sc = slot(c, kSlotOne); a.pc = nullptr;
+            a.diag = c->m->d_diag;
+            a.shift = (E / double(c->m->nbond)) * double(c->m->nbond);
+            a.table = c->m->d_table; a.partials = c->partials;
+            a.dim = n; a.R = 1; a.K = 1;
+            e = launch_hv(c->m, a, nb, c->stream);
+            if (e != cudaSuccess) return cuda_fail(e, "cg hv");
+            double2 crp, cyp, rc1, rc2;
+            if ((rc = dot(p, r, crp)) || (rc = dot(p, y, cyp)) || (rc = dot(r, r, rc1))) return rc;
+            const double den = cyp.x * cyp.x + cyp.y * cyp.y;
+            const double2 al = make_double2((crp.x * cyp.x + crp.y * cyp.y) / den, (crp.y * cyp.x - crp.x * cyp.y) / den);
+            cg_update_xr<<<nb, kThreads, 0, c->stream>>>(x, r, p, y, al, n);
+            if ((rc = dot(r, r, rc2))) return rc;
+            const double beta = rc2.x / rc1.x;
+            cg_update_p<<<nb, kThreads, 0, c->stream>>>(p, r, beta, n);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail(e, "cg update");
+            if (k % 5 != 0) continue;
+            if (std::sqrt(std::hypot(rc2.x, rc2.y)) < 1.0e-9 * std::sqrt(std::hypot(bc.x, bc.y))) cg_loop_saved = true;
+            if (cg_loop_saved) break;
+        }
+        // ---- normalise x, test |<x|b>| = 1
+        double2 xx, xb;
+        if ((rc = dot(x, x, xx))) return rc;
+        scale_real_kernel<<<nb, kThreads, 0, c->stream>>>(x, 1.0 / std::sqrt(xx.x), n);
+        if ((rc = dot(x, b, xb))) return rc;
+        if (std::fabs(std::hypot(xb.x, xb.y) - 1.0) < 1.0e-12) break;
+        e = cudaMemcpyAsync(b, x, bytes, cudaMemcpyDeviceToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cg copy");
+    }
+    e = cudaMemcpyAsync(x_out, x, bytes, (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_cg_run: result");
+    if (n_inv) *n_inv = itr_inv;
+    if (n_cg) *n_cg = total_cg;
+    return PNED_OK;
+}

@@ -1,0 +1,65 @@
+// Internal declarations shared by the host and device translation units of
+// libpned_gpu.so.  Nothing here is part of the C ABI.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pned_gpu.h"
+
+namespace pned {
+
+using cd = std::complex<double>;
+
+// Thread-local error message behind pned_last_error().
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+
+// ---------------------------------------------------------------------------
+// Compiled term program
+// ---------------------------------------------------------------------------
+constexpr int kMaxDeps = 4;      // dependency bits per xor term
+constexpr int kMaxTerms = 640;   // gather terms per program (kernel parameter space)
+constexpr int kMaxTable = 3072;  // coefficient-table entries (48 KB of shared memory)
+
+// One gather term of the S = 1/2 (q = 2) program: partner = s ^ xmask,
+// coefficient = table[tab + idx] with idx gathered from the `nb` dependency
+// bits (pos packed 8 bits each, bit k of idx = bit pos_k of s).
+struct XorTerm {
+    uint32_t xmask;
+    uint32_t pos4;
+    uint16_t tab;
+    uint8_t nb;
+    uint8_t pad;
+};
+
+// One gather term of the mixed-radix (q > 2) program: partner = s + offset,
+// coefficient = table[tab + d(s1) + q*d(s2)] (zero where the target digit
+// leaves 0..q-1; the load is skipped for zero coefficients).
+struct RadixTerm {
+    int64_t offset;
+    uint8_t s1, s2;
+    uint16_t tab;
+    uint32_t pad;
+};
+
+struct HostProgram {
+    int n = 0, q = 2;
+    int64_t dim = 0;
+    int nbond = 0;
+    bool real = true;                    // every coefficient and diagonal entry real
+    std::vector<XorTerm> xterms;         // q == 2
+    std::vector<RadixTerm> rterms;       // q > 2
+    std::vector<cd> table;               // coefficient tables
+    // diagonal: per bond (s1, s2) and q*q diagonal values (pair state st)
+    std::vector<int> dsite1, dsite2;
+    std::vector<cd> dtab;                // [nbond][Q]
+};
+
+// Builds the program from a model description (bond order, skip mask and
+// element order follow make_cpu_list2; see model.cpp).
+int compile_program(const pned_model_desc *d, HostProgram &out);
+
+}  // namespace pned

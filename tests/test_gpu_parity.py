@@ -1,0 +1,250 @@
+"""GPU parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerances (FP64 complex throughout):
+  H.v           relative 2-norm <= 1e-12, prdct relative <= 1e-12
+  Lanczos E0    relative <= 1e-10; first alpha/beta relative <= 1e-10
+  TPS           alpha, beta, coef relative <= 1e-10
+  DSF           cnorm, chain coefficients and spectra relative <= 1e-10
+"""
+import math
+
+import numpy as np
+import pytest
+
+import pned_b200 as P
+from oracle import oracle as O
+from pned_b200 import couplings as CP
+from pned_b200.lattice import honeycomb
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+KH = CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi))
+KHGH = CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi), gamma=0.1)
+FIELD = CP.field_111(0.05)
+
+
+def models(cl, q, tree, cpl, fld=None, tps_L=None):
+    X, skip, pt = P.build_xlocal(q, tree, cpl, field=fld)
+    if tps_L is not None:
+        X, _ = P.tps_transform(q, tree, cl.nbond, X, L=tps_L)
+    gm = P.Model(cl.n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt)
+    om = O.Model(cl.n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt)
+    return gm, om
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+HV_CASES = [
+    # (L1, L2, q, tree, couplings, field, R)
+    (2, 2, 2, 0, KH, None, 1),
+    (3, 2, 2, 0, KHGH, FIELD, 1),
+    (3, 2, 2, 0, KHGH, FIELD, 3),
+    (2, 4, 2, 0, KH, None, 4),
+    (2, 4, 2, 0, KHGH, FIELD, 12),
+    (3, 2, 2, 0, KH, None, 16),
+    (3, 2, 2, 1, KHGH, FIELD, 2),
+    (3, 1, 3, 1, CP.kitaev_heisenberg(0.2, -1.0), None, 1),
+    (3, 1, 3, 1, CP.kitaev_heisenberg(0.2, -1.0, gamma=0.1), FIELD, 4),
+    (2, 2, 3, 1, CP.kitaev_heisenberg(0.2, -1.0), None, 6),
+    (3, 1, 4, 1, CP.kitaev_heisenberg(0.5, 0.3, gamma=-0.2), FIELD, 8),
+]
+
+
+@pytest.mark.parametrize("case", HV_CASES, ids=[f"{c[0]}x{c[1]}q{c[2]}t{c[3]}R{c[6]}" for c in HV_CASES])
+def test_hv_parity(case):
+    L1, L2, q, tree, cpl, fld, R = case
+    cl = honeycomb(L1, L2)
+    gm, om = models(cl, q, tree, cpl, fld)
+    ctx = P.Context(gm, R=R)
+    rng = np.random.default_rng(17)
+    D = gm.dim
+    v1 = (rng.standard_normal((D, R)) + 1j * rng.standard_normal((D, R))).astype(np.complex128)
+    v0 = (0.2 * rng.standard_normal((D, R)) + 0.1j * rng.standard_normal((D, R))).astype(np.complex128)
+    eperbd = 0.0625
+    w = np.ascontiguousarray(v0).reshape(-1).copy()
+    pr = ctx.p_mltply_v3(np.ascontiguousarray(v1).reshape(-1), w, eperbd)
+    w = w.reshape(D, R)
+    for r in range(R):
+        ref = np.ascontiguousarray(v0[:, r]).copy()
+        prr = om.p_mltply_v3(np.ascontiguousarray(v1[:, r]), ref, eperbd)
+        assert rel(w[:, r], ref) <= 1e-12
+        assert abs(pr[r] - prr) <= 1e-12 * abs(prr)
+
+
+def test_hv_device_pointers_and_dots():
+    cl = honeycomb(2, 4)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    ctx = P.Context(gm, R=4)
+    rng = np.random.default_rng(3)
+    n = gm.dim * 4
+    a = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    pr = ctx.p_mltply_v3(ta, tb)
+    b2 = b.copy()
+    pr2 = ctx.p_mltply_v3(a, b2)
+    assert np.array_equal(pr, pr2)
+    assert np.array_equal(tb.cpu().numpy(), b2)
+    d = ctx.calc_vec_inprdct(a, b2)
+    for r in range(4):
+        ref = O.inprdct(np.ascontiguousarray(a.reshape(-1, 4)[:, r]), np.ascontiguousarray(b2.reshape(-1, 4)[:, r]))
+        assert abs(d[r] - ref) <= 1e-12 * abs(ref)
+    al = np.array([0.3 + 0.01j, -1.0, 2.0 - 0.5j, 0.0])
+    cb = ctx.calc_beta(al, a, b2)
+    for r in range(4):
+        x1 = a.reshape(-1, 4)[:, r]
+        x2 = b2.reshape(-1, 4)[:, r]
+        ref = np.sum(np.abs(x2 - al[r] * x1) ** 2)
+        assert abs(cb[r] - ref) <= 1e-12 * ref
+
+
+def test_gaussian_matches_oracle():
+    cl = honeycomb(2, 4)
+    gm, _ = models(cl, 2, 0, KH)
+    for R in (1, 3, 16):
+        ctx = P.Context(gm, R=R)
+        t = torch.empty(gm.dim * R, dtype=torch.complex128, device="cuda")
+        ctx.fill_gaussian(20261203, t, normalise=False)
+        ref = O.gaussian(20261203, gm.dim, R)
+        assert np.max(np.abs(t.cpu().numpy() - ref)) <= 1e-14
+        ctx.fill_gaussian(20261203, t, normalise=True)
+        nrm = np.linalg.norm(t.cpu().numpy().reshape(-1, R), axis=0)
+        assert np.allclose(nrm, 1.0, atol=1e-14)
+
+
+@pytest.mark.parametrize("L1,L2,q,tree,cpl,fld,steps", [
+    (3, 2, 2, 0, KH, None, 90),
+    (2, 4, 2, 0, KHGH, FIELD, 120),
+    (3, 1, 3, 1, CP.kitaev_heisenberg(0.2, -1.0), None, 80),
+])
+def test_lanczos_parity(L1, L2, q, tree, cpl, fld, steps):
+    cl = honeycomb(L1, L2)
+    gm, om = models(cl, q, tree, cpl, fld)
+    v = O.gaussian(7, gm.dim)
+    v /= np.linalg.norm(v)
+    ref = om.lanczos(v, steps)
+    ctx = P.Context(gm, R=1)
+    out = ctx.lanczos(v, steps)
+    assert out["itr"] == steps
+    assert abs(out["ene"][0] - ref["ene"][0]) <= 1e-10 * abs(ref["ene"][0])
+    k = 15
+    assert rel(out["alpha"][:k, 0], ref["alpha"][:k]) <= 1e-10
+    assert rel(out["beta"][:k, 0], ref["beta"][:k]) <= 1e-10
+
+
+def test_lanczos_batched_chains_are_independent():
+    cl = honeycomb(2, 4)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    R = 4
+    V = O.gaussian(11, gm.dim, R).reshape(gm.dim, R)
+    V /= np.linalg.norm(V, axis=0)
+    ctx = P.Context(gm, R=R)
+    out = ctx.lanczos(np.ascontiguousarray(V).reshape(-1), 40)
+    for r in range(R):
+        ref = om.lanczos(np.ascontiguousarray(V[:, r]), 40)
+        assert rel(out["alpha"][:12, r], ref["alpha"][:12]) <= 1e-10
+        e0 = P.bisec(out["alpha"][:, r], out["beta"][:, r], 40, 1)[0]
+        assert abs(e0 - ref["ene"][0]) <= 1e-10 * abs(ref["ene"][0])
+
+
+def test_lanczos_convergence_stop_matches_oracle():
+    cl = honeycomb(2, 2)
+    gm, om = models(cl, 2, 0, KH)
+    v = O.gaussian(11, gm.dim)
+    v /= np.linalg.norm(v)
+    ref = om.lanczos(v, 1024, check_conv=True)
+    out = P.Context(gm, R=1).lanczos(v, 1024, check_conv=True)
+    assert abs(out["ene"][0] - ref["ene"][0]) <= 1e-12 * abs(ref["ene"][0])
+    assert out["itr"] % 5 == 0 and out["itr"] < 1024
+
+
+@pytest.mark.parametrize("R", [1, 4])
+def test_tps_parity(R):
+    cl = honeycomb(2, 4)
+    L = 2.0 * cl.n
+    gm, om = models(cl, 2, 0, KHGH, FIELD, tps_L=L)
+    V = O.gaussian(5, gm.dim, R).reshape(gm.dim, R)
+    V /= np.linalg.norm(V, axis=0)
+    # observables as the reference evaluates them: z-bond SzSz (1-based ipair
+    # values as bit shifts) and S^zS^z(q), S^+S^-(q) at one momentum
+    zb = [(int(cl.ipair[2 * i]), int(cl.ipair[2 * i + 1])) for i in range(cl.nbond) if cl.ibond_type[i] == 3]
+    T_zz = np.array([[0.25, -0.25], [-0.25, 0.25]], dtype=complex)
+    qr = cl.qr(1)
+    T_pp = np.array([[0, 0.25], [0.25, 0]], dtype=complex)
+    obs = [
+        ([(a, b, 1.0) for a, b in zb], T_zz),
+        ([(j, 0, np.exp(1j * qr[j])) for j in range(cl.n)], T_zz),
+        ([(j, 0, np.exp(1j * qr[j])) for j in range(cl.n)], T_pp),
+    ]
+    specs = [P.ObservableSpec(a=np.array([t[0] for t in o[0]]), b=np.array([t[1] for t in o[0]]),
+                              c=np.array([t[2] for t in o[0]], dtype=complex), T=o[1]) for o in obs]
+    steps = 40
+    out = P.Context(gm, R=R).tps(L, np.ascontiguousarray(V).reshape(-1), steps, specs)
+    for r in range(R):
+        ref = om.tps(L, np.ascontiguousarray(V[:, r]), steps, obs)
+        assert rel(out["alpha"][:, r], ref["alpha"]) <= 1e-10
+        assert rel(out["beta"][:, r], ref["beta"]) <= 1e-10
+        for j in range(ref["coef"].shape[1]):
+            assert rel(out["coef"][:, r, j], ref["coef"][:, j]) <= 1e-10, j
+
+
+def test_dsf_parity():
+    cl = honeycomb(2, 4)
+    gm, om = models(cl, 2, 0, KH)
+    # ground state from the oracle's inverse iteration on a Lanczos E0
+    v = O.gaussian(3, gm.dim)
+    v /= np.linalg.norm(v)
+    e0 = om.lanczos(v, 120)["ene"][0]
+    b = O.gaussian(4, gm.dim)
+    b /= np.linalg.norm(b)
+    x, _, _ = om.inverse_iteration(e0 - 1e-9, b, inv_max=30)
+    R = 4
+    qrs = np.stack([cl.qr(i) for i in range(R)])
+    steps = 40
+    out = P.Context(gm, R=R).dsf(x, qrs, steps)
+    for r in range(R):
+        vq, cn = om.intalv_zz(qrs[r], x)
+        assert abs(out["cnorm"][r] - cn.real) <= 1e-12 * abs(cn)
+        sa, sb = om.dsf_chain(vq, cn, steps)
+        assert rel(out["salpha"][:20, r], sa[:20]) <= 1e-10
+        assert rel(out["sbeta"][:21, r], sb[:21]) <= 1e-10
+        # spectra from both chains through the (host) continued fraction
+        _, _, d1 = P.exec_renbun(400, steps + 2, 3.0 / 399, e0, 0.05, out["salpha"][:, r], out["sbeta"][:, r])
+        _, _, d2 = O.exec_renbun(400, steps + 2, 3.0 / 399, e0, 0.05, sa, sb)
+        assert rel(d1, d2) <= 1e-10
+
+
+def test_cg_inverse_iteration():
+    cl = honeycomb(2, 2)
+    gm, om = models(cl, 2, 0, KH)
+    v = O.gaussian(3, gm.dim)
+    v /= np.linalg.norm(v)
+    e0 = om.lanczos(v, 100)["ene"][0]
+    b = O.gaussian(8, gm.dim)
+    b /= np.linalg.norm(b)
+    ctx = P.Context(gm, R=1)
+    x, ni, nc = ctx.cg(e0 - 1e-9, b, inv_max=30, cg_max=500)
+    xr, _, _ = om.inverse_iteration(e0 - 1e-9, b, inv_max=30, cg_max=500)
+    assert abs(abs(np.vdot(xr, x)) - 1) < 1e-9
+    # residual of the eigenpair
+    hx = np.zeros_like(x)
+    om.p_mltply_v3(x, hx)
+    assert np.linalg.norm(hx - e0 * x) < 1e-6
+
+
+def test_larger_hv_parity_n24():
+    cl = honeycomb(3, 4)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    v1 = O.gaussian(1, gm.dim)
+    v0 = np.zeros(gm.dim, dtype=np.complex128)
+    w = v0.copy()
+    pr = P.Context(gm, R=1).p_mltply_v3(v1, w)
+    prr = om.p_mltply_v3(v1, v0)
+    assert rel(w, v0) <= 1e-12
+    assert abs(pr[0] - prr) <= 1e-12 * abs(prr)
