@@ -149,6 +149,27 @@ int pned_ctx_bytes(const pned_ctx *c, size_t *bytes);
  */
 int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double eperbd, pned_c128 *prdct, int ptr_flags);
 
+/*
+ * Allocation-free H.v (no counterpart in the reference): the same product as
+ * pned_hv on device vectors, v0 += (H - eperbd*n_bonds)^T v1 and
+ * prdct[r] = <v1_r|...>, without a context and without allocating device
+ * memory.  For callers that cannot call cudaMalloc: a host that hands all of
+ * its HBM to its own pool (or to the resident state vectors) and would see a
+ * hidden allocation fail or fragment that pool, or a thread that must not
+ * allocate at all.  The reduction scratch is a fixed device array inside the
+ * library (4096 complex values, 64 KB, held by every GPU that loads the
+ * library until exit); R may be 1, 2, 3, 4, 6, 8, 12 or 16, and anything else
+ * is rejected with PNED_EINVAL.  The first call on a device resolves the
+ * array's device address (set-up), so make that first call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU race and
+ * must be ordered by the caller (one stream, or events).  v1, v0 are device
+ * pointers ([dim][R]); prdct is host memory (may be NULL); stream is a
+ * cudaStream_t (NULL = default stream); the call returns after the stream has
+ * finished the product.
+ */
+int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1_dev, pned_c128 *v0_dev, double eperbd,
+                    pned_c128 *prdct, void *stream);
+
 /* calc_vec_inprdct (S1/2 parallel.f90:104-126): out[r] = sum conj(x1_r) x2_r. */
 int pned_inprdct(pned_ctx *c, const pned_c128 *x1, const pned_c128 *x2, pned_c128 *out, int ptr_flags);
 

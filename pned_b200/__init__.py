@@ -7,7 +7,7 @@ include/pned_gpu.h); this package is the Python host side over that ABI.
 from . import couplings, lattice  # noqa: F401
 from ._capi import PnedError, lib  # noqa: F401
 from .api import (Context, Model, ObservableSpec, bisec, build_xlocal, exec_renbun,  # noqa: F401
-                  mk_list12, normalize_dsf, tps_transform, vec12)
+                  hv_noalloc, mk_list12, normalize_dsf, tps_transform, vec12)
 
-__all__ = ["Context", "Model", "ObservableSpec", "PnedError", "bisec", "build_xlocal", "couplings", "exec_renbun",
+__all__ = ["Context", "Model", "ObservableSpec", "PnedError", "bisec", "build_xlocal", "couplings", "exec_renbun", "hv_noalloc",
            "lattice", "lib", "mk_list12", "normalize_dsf", "tps_transform", "vec12"]

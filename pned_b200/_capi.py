@@ -52,7 +52,7 @@ EXPORTS = [
     "pned_hv", "pned_inprdct", "pned_calc_beta", "pned_fill_gaussian", "pned_lanczos_run", "pned_tps_run",
     "pned_dsf_run", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
     "pned_session_begin", "pned_session_begin_dsf", "pned_session_step", "pned_session_read", "pned_session_vector",
-    "pned_session_end", "pned_session_profile",
+    "pned_session_end", "pned_session_profile", "pned_hv_noalloc",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
     L.pned_session_vector.argtypes = [vp, C.POINTER(vp), dp]
     L.pned_session_end.argtypes = [vp]
     L.pned_session_profile.argtypes = [vp, i32, dp, dp]
+    L.pned_hv_noalloc.argtypes = [vp, i32, vp, vp, dbl, vp, vp]
     _lib = L
     return L
 

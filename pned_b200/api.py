@@ -127,6 +127,23 @@ def normalize_dsf(i_range: int, split: float, sq_re: float, dsf):
 
 # --------------------------------------------------------------------------- model / context
 
+
+def hv_noalloc(model, R: int, v1, v0, eperbd: float = 0.0, stream=None):
+    """pned_hv_noalloc: v0 += (H - eperbd*ibond)^T v1 on CUDA tensors without
+    any device allocation by the library; returns prdct (R complex)."""
+    p1, f1 = _ptr(v1)
+    p0, f0 = _ptr(v0, writable=True)
+    if f1 != PTR_DEVICE or f0 != PTR_DEVICE:
+        raise TypeError("hv_noalloc takes CUDA tensors")
+    for v in (v1, v0):
+        if v.numel() != model.dim * R:
+            raise ValueError("vectors must have dim*R elements")
+    sp = None if stream is None else C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
+    pr = np.zeros(R, dtype=np.complex128)
+    check(lib().pned_hv_noalloc(model._h, int(R), p1, p0, float(eperbd), C.c_void_p(pr.ctypes.data), sp))
+    return pr
+
+
 class Model:
     """A compiled model on the current device (pned_model_create)."""
 

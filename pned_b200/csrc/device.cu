@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -728,4 +729,85 @@ extern "C" int pned_fill_gaussian(pned_ctx *c, uint64_t seed, int normalise, pne
     cudaError_t e = launch_gaussian(c, seed, normalise != 0, reinterpret_cast<double2 *>(v_dev), c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_fill_gaussian");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free H.v: reduction scratch in a fixed device array
+// ---------------------------------------------------------------------------
+namespace pned {
+
+// 4096 complex values (64 KB): [0, 16) holds 32 doubles set to 1 (scales),
+// [16, 32) the R totals, [32, 32 + nblocks*R) the per-block partial sums.
+constexpr int kNoAllocScratch = 4096;
+constexpr int kNoAllocHead = 32;
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratch];
+
+static std::mutex g_noalloc_mu;
+static double2 *g_noalloc_addr[64] = {};
+
+// Device address of g_noalloc_scratch on `device` (which must be current),
+// resolved once per device.
+static int noalloc_address(int device, double2 **out)
+{
+    if (device < 0 || device >= 64) return fail(PNED_EINVAL, "pned_hv_noalloc: device index above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "pned_hv_noalloc: cudaGetSymbolAddress");
+        g_noalloc_addr[device] = static_cast<double2 *>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return PNED_OK;
+}
+
+__global__ void noalloc_fill_ones(double *p, int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 1.0;
+}
+
+}  // namespace pned
+
+extern "C" int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1, pned_c128 *v0, double eperbd,
+                               pned_c128 *prdct, void *stream)
+{
+    if (!m || !v1 || !v0) return fail(PNED_EINVAL, "pned_hv_noalloc: null argument");
+    if (pick_vpt(R) == 0)
+        return fail(PNED_EINVAL, "pned_hv_noalloc: R = " + std::to_string(R) +
+                                     " is not one of 1, 2, 3, 4, 6, 8, 12, 16 (the 4096-value scratch limit)");
+    cudaError_t e = cudaSetDevice(m->device);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_hv_noalloc: cudaSetDevice");
+    double2 *scr = nullptr;
+    int rc = noalloc_address(m->device, &scr);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    const int64_t items = m->dim * (R / pick_vpt(R));
+    int64_t nb = std::min<int64_t>(int64_t(nsm) * 8, (items + kThreads - 1) / kThreads);
+    nb = std::min<int64_t>(nb, (kNoAllocScratch - kNoAllocHead) / R);
+    nb = std::max<int64_t>(1, nb);
+    double *ones = reinterpret_cast<double *>(scr);
+    double2 *sums = scr + 16;
+    double2 *partials = scr + kNoAllocHead;
+    noalloc_fill_ones<<<1, 32, 0, st>>>(ones, 2 * 16);
+    e = cudaGetLastError();
+    HvArgs a{};
+    a.C = reinterpret_cast<const double2 *>(v1);
+    a.P = reinterpret_cast<double2 *>(v0);
+    a.W = reinterpret_cast<double2 *>(v0);
+    a.sc = ones;
+    a.pc = ones;
+    a.diag = m->d_diag;
+    a.shift = eperbd * m->nbond;
+    a.table = m->d_table;
+    a.partials = partials;
+    a.dim = m->dim;
+    a.R = R;
+    a.K = 1;
+    if (e == cudaSuccess) e = launch_hv(m, a, int(nb), st);
+    if (e == cudaSuccess) e = launch_finish(partials, int(nb), R, sums, st);
+    if (e == cudaSuccess && prdct) e = cudaMemcpyAsync(prdct, sums, sizeof(double2) * R, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_hv_noalloc");
 }
