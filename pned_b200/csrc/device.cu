@@ -118,6 +118,135 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
     block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
 }
 
+// Tiled single-vector (R = 1) H.v on the S = 1/2 full basis.  A block owns a
+// tile of 256 * 2^JB states: thread t holds states t + 256 j (j < 2^JB), whose
+// global index is base | jexp[j].  The tile is staged in shared memory, so
+// flip masks inside the tile gather from shared memory; the others gather
+// through L1/L2 from the partner tile.  The term decode (coefficient index) is
+// done once per term for the thread's 2^JB states.
+template <int JB, bool RC, bool RD, int K>
+__global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
+{
+    constexpr int SPT = 1 << JB;
+    constexpr int TILE = kThreads * SPT;
+    extern __shared__ double2 smem[];
+    double2 *s_v = smem;
+    double2 *s_tab = smem + TILE;
+    for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
+    const uint32_t tid = threadIdx.x;
+    const int64_t ntiles = int64_t(1) << prog.nouter;
+    double2 red[K][1];
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k][0] = make_double2(0.0, 0.0);
+    const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint32_t base = tid;
+        for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
+        uint32_t s[SPT];
+        double2 v[SPT], acc[SPT];
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            s[j] = base | prog.jexp[j];
+            v[j] = __ldg(a.C + s[j]);
+        }
+        __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) s_v[tid + kThreads * j] = v[j];
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            if (!prog.first) {
+                acc[j] = make_double2(0.0, 0.0);
+            } else if (RD) {
+                const double dd = __ldcs(static_cast<const double *>(a.diag) + s[j]) - a.shift;
+                acc[j] = cscale(dd, v[j]);
+            } else {
+                double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + s[j]);
+                dd.x -= a.shift;
+                acc[j] = cmul(dd, v[j]);
+            }
+        }
+        __syncthreads();
+        // flip masks inside the tile: partners from shared memory
+        for (int t = 0; t < prog.nin; ++t) {
+            const TileTerm T = prog.t[t];
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            const double2 *sv = s_v + (tid ^ (T.mask & 0xffu));
+            const uint32_t mhi = T.mask >> 8;
+            if (!T.hasj) {
+                const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 w = sv[kThreads * (j ^ mhi)];
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
+                    const double2 w = sv[kThreads * (j ^ mhi)];
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+            }
+        }
+        // flip masks leaving the tile: partners through L1/L2
+        for (int t = prog.nin; t < prog.nterms; ++t) {
+            const TileTerm T = prog.t[t];
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            if (!T.hasj) {
+                const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 w = __ldg(a.C + (s[j] ^ T.mask));
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
+                    const double2 w = __ldg(a.C + (s[j] ^ T.mask));
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            const int64_t e = s[j];
+            const double2 hv = cscale(sc, acc[j]);
+            double2 out = hv;
+            if (!prog.first) {
+                const double2 w0 = __ldcs(a.W + e);
+                out.x += w0.x;
+                out.y += w0.y;
+            } else if (a.P) {
+                const double2 p = __ldcs(a.P + e);
+                out.x = fma(pc, p.x, out.x);
+                out.y = fma(pc, p.y, out.y);
+            }
+            __stcs(a.W + e, out);
+            const double2 vv = cscale(sc, v[j]);
+            red[0][0] = cadd(red[0][0], cconjmul(vv, hv));
+            if (!prog.last) continue;
+            if (K >= 2) red[1][0].x += out.x * out.x + out.y * out.y;
+            if (K >= 4 && a.G) {
+                const double2 gv = cscale(gs, a.G[e]);
+                red[2][0] = cadd(red[2][0], cconjmul(gv, out));
+                red[3][0] = cadd(red[3][0], cconjmul(gv, vv));
+            }
+        }
+    }
+    block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
+}
+
 // Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by
 // the two bond digits; zero coefficients (target digit out of range) skip the load.
 template <int VPT, bool RC, bool RD, int K>
@@ -320,14 +449,63 @@ int pick_vpt(int R)
     }
 }
 
+// Opts a kernel into more than 48 KB of dynamic shared memory, once per kernel
+// and device (static + dynamic above 48 KB fails to launch without it).
+static cudaError_t allow_dynamic_smem(const void *kern, int device)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, int>> done;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &d : done)
+        if (d.first == kern && d.second == device) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) done.push_back({kern, device});
+    return e;
+}
+
+static int tile_grid(const pned_model *m, int nblocks) { return std::max(1, std::min(nblocks, 2 * m->nsm)); }
+
+template <bool RC, bool RD, int K>
+static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    auto kern = hv_tile_kernel<3, RC, RD, K>;
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+    if (e != cudaSuccess) return e;
+    // persistent grid (two blocks per SM): the blocks in flight sweep consecutive
+    // tiles, so partner tiles on the fast outer bits are found in L2
+    const int grid = tile_grid(m, nblocks);
+    HvArgs b = a;
+    for (size_t p = 0; p < m->tprogs.size(); ++p) {
+        b.partials = a.partials + size_t(p) * grid * K * a.R;
+        kern<<<grid, kThreads, m->tile_smem, st>>>(*m->tprogs[p], b);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <int K>
+static cudaError_t launch_tile(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    if (m->real_coef && m->real_diag) return launch_tile_t<true, true, K>(m, a, nblocks, st);
+    if (m->real_diag) return launch_tile_t<false, true, K>(m, a, nblocks, st);
+    return launch_tile_t<false, false, K>(m, a, nblocks, st);
+}
+
 template <int VPT, bool RC, bool RD, int K>
 static cudaError_t launch_hv_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
     const size_t smem = sizeof(double2) * std::max(1, m->ntab);
     if (m->q == 2) {
-        hv_xor_kernel<VPT, RC, RD, K><<<nblocks, kThreads, smem, st>>>(*m->xprog, a);
+        auto kern = hv_xor_kernel<VPT, RC, RD, K>;
+        cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+        if (e != cudaSuccess) return e;
+        kern<<<nblocks, kThreads, smem, st>>>(*m->xprog, a);
     } else {
-        hv_radix_kernel<VPT, RC, RD, K><<<nblocks, kThreads, smem, st>>>(*m->rprog, a, m->q);
+        auto kern = hv_radix_kernel<VPT, RC, RD, K>;
+        cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+        if (e != cudaSuccess) return e;
+        kern<<<nblocks, kThreads, smem, st>>>(*m->rprog, a, m->q);
     }
     return cudaGetLastError();
 }
@@ -352,8 +530,18 @@ static cudaError_t launch_hv_k(const pned_model *m, const HvArgs &a, int nblocks
     }
 }
 
+int hv_partial_blocks(const pned_model *m, int R, int nblocks)
+{
+    if (!m->tprogs.empty() && R == 1 && m->use_tile) return int(m->tprogs.size()) * tile_grid(m, nblocks);
+    return nblocks;
+}
+
 cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
+    if (!m->tprogs.empty() && a.R == 1 && m->use_tile) {
+        if (a.K == 1) return launch_tile<1>(m, a, nblocks, st);
+        if (a.K == 4) return launch_tile<4>(m, a, nblocks, st);
+    }
     switch (a.K) {
     case 1: return launch_hv_k<1>(m, a, nblocks, st);
     case 4: return launch_hv_k<4>(m, a, nblocks, st);
@@ -451,6 +639,37 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
         m->rprog->n = hp.n;
         std::copy(hp.rterms.begin(), hp.rterms.end(), m->rprog->t);
         m->nterms = m->rprog->nterms;
+    }
+    // tiled single-vector program (S = 1/2, n >= 12), one launch per pass
+    {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g_device);
+        m->nsm = nsm;
+    }
+    if (hp.q == 2 && hp.n >= 12 && plan_tiles(m->hp, 3, kTileWindowBits, kTileMaxPasses) == PNED_OK) {
+        const HostProgram &h2 = m->hp;
+        for (size_t p = 0; p < h2.passes.size(); ++p) {
+            const HostProgram::TilePass &ps = h2.passes[p];
+            std::unique_ptr<TileProgram> T(new TileProgram());
+            T->n = h2.n;
+            T->jb = ps.jb;
+            T->nin = ps.nin;
+            T->nterms = int(ps.tterms.size());
+            T->ntab = m->ntab;
+            T->nouter = int(ps.outer.size());
+            T->first = p == 0;
+            T->last = p + 1 == h2.passes.size();
+            for (int j = 0; j < (1 << ps.jb); ++j) {
+                uint32_t e = 0;
+                for (int k = 0; k < ps.jb; ++k) if ((j >> k) & 1) e |= 1u << ps.jpos[k];
+                T->jexp[j] = e;
+            }
+            for (int k = 0; k < T->nouter; ++k) T->outer[k] = uint8_t(ps.outer[k]);
+            std::copy(ps.tterms.begin(), ps.tterms.end(), T->t);
+            m->tprogs.push_back(std::move(T));
+        }
+        m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << 3) + std::max(1, m->ntab));
+        m->use_tile = true;
     }
     // coefficient table
     std::vector<double2> tab(std::max<size_t>(1, hp.table.size()));
@@ -674,7 +893,8 @@ extern "C" int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double e
     a.table = c->m->d_table; a.partials = c->partials;
     a.dim = c->m->dim; a.R = c->R; a.K = 1;
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
-    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, c->R, c->sums, c->stream);
+    if (e == cudaSuccess)
+        e = launch_finish(c->partials, hv_partial_blocks(c->m, c->R, c->nblocks), c->R, c->sums, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pned_hv launch");
     if (!(flags & PNED_PTR_DEVICE)) {
         e = cudaMemcpyAsync(v0, dv0, sizeof(double2) * size_t(c->m->dim) * c->R, cudaMemcpyDeviceToHost, c->stream);
@@ -787,6 +1007,7 @@ extern "C" int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1, 
     int64_t nb = std::min<int64_t>(int64_t(nsm) * 8, (items + kThreads - 1) / kThreads);
     nb = std::min<int64_t>(nb, (kNoAllocScratch - kNoAllocHead) / R);
     nb = std::max<int64_t>(1, nb);
+    while (nb > 1 && int64_t(hv_partial_blocks(m, R, int(nb))) * R > kNoAllocScratch - kNoAllocHead) --nb;
     double *ones = reinterpret_cast<double *>(scr);
     double2 *sums = scr + 16;
     double2 *partials = scr + kNoAllocHead;
@@ -806,7 +1027,7 @@ extern "C" int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1, 
     a.R = R;
     a.K = 1;
     if (e == cudaSuccess) e = launch_hv(m, a, int(nb), st);
-    if (e == cudaSuccess) e = launch_finish(partials, int(nb), R, sums, st);
+    if (e == cudaSuccess) e = launch_finish(partials, hv_partial_blocks(m, R, int(nb)), R, sums, st);
     if (e == cudaSuccess && prdct) e = cudaMemcpyAsync(prdct, sums, sizeof(double2) * R, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_hv_noalloc");

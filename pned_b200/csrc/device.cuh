@@ -17,6 +17,10 @@ struct pned_model {
     int ntab = 0, nterms = 0;
     std::unique_ptr<pned::XorProgram> xprog;
     std::unique_ptr<pned::RadixProgram> rprog;
+    std::vector<std::unique_ptr<pned::TileProgram>> tprogs;   // tiled single-vector passes (q == 2)
+    size_t tile_smem = 0;
+    bool use_tile = false;   // single-vector H.v uses the tiled kernel
+    int nsm = 148;
     double2 *d_table = nullptr;
     void *d_diag = nullptr;
 };
@@ -86,6 +90,8 @@ int pick_vpt(int R);
 void session_release(pned_ctx *c);
 
 cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
+// Number of partial-sum blocks launch_hv writes for this model, R and grid.
+int hv_partial_blocks(const pned_model *m, int R, int nblocks);
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);
 cudaError_t launch_dot(const pned_ctx *c, const double2 *x1, const double2 *x2, const double2 *alpha, int mode,
                        double2 *out, cudaStream_t st);

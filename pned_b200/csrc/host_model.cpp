@@ -413,6 +413,125 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
     return PNED_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Tile planner for the single-vector S = 1/2 kernel
+// ---------------------------------------------------------------------------
+namespace {
+
+// Tile j-bits (greedy: most masks made in-tile) and outer order (bits most used
+// by out-of-tile masks first) for a set of masks.
+void choose_tile(const std::vector<uint32_t> &masks, int n, int jb, std::vector<int> &jpos, std::vector<int> &outer,
+                 uint32_t &tilemask)
+{
+    tilemask = 0xffu;
+    jpos.clear();
+    for (int k = 0; k < jb; ++k) {
+        int best = -1, bestc = -1;
+        for (int b = 8; b < n; ++b) {
+            if (tilemask & (1u << b)) continue;
+            const uint32_t tm = tilemask | (1u << b);
+            int cnt = 0, use = 0;
+            for (uint32_t m : masks) {
+                if ((m & ~tm) == 0) ++cnt;
+                if (m & (1u << b)) ++use;
+            }
+            const int score = cnt * 64 + use;
+            if (score > bestc) { bestc = score; best = b; }
+        }
+        jpos.push_back(best);
+        tilemask |= 1u << best;
+    }
+    std::sort(jpos.begin(), jpos.end());
+    std::vector<std::pair<int, int>> ob;
+    for (int b = 8; b < n; ++b) {
+        if (tilemask & (1u << b)) continue;
+        int use = 0;
+        for (uint32_t m : masks) if ((m & ~tilemask) && (m & (1u << b))) ++use;
+        ob.push_back({-use, b});
+    }
+    std::sort(ob.begin(), ob.end());
+    outer.clear();
+    for (auto &x : ob) outer.push_back(x.second);
+}
+
+}  // namespace
+
+int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
+{
+    if (P.q != 2 || jb < 1 || jb > kTileMaxJB || P.n < 8 + jb + 1) return PNED_ENOTSUP;
+    const int n = P.n;
+    std::vector<int> remaining(P.xterms.size());
+    for (size_t i = 0; i < remaining.size(); ++i) remaining[i] = int(i);
+    P.passes.clear();
+    while (!remaining.empty()) {
+        std::vector<uint32_t> rm;
+        for (int i : remaining) rm.push_back(P.xterms[i].xmask);
+        std::vector<int> jpos, outer;
+        uint32_t tilemask;
+        choose_tile(rm, n, jb, jpos, outer, tilemask);
+        uint32_t nearmask = tilemask;
+        for (int k = 0; k < window_bits && k < int(outer.size()); ++k) nearmask |= 1u << outer[k];
+        std::vector<int> take, rest;
+        const bool last = int(P.passes.size()) + 1 >= max_passes;
+        for (int i : remaining) {
+            if (last || (P.xterms[i].xmask & ~nearmask) == 0) take.push_back(i);
+            else rest.push_back(i);
+        }
+        if (take.empty()) { take = rest; rest.clear(); }
+        // re-plan the tile for the masks of this pass only
+        std::vector<uint32_t> tm;
+        for (int i : take) tm.push_back(P.xterms[i].xmask);
+        choose_tile(tm, n, jb, jpos, outer, tilemask);
+        HostProgram::TilePass pass;
+        pass.jb = jb;
+        for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
+        pass.outer = outer;
+        auto local = [&](uint32_t m) {
+            uint32_t l = m & 0xffu;
+            for (int k = 0; k < jb; ++k) if (m & (1u << jpos[k])) l |= 1u << (8 + k);
+            return l;
+        };
+        std::vector<TileTerm> in, out;
+        for (int i : take) {
+            const XorTerm &t = P.xterms[i];
+            TileTerm q{};
+            q.pos4 = t.pos4;
+            q.tab = t.tab;
+            q.nb = t.nb;
+            for (int j = 0; j < (1 << jb); ++j) {
+                uint32_t bits = 0;
+                for (int d = 0; d < t.nb; ++d) {
+                    const int pos = (t.pos4 >> (8 * d)) & 0xff;
+                    for (int k = 0; k < jb; ++k) {
+                        if (pos != jpos[k]) continue;
+                        q.hasj = 1;
+                        if ((j >> k) & 1) bits |= 1u << d;
+                    }
+                }
+                q.jtab |= bits << (4 * j);
+            }
+            if ((t.xmask & ~tilemask) == 0) { q.mask = local(t.xmask); in.push_back(q); }
+            else { q.mask = t.xmask; out.push_back(q); }
+        }
+        pass.nin = int(in.size());
+        pass.tterms = in;
+        pass.tterms.insert(pass.tterms.end(), out.begin(), out.end());
+        P.passes.push_back(pass);
+        remaining = rest;
+    }
+    if (P.passes.empty()) {   // diagonal-only model: one pass with no terms
+        HostProgram::TilePass pass;
+        pass.jb = jb;
+        std::vector<int> jpos, outer;
+        uint32_t tilemask;
+        choose_tile({}, n, jb, jpos, outer, tilemask);
+        for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
+        pass.outer = outer;
+        P.passes.push_back(pass);
+    }
+    return PNED_OK;
+}
+
 }  // namespace pned
 
 // ---------------------------------------------------------------------------

@@ -50,6 +50,15 @@ struct RadixProgram {
     RadixTerm t[kMaxTerms];
 };
 
+// Tiled single-vector S = 1/2 program (see TileTerm).
+struct TileProgram {
+    int n, jb, nin, nterms, ntab, nouter;
+    int first, last;                  // pass flags: first adds diagonal and P, last forms the K >= 2 sums
+    uint32_t jexp[1 << kTileMaxJB];   // global bits of the thread's j-th state
+    uint8_t outer[32];                // tile-id bit k -> global bit outer[k]
+    TileTerm t[kMaxTerms];
+};
+
 // Per-call scalars: W = pc_r * P + sc_r * (H - shift) (sc_r * C); all from device memory.
 struct HvArgs {
     const double2 *C;       // input vectors (scaled by sc)

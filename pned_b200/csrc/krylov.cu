@@ -209,7 +209,7 @@ static cudaError_t lanczos_step(pned_ctx *c, Session &S, bool first)
     if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
-    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, sa, c->stream);
+    if (e == cudaSuccess) e = launch_finish(c->partials, hv_partial_blocks(c->m, R, c->nblocks), R, sa, c->stream);
     if (e == cudaSuccess)
         e = launch_residual(c, c->buf[S.b2], c->buf[S.b0], c->buf[S.b1], slot(c, kSlotSc), sa, c->stream);
     if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, sb, c->stream);
@@ -238,7 +238,8 @@ static cudaError_t tps_step(pned_ctx *c, Session &S, bool first)
     if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
-    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, 4 * R, c->sums, c->stream);
+    if (e == cudaSuccess)
+        e = launch_finish(c->partials, hv_partial_blocks(c->m, R, c->nblocks), 4 * R, c->sums, c->stream);
     if (first && e == cudaSuccess) e = cudaMemsetAsync(c->sums + 2 * R, 0, sizeof(double2) * 2 * R, c->stream);
     for (int o = 0; o < S.nobs && e == cudaSuccess; ++o) {
         const DevObs &ob = S.obs[o];

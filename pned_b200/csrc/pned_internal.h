@@ -45,6 +45,22 @@ struct RadixTerm {
     uint32_t pad;
 };
 
+// Tiled S = 1/2 program (single vector): a tile is 2^(8+JB) states -- global
+// bits 0..7 (one per thread of a 256-thread block) times the JB "j-bits" at
+// global positions jpos (each thread owns 2^JB states) -- and the remaining
+// "outer" bits enumerate tiles, outer[0] varying fastest.
+struct TileTerm {
+    uint32_t mask;   // in-tile: local xor (bits 0..7 thread part, bits 8.. j part); out-of-tile: global xor
+    uint32_t pos4;   // dependency bit positions (global), 8 bits each
+    uint32_t jtab;   // coefficient-index bits contributed by j (4 bits per j)
+    uint16_t tab;    // coefficient table offset
+    uint8_t nb;      // number of dependency bits
+    uint8_t hasj;    // 1 if a dependency bit is a j-bit
+};
+constexpr int kTileMaxJB = 3;
+constexpr int kTileWindowBits = 10;   // outer bits whose partner tiles stay in L2 during a sweep
+constexpr int kTileMaxPasses = 4;
+
 struct HostProgram {
     int n = 0, q = 2;
     int64_t dim = 0;
@@ -56,7 +72,22 @@ struct HostProgram {
     // diagonal: per bond (s1, s2) and q*q diagonal values (pair state st)
     std::vector<int> dsite1, dsite2;
     std::vector<cd> dtab;                // [nbond][Q]
+    // tiled program (q == 2): one or more passes, each with its own tile plan
+    struct TilePass {
+        int jb = 0;
+        int jpos[kTileMaxJB] = {0, 0, 0};
+        std::vector<int> outer;          // outer bit positions, fastest first
+        int nin = 0;                     // in-tile terms first, then out-of-tile terms
+        std::vector<TileTerm> tterms;
+    };
+    std::vector<TilePass> passes;
 };
+
+// Splits the flip masks into passes for the tiled kernel (q == 2,
+// n >= 8 + jb + 1): each pass takes the masks whose partner tiles lie within
+// `window_bits` outer bits of its own tile order (so they are found in L2),
+// the last pass takes what is left.
+int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes);
 
 // Builds the program from a model description (bond order, skip mask and
 // element order follow make_cpu_list2; see model.cpp).
