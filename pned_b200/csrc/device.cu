@@ -118,12 +118,14 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
     block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
 }
 
-// Tiled single-vector (R = 1) H.v on the S = 1/2 full basis.  A block owns a
-// tile of 256 * 2^JB states: thread t holds states t + 256 j (j < 2^JB), whose
-// global index is base | jexp[j].  The tile is staged in shared memory, so
-// flip masks inside the tile gather from shared memory; the others gather
-// through L1/L2 from the partner tile.  The term decode (coefficient index) is
-// done once per term for the thread's 2^JB states.
+// Tiled single-vector (R = 1) H.v on the S = 1/2 full basis, one pass of a
+// multi-pass program (each pass owns a subset of the flip masks).  A block owns
+// a tile of 256 * 2^JB states: thread t holds states t + 256 j (j < 2^JB),
+// whose global index is base | jexp[j].  The tile is staged in shared memory,
+// so flip masks inside the tile gather from shared memory; the others gather
+// through L1/L2 from the partner tile, two terms at a time so that 2 * 2^JB
+// loads per thread are in flight.  The term decode (coefficient index) is done
+// once per term for the thread's 2^JB states.
 template <int JB, bool RC, bool RD, int K>
 __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
 {
@@ -142,27 +144,27 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         uint32_t base = tid;
         for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
-        uint32_t s[SPT];
-        double2 v[SPT], acc[SPT];
+        double2 acc[SPT];
+        {
+            double2 v[SPT];
 #pragma unroll
-        for (int j = 0; j < SPT; ++j) {
-            s[j] = base | prog.jexp[j];
-            v[j] = __ldg(a.C + s[j]);
-        }
-        __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+            for (int j = 0; j < SPT; ++j) v[j] = __ldg(a.C + (base | prog.jexp[j]));
+            __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
 #pragma unroll
-        for (int j = 0; j < SPT; ++j) s_v[tid + kThreads * j] = v[j];
+            for (int j = 0; j < SPT; ++j) s_v[tid + kThreads * j] = v[j];
 #pragma unroll
-        for (int j = 0; j < SPT; ++j) {
-            if (!prog.first) {
-                acc[j] = make_double2(0.0, 0.0);
-            } else if (RD) {
-                const double dd = __ldcs(static_cast<const double *>(a.diag) + s[j]) - a.shift;
-                acc[j] = cscale(dd, v[j]);
-            } else {
-                double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + s[j]);
-                dd.x -= a.shift;
-                acc[j] = cmul(dd, v[j]);
+            for (int j = 0; j < SPT; ++j) {
+                const uint32_t sj = base | prog.jexp[j];
+                if (!prog.first) {
+                    acc[j] = make_double2(0.0, 0.0);
+                } else if (RD) {
+                    const double dd = __ldcs(static_cast<const double *>(a.diag) + sj) - a.shift;
+                    acc[j] = cscale(dd, v[j]);
+                } else {
+                    double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + sj);
+                    dd.x -= a.shift;
+                    acc[j] = cmul(dd, v[j]);
+                }
             }
         }
         __syncthreads();
@@ -175,52 +177,34 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
                 if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
             const double2 *sv = s_v + (tid ^ (T.mask & 0xffu));
             const uint32_t mhi = T.mask >> 8;
-            if (!T.hasj) {
-                const double2 c = s_tab[T.tab + ib];
 #pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    const double2 w = sv[kThreads * (j ^ mhi)];
-                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                    else acc[j] = cfma(c, w, acc[j]);
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
-                    const double2 w = sv[kThreads * (j ^ mhi)];
-                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                    else acc[j] = cfma(c, w, acc[j]);
-                }
+            for (int j = 0; j < SPT; ++j) {
+                const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
+                const double2 w = sv[kThreads * (j ^ mhi)];
+                if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                else acc[j] = cfma(c, w, acc[j]);
             }
         }
         // flip masks leaving the tile: partners through L1/L2
         for (int t = prog.nin; t < prog.nterms; ++t) {
             const TileTerm T = prog.t[t];
+            double2 w0[SPT];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + ((base | prog.jexp[j]) ^ T.mask));
             uint32_t ib = 0;
 #pragma unroll
             for (int d = 0; d < kMaxDeps; ++d)
                 if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
-            if (!T.hasj) {
-                const double2 c = s_tab[T.tab + ib];
 #pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    const double2 w = __ldg(a.C + (s[j] ^ T.mask));
-                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                    else acc[j] = cfma(c, w, acc[j]);
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
-                    const double2 w = __ldg(a.C + (s[j] ^ T.mask));
-                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                    else acc[j] = cfma(c, w, acc[j]);
-                }
+            for (int j = 0; j < SPT; ++j) {
+                const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
+                if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
+                else acc[j] = cfma(c, w0[j], acc[j]);
             }
         }
 #pragma unroll
         for (int j = 0; j < SPT; ++j) {
-            const int64_t e = s[j];
+            const int64_t e = base | prog.jexp[j];
             const double2 hv = cscale(sc, acc[j]);
             double2 out = hv;
             if (!prog.first) {
@@ -233,7 +217,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
                 out.y = fma(pc, p.y, out.y);
             }
             __stcs(a.W + e, out);
-            const double2 vv = cscale(sc, v[j]);
+            const double2 vv = cscale(sc, s_v[tid + kThreads * j]);
             red[0][0] = cadd(red[0][0], cconjmul(vv, hv));
             if (!prog.last) continue;
             if (K >= 2) red[1][0].x += out.x * out.x + out.y * out.y;
@@ -665,6 +649,9 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
                 T->jexp[j] = e;
             }
             for (int k = 0; k < T->nouter; ++k) T->outer[k] = uint8_t(ps.outer[k]);
+            T->ngroups = int(ps.gxor.size());
+            for (int g = 0; g <= T->ngroups; ++g) T->gstart[g] = uint16_t(ps.gstart[g]);
+            for (int g = 0; g < T->ngroups; ++g) T->gxor[g] = ps.gxor[g];
             std::copy(ps.tterms.begin(), ps.tterms.end(), T->t);
             m->tprogs.push_back(std::move(T));
         }
@@ -774,6 +761,8 @@ extern "C" int pned_ctx_create(pned_model *m, int R, size_t budget, pned_ctx **o
     if (e == cudaSuccess) e = cudaMalloc(&c->sums, sizeof(double2) * kMaxK * kMaxR * 4);
     if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(double) * kScalSlots * kMaxR);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_sums, sizeof(double2) * kMaxK * kMaxR * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&c->flag, sizeof(int) * 4);
+    if (e == cudaSuccess) e = cudaMemset(c->flag, 0, sizeof(int) * 4);
     if (e != cudaSuccess) {
         pned_ctx_destroy(c.release());
         return cuda_fail(e, "pned_ctx_create: scratch");
@@ -857,7 +846,23 @@ int sums_to_host(pned_ctx *c, int KR)
 {
     cudaError_t e = cudaMemcpyAsync(c->h_sums, c->sums, sizeof(double2) * KR, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "reading reduction results");
+    if (e != cudaSuccess) return cuda_fail(e, "reading reduction results");
+    return check_kernel_flag(c);
+}
+
+// PNED_ETIMEOUT (and the flag cleared) if a kernel's bounded wait gave up.
+int check_kernel_flag(pned_ctx *c)
+{
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "reading the kernel error flag");
+    if (h) {
+        cudaMemsetAsync(c->flag, 0, sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
+        return fail(PNED_ETIMEOUT, "a kernel's bounded wait for a TMA copy gave up");
+    }
+    return PNED_OK;
 }
 
 // scal slot pointer
@@ -892,6 +897,7 @@ extern "C" int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double e
     a.diag = c->m->d_diag; a.shift = eperbd * c->m->nbond;
     a.table = c->m->d_table; a.partials = c->partials;
     a.dim = c->m->dim; a.R = c->R; a.K = 1;
+    a.err = c->flag;
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (e == cudaSuccess)
         e = launch_finish(c->partials, hv_partial_blocks(c->m, c->R, c->nblocks), c->R, c->sums, c->stream);
@@ -957,9 +963,10 @@ extern "C" int pned_fill_gaussian(pned_ctx *c, uint64_t seed, int normalise, pne
 namespace pned {
 
 // 4096 complex values (64 KB): [0, 16) holds 32 doubles set to 1 (scales),
-// [16, 32) the R totals, [32, 32 + nblocks*R) the per-block partial sums.
+// [16, 32) the R totals, [32] a kernel error flag, [33, 33 + blocks*R) the
+// per-block partial sums.
 constexpr int kNoAllocScratch = 4096;
-constexpr int kNoAllocHead = 32;
+constexpr int kNoAllocHead = 33;
 static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratch];
 
 static std::mutex g_noalloc_mu;
@@ -981,9 +988,10 @@ static int noalloc_address(int device, double2 **out)
     return PNED_OK;
 }
 
-__global__ void noalloc_fill_ones(double *p, int n)
+__global__ void noalloc_fill_ones(double *p, int n, int *err)
 {
     for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = 1.0;
+    if (threadIdx.x == 0) *err = 0;
 }
 
 }  // namespace pned
@@ -1011,7 +1019,8 @@ extern "C" int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1, 
     double *ones = reinterpret_cast<double *>(scr);
     double2 *sums = scr + 16;
     double2 *partials = scr + kNoAllocHead;
-    noalloc_fill_ones<<<1, 32, 0, st>>>(ones, 2 * 16);
+    int *err = reinterpret_cast<int *>(scr + 32);
+    noalloc_fill_ones<<<1, 32, 0, st>>>(ones, 2 * 16, err);
     e = cudaGetLastError();
     HvArgs a{};
     a.C = reinterpret_cast<const double2 *>(v1);
@@ -1026,9 +1035,14 @@ extern "C" int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1, 
     a.dim = m->dim;
     a.R = R;
     a.K = 1;
+    a.err = err;
     if (e == cudaSuccess) e = launch_hv(m, a, int(nb), st);
     if (e == cudaSuccess) e = launch_finish(partials, hv_partial_blocks(m, R, int(nb)), R, sums, st);
     if (e == cudaSuccess && prdct) e = cudaMemcpyAsync(prdct, sums, sizeof(double2) * R, cudaMemcpyDeviceToHost, st);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_hv_noalloc");
+    if (e != cudaSuccess) return cuda_fail(e, "pned_hv_noalloc");
+    if (herr) return fail(PNED_ETIMEOUT, "pned_hv_noalloc: a bounded wait for a TMA copy gave up");
+    return PNED_OK;
 }

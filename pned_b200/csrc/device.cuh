@@ -84,6 +84,7 @@ int cuda_fail(cudaError_t e, const char *what);
 int ctx_alloc_buffer(pned_ctx *c, int k);
 int stage_in(pned_ctx *c, const pned_c128 *src, int flags, int k, const double2 **dev);
 int sums_to_host(pned_ctx *c, int KR);
+int check_kernel_flag(pned_ctx *c);
 double *slot(pned_ctx *c, int s);
 int set_slot(pned_ctx *c, int s, double value);
 int pick_vpt(int R);

@@ -491,7 +491,8 @@ int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
             for (int k = 0; k < jb; ++k) if (m & (1u << jpos[k])) l |= 1u << (8 + k);
             return l;
         };
-        std::vector<TileTerm> in, out;
+        std::vector<TileTerm> in;
+        std::vector<std::pair<uint32_t, TileTerm>> out;   // (partner-tile xor, term)
         for (int i : take) {
             const XorTerm &t = P.xterms[i];
             TileTerm q{};
@@ -510,12 +511,30 @@ int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
                 }
                 q.jtab |= bits << (4 * j);
             }
-            if ((t.xmask & ~tilemask) == 0) { q.mask = local(t.xmask); in.push_back(q); }
-            else { q.mask = t.xmask; out.push_back(q); }
+            // in-tile terms: the local xor inside the tile; out-of-tile terms: the global xor
+            if ((t.xmask & ~tilemask) == 0) {
+                q.mask = local(t.xmask);
+                in.push_back(q);
+            } else {
+                q.mask = t.xmask;
+                out.push_back({t.xmask & ~tilemask, q});
+            }
         }
+        std::stable_sort(out.begin(), out.end(),
+                         [](const std::pair<uint32_t, TileTerm> &a, const std::pair<uint32_t, TileTerm> &b) {
+                             return a.first < b.first;
+                         });
         pass.nin = int(in.size());
         pass.tterms = in;
-        pass.tterms.insert(pass.tterms.end(), out.begin(), out.end());
+        for (size_t k = 0; k < out.size(); ++k) {
+            if (k == 0 || out[k].first != out[k - 1].first) {
+                pass.gstart.push_back(int(pass.tterms.size()));
+                pass.gxor.push_back(out[k].first);
+            }
+            pass.tterms.push_back(out[k].second);
+        }
+        pass.gstart.push_back(int(pass.tterms.size()));
+        if (int(pass.gxor.size()) > kTileMaxGroups) return PNED_ENOTSUP;
         P.passes.push_back(pass);
         remaining = rest;
     }
@@ -527,6 +546,7 @@ int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
         choose_tile({}, n, jb, jpos, outer, tilemask);
         for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
         pass.outer = outer;
+        pass.gstart.push_back(0);
         P.passes.push_back(pass);
     }
     return PNED_OK;

@@ -56,6 +56,9 @@ struct TileProgram {
     int first, last;                  // pass flags: first adds diagonal and P, last forms the K >= 2 sums
     uint32_t jexp[1 << kTileMaxJB];   // global bits of the thread's j-th state
     uint8_t outer[32];                // tile-id bit k -> global bit outer[k]
+    int ngroups;                      // out-of-tile groups, one partner tile each
+    uint16_t gstart[kTileMaxGroups + 1];
+    uint32_t gxor[kTileMaxGroups];
     TileTerm t[kMaxTerms];
 };
 
@@ -75,6 +78,7 @@ struct HvArgs {
     int64_t dim;
     int R;
     int K;                  // 1: alpha; 2: alpha, ||W||^2; 4: + <G|W>, <G|C>
+    int *err;               // set to 1 by a kernel whose bounded wait gave up (may be null)
 };
 
 }  // namespace pned

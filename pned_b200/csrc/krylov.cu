@@ -205,6 +205,7 @@ static cudaError_t lanczos_step(pned_ctx *c, Session &S, bool first)
     a.dim = c->m->dim;
     a.R = R;
     a.K = 1;
+    a.err = c->flag;
     double2 *sa = c->sums, *sb = c->sums + kMaxK * kMaxR;
     if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
@@ -235,6 +236,7 @@ static cudaError_t tps_step(pned_ctx *c, Session &S, bool first)
     a.table = c->m->d_table; a.partials = c->partials;
     a.G = first ? nullptr : c->buf[S.b2]; a.gsc = slot(c, kSlotGsc);
     a.dim = c->m->dim; a.R = R; a.K = 4;
+    a.err = c->flag;
     if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
@@ -478,6 +480,8 @@ extern "C" int pned_session_read(pned_ctx *c, double *alpha, double *beta, doubl
     if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, S.d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pned_session_read");
+    const int kf = check_kernel_flag(c);
+    if (kf) return kf;
     if (steps_done) *steps_done = k;
     if (status_out) *status_out = flag;
     return PNED_OK;
@@ -666,6 +670,7 @@ extern "C" int pned_cg_run(pned_ctx *c, double E, const pned_c128 *b_init, int i
             a.shift = (E / double(c->m->nbond)) * double(c->m->nbond);
             a.table = c->m->d_table; a.partials = c->partials;
             a.dim = n; a.R = 1; a.K = 1;
+            a.err = c->flag;
             e = launch_hv(c->m, a, nb, c->stream);
             if (e != cudaSuccess) return cuda_fail(e, "cg hv");
             double2 crp, cyp, rc1, rc2;

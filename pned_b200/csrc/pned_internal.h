@@ -60,6 +60,7 @@ struct TileTerm {
 constexpr int kTileMaxJB = 3;
 constexpr int kTileWindowBits = 10;   // outer bits whose partner tiles stay in L2 during a sweep
 constexpr int kTileMaxPasses = 4;
+constexpr int kTileMaxGroups = 64;    // partner tiles per pass
 
 struct HostProgram {
     int n = 0, q = 2;
@@ -77,8 +78,10 @@ struct HostProgram {
         int jb = 0;
         int jpos[kTileMaxJB] = {0, 0, 0};
         std::vector<int> outer;          // outer bit positions, fastest first
-        int nin = 0;                     // in-tile terms first, then out-of-tile terms
+        int nin = 0;                     // in-tile terms first, then out-of-tile terms grouped by partner tile
         std::vector<TileTerm> tterms;
+        std::vector<int> gstart;         // out-of-tile group g: terms gstart[g] .. gstart[g+1]-1
+        std::vector<uint32_t> gxor;      // partner tile of group g: outer bits flipped by gxor[g]
     };
     std::vector<TilePass> passes;
 };
