@@ -285,6 +285,75 @@ int pned_session_end(pned_ctx *c);
 int pned_session_profile(pned_ctx *c, int n_steps, double *hv_ms, double *step_ms);
 
 /* ------------------------------------------------------------------------ */
+/* slot batches: continuous batching of chains with different couplings      */
+/* ------------------------------------------------------------------------ */
+/*
+ * No counterpart in the reference, whose solvers run one chain per process;
+ * each slot runs the reference's own recurrences:
+ *   PNED_SLOT_LANCZOS  parallelized_lnc1z (S1/2 Lanczos.f90:48-163); also the
+ *                      DSF momentum chains (parallelized_dsflnc1z, S1/2
+ *                      DSF.f90:195-261) when loaded by pned_slots_load_szq
+ *   PNED_SLOT_TPS      parallelized_TPSz with L - H (S1/2 TPS.f90:325-409),
+ *                      coefficients as eval_phys_val (S1/2 TPS.f90:83-111)
+ *   PNED_SLOT_VECTOR   parallelized_lncv1z (S1/2 Lanczos.f90:183-329): replays
+ *                      a chain with its stored alpha/beta, x = sum_k c_k v_k
+ * A batch holds R slots (R one of 1, 2, 3, 4, 6, 8, 12, 16) over one S = 1/2
+ * lattice, fixed at creation by `structure` (sites, bonds, tree; its
+ * couplings only fix which spin flips exist, so give it generic non-zero
+ * local matrices).  Each slot carries its own couplings (same lattice,
+ * real diagonal).  Vectors are the columns of interleaved [dim][R] buffers;
+ * all slots advance together, one batched H.V per step, and slots are loaded
+ * and released between steps while the others keep running.  Start vectors
+ * are normalised on load.  Device memory: 16 dim R (3 vectors) + 8 dim R
+ * (diagonals); hbm_budget (0: none) bounds it (PNED_EBUDGET).
+ */
+typedef struct pned_slots pned_slots;
+#define PNED_SLOT_FREE 0
+#define PNED_SLOT_LANCZOS 1
+#define PNED_SLOT_TPS 2
+#define PNED_SLOT_VECTOR 3
+
+int pned_slots_create(const pned_model_desc *structure, int R, int max_steps, size_t hbm_budget, pned_slots **out);
+int pned_slots_destroy(pned_slots *s);
+int pned_slots_info(const pned_slots *s, int64_t *dim, int *R, int *max_steps, size_t *bytes);
+/* stream: a cudaStream_t, or NULL for the batch's own stream */
+int pned_slots_set_stream(pned_slots *s, void *stream);
+/* kind PNED_SLOT_LANCZOS or PNED_SLOT_TPS (L: total shift of L - H); v_init [dim] */
+int pned_slots_load(pned_slots *s, int slot, int kind, const pned_model_desc *couplings, const pned_c128 *v_init,
+                    int n_steps, double L, int ptr_flags);
+/* DSF momentum chain from S^z_q x (intalv_zz, S1/2 DSF.f90:18-87); qr [n] phases q.r_j */
+int pned_slots_load_szq(pned_slots *s, int slot, const pned_model_desc *couplings, const pned_c128 *x,
+                        const double *qr, int n_steps, int ptr_flags);
+/* eigenvector pass: alpha/beta/coef [n_steps] of the first pass; x_dev [dim] device memory, overwritten */
+int pned_slots_load_vector(pned_slots *s, int slot, const pned_model_desc *couplings, const pned_c128 *v_init,
+                           int n_steps, const double *alpha, const double *beta, const double *coef,
+                           pned_c128 *x_dev, int ptr_flags);
+/* marks the slot free (its column keeps running as zeros) */
+int pned_slots_release(pned_slots *s, int slot);
+/* enqueues n_steps batch steps on the batch's stream and returns without waiting */
+int pned_slots_step(pned_slots *s, int n_steps);
+/* 1 when all enqueued work has finished, 0 while it runs, else an error status */
+int pned_slots_query(pned_slots *s);
+int pned_slots_synchronize(pned_slots *s);
+/*
+ * Waits for the batch's stream and reads one slot: kind, steps done, status
+ * (1: beta breakdown), alpha/beta [steps_done] (TPS: L - alpha1 and beta),
+ * TPS coef [steps_done][5] (2k/alpha1, L, beta, L - alpha1, Re(L<k-1|k> -
+ * <k-1|L-H|k>)) and the DSF norm ||S^z_q x||^2 / (n ||x||^2).  Any output may
+ * be NULL.
+ */
+int pned_slots_read(pned_slots *s, int slot, int *kind, int *steps_done, int *status, double *alpha, double *beta,
+                    double *coef, double *cnorm);
+/*
+ * Column r of the seeded complex Gaussian [dim][R] start vectors of
+ * pned_fill_gaussian (unnormalised), written as a dense [dim] device vector
+ * on `stream` (a cudaStream_t, NULL: the default stream); returns without
+ * waiting.  Replaces parallelized_set_initial_vec_p (S1/2 parallel.f90:17-102)
+ * for one vector of a batch.
+ */
+int pned_gaussian_column(int64_t dim, int R, int r, uint64_t seed, pned_c128 *v_dev, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* host tridiagonal / continued-fraction routines                             */
 /* ------------------------------------------------------------------------ */
 /* bisec (S1/2 basic.f90:25-107) */

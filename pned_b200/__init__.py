@@ -6,8 +6,8 @@ include/pned_gpu.h); this package is the Python host side over that ABI.
 """
 from . import couplings, lattice  # noqa: F401
 from ._capi import PnedError, lib  # noqa: F401
-from .api import (Context, Model, ObservableSpec, bisec, build_xlocal, exec_renbun,  # noqa: F401
-                  hv_noalloc, mk_list12, normalize_dsf, tps_transform, vec12)
+from .api import (Context, Model, ModelInput, ObservableSpec, SlotBatch, bisec, build_xlocal,  # noqa: F401
+                  exec_renbun, hv_noalloc, mk_list12, normalize_dsf, tps_transform, vec12)
 
-__all__ = ["Context", "Model", "ObservableSpec", "PnedError", "bisec", "build_xlocal", "couplings", "exec_renbun", "hv_noalloc",
+__all__ = ["Context", "Model", "ModelInput", "ObservableSpec", "SlotBatch", "PnedError", "bisec", "build_xlocal", "couplings", "exec_renbun", "hv_noalloc",
            "lattice", "lib", "mk_list12", "normalize_dsf", "tps_transform", "vec12"]

@@ -53,6 +53,9 @@ EXPORTS = [
     "pned_dsf_run", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
     "pned_session_begin", "pned_session_begin_dsf", "pned_session_step", "pned_session_read", "pned_session_vector",
     "pned_session_end", "pned_session_profile", "pned_hv_noalloc",
+    "pned_slots_create", "pned_slots_destroy", "pned_slots_info", "pned_slots_set_stream", "pned_slots_load",
+    "pned_slots_load_szq", "pned_slots_load_vector", "pned_slots_release", "pned_slots_step", "pned_slots_query",
+    "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -103,6 +106,19 @@ def lib() -> C.CDLL:
     L.pned_session_end.argtypes = [vp]
     L.pned_session_profile.argtypes = [vp, i32, dp, dp]
     L.pned_hv_noalloc.argtypes = [vp, i32, vp, vp, dbl, vp, vp]
+    L.pned_slots_create.argtypes = [C.POINTER(ModelDesc), i32, i32, C.c_size_t, C.POINTER(vp)]
+    L.pned_slots_destroy.argtypes = [vp]
+    L.pned_slots_info.argtypes = [vp, C.POINTER(i64), ip, ip, C.POINTER(C.c_size_t)]
+    L.pned_slots_set_stream.argtypes = [vp, vp]
+    L.pned_slots_load.argtypes = [vp, i32, i32, C.POINTER(ModelDesc), vp, i32, dbl, i32]
+    L.pned_slots_load_szq.argtypes = [vp, i32, C.POINTER(ModelDesc), vp, dp, i32, i32]
+    L.pned_slots_load_vector.argtypes = [vp, i32, C.POINTER(ModelDesc), vp, i32, dp, dp, dp, vp, i32]
+    L.pned_slots_release.argtypes = [vp, i32]
+    L.pned_slots_step.argtypes = [vp, i32]
+    L.pned_slots_query.argtypes = [vp]
+    L.pned_slots_synchronize.argtypes = [vp]
+    L.pned_slots_read.argtypes = [vp, i32, ip, ip, ip, dp, dp, dp, dp]
+    L.pned_gaussian_column.argtypes = [i64, i32, i32, C.c_uint64, vp, vp]
     _lib = L
     return L
 

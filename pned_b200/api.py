@@ -144,8 +144,8 @@ def hv_noalloc(model, R: int, v1, v0, eperbd: float = 0.0, stream=None):
     return pr
 
 
-class Model:
-    """A compiled model on the current device (pned_model_create)."""
+class ModelInput:
+    """Host-side model description (pned_model_desc) with the arrays it points to."""
 
     def __init__(self, n, q, tree, ipair, bond_type, xlocal, skip, parity_type, total_sz=None):
         if total_sz is None:
@@ -156,6 +156,7 @@ class Model:
         self._x = np.ascontiguousarray(xlocal, dtype=np.complex128)
         self._skip = None if skip is None else np.ascontiguousarray(skip, dtype=np.uint8)
         self.n_bonds = int(self._bt.shape[0])
+        self.parity_type = int(parity_type)
         d = _capi.ModelDesc()
         d.n_sites, d.q_spin, d.tree, d.n_bonds = self.n, self.q, self.tree, self.n_bonds
         d.ipair = self._ipair.ctypes.data_as(C.POINTER(C.c_int32))
@@ -163,6 +164,30 @@ class Model:
         d.xlocal = C.c_void_p(self._x.ctypes.data)
         d.skip = None if self._skip is None else self._skip.ctypes.data_as(C.POINTER(C.c_uint8))
         d.parity_type, d.total_sz = int(parity_type), int(total_sz)
+        self.c = d
+
+    @classmethod
+    def from_couplings(cls, cluster, couplings, q=2, tree=0, field=None, tps_L=None, simple=0):
+        X, skip, pt = build_xlocal(q, tree, couplings, simple=simple, field=field)
+        if tps_L is not None:
+            X, _ = tps_transform(q, tree, cluster.nbond, X, L=tps_L)
+        return cls(cluster.n, q, tree, cluster.ipair, cluster.ibond_type, X, skip, pt)
+
+    @classmethod
+    def structure(cls, cluster, tree=0):
+        """Generic S = 1/2 structure of a cluster: every local-matrix entry non-zero,
+        so every one- and two-site flip of every bond is a term (slot batches)."""
+        X = np.ones((9, 4, 4), dtype=np.complex128)
+        return cls(cluster.n, 2, tree, cluster.ipair, cluster.ibond_type, X, None, 1)
+
+
+class Model:
+    """A compiled model on the current device (pned_model_create)."""
+
+    def __init__(self, n, q, tree, ipair, bond_type, xlocal, skip, parity_type, total_sz=None):
+        self.desc = ModelInput(n, q, tree, ipair, bond_type, xlocal, skip, parity_type, total_sz)
+        self.n, self.q, self.tree, self.n_bonds = self.desc.n, self.desc.q, self.desc.tree, self.desc.n_bonds
+        d = self.desc.c
         h = C.c_void_p()
         check(lib().pned_model_create(C.byref(d), C.byref(h)))
         self._h = h
@@ -412,3 +437,118 @@ class Context:
     def session_end(self):
         check(lib().pned_session_end(self._h))
         self._sess = None
+
+
+# --------------------------------------------------------------------------- slot batches
+
+
+def gaussian_column(dim: int, R: int, r: int, seed: int, out, stream=None):
+    """Column r of the seeded [dim][R] complex Gaussian start vectors (unnormalised)
+    into the CUDA tensor `out` on `stream`; does not wait."""
+    p, f = _ptr(out, writable=True)
+    if f != PTR_DEVICE or out.numel() != dim:
+        raise TypeError("out must be a CUDA tensor of dim elements")
+    sp = None if stream is None else C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
+    check(lib().pned_gaussian_column(int(dim), int(R), int(r), C.c_uint64(int(seed) & (2**64 - 1)), p, sp))
+
+SLOT_KINDS = {"free": 0, "lanczos": 1, "tps": 2, "vector": 3}
+_SLOT_NAMES = {v: k for k, v in SLOT_KINDS.items()}
+
+
+class SlotBatch:
+    """R slots of independent chains over one S = 1/2 lattice (pned_slots_*).
+
+    Each slot carries its own couplings (a ModelInput on the batch's lattice);
+    all slots advance together, one batched H.V per step, and a slot is loaded
+    or released between steps while the others keep running."""
+
+    def __init__(self, structure: ModelInput, R: int, max_steps: int, hbm_budget: int = 0, stream=None):
+        self.structure = structure
+        h = C.c_void_p()
+        check(lib().pned_slots_create(C.byref(structure.c), int(R), int(max_steps), C.c_size_t(int(hbm_budget)),
+                                      C.byref(h)))
+        self._h = h
+        dim, r, ms, nb = C.c_int64(0), C.c_int(0), C.c_int(0), C.c_size_t(0)
+        check(lib().pned_slots_info(h, C.byref(dim), C.byref(r), C.byref(ms), C.byref(nb)))
+        self.dim, self.R, self.max_steps, self.bytes = dim.value, r.value, ms.value, nb.value
+        self.n = structure.n
+        if stream is not None:
+            self.set_stream(stream)
+
+    def set_stream(self, stream):
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        check(lib().pned_slots_set_stream(self._h, C.c_void_p(sp)))
+
+    def _vec(self, v):
+        p, f = _ptr(v)
+        n = v.numel() if _is_dev(v) else v.size
+        if n != self.dim:
+            raise ValueError(f"vector has {n} elements, expected dim = {self.dim}")
+        return p, f
+
+    def load(self, slot: int, kind: str, couplings: ModelInput, v_init, n_steps: int, L: float = 0.0):
+        """Starts a Lanczos ('lanczos') or TPS ('tps', shift L) chain in `slot` from v_init (normalised here)."""
+        p, f = self._vec(v_init)
+        check(lib().pned_slots_load(self._h, int(slot), SLOT_KINDS[kind], C.byref(couplings.c), p, int(n_steps),
+                                    float(L), f))
+
+    def load_szq(self, slot: int, couplings: ModelInput, x, qr, n_steps: int):
+        """Starts a DSF momentum chain from S^z_q x (phases qr[j] = q.r_j)."""
+        p, f = self._vec(x)
+        q = np.ascontiguousarray(qr, dtype=np.float64)
+        if q.shape != (self.n,):
+            raise ValueError("qr must have n entries")
+        check(lib().pned_slots_load_szq(self._h, int(slot), C.byref(couplings.c), p, _dp(q), int(n_steps), f))
+
+    def load_vector(self, slot: int, couplings: ModelInput, v_init, alpha, beta, coef, x_dev):
+        """Eigenvector pass: replays the chain of v_init with stored alpha/beta and
+        accumulates x = sum_k coef[k] v_k into the CUDA tensor x_dev."""
+        p, f = self._vec(v_init)
+        px, fx = _ptr(x_dev, writable=True)
+        if fx != PTR_DEVICE or x_dev.numel() != self.dim:
+            raise TypeError("x_dev must be a CUDA tensor of dim elements")
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        n = len(c)
+        if len(a) < n or len(b) < n:
+            raise ValueError("alpha and beta need at least len(coef) entries")
+        check(lib().pned_slots_load_vector(self._h, int(slot), C.byref(couplings.c), p, n, _dp(a), _dp(b), _dp(c),
+                                           px, f))
+
+    def release(self, slot: int):
+        check(lib().pned_slots_release(self._h, int(slot)))
+
+    def step(self, n: int):
+        check(lib().pned_slots_step(self._h, int(n)))
+
+    def query(self) -> bool:
+        rc = lib().pned_slots_query(self._h)
+        if rc not in (0, 1):
+            check(rc)
+        return rc == 1
+
+    def synchronize(self):
+        check(lib().pned_slots_synchronize(self._h))
+
+    def read(self, slot: int) -> dict:
+        kind, steps, status, cn = C.c_int(0), C.c_int(0), C.c_int(0), C.c_double(0.0)
+        check(lib().pned_slots_read(self._h, int(slot), C.byref(kind), C.byref(steps), C.byref(status), None, None,
+                                    None, None))
+        k = steps.value
+        a, b, c = np.zeros(max(1, k)), np.zeros(max(1, k)), np.zeros((max(1, k), 5))
+        check(lib().pned_slots_read(self._h, int(slot), C.byref(kind), C.byref(steps), C.byref(status), _dp(a),
+                                    _dp(b), _dp(c), C.byref(cn)))
+        return {"kind": _SLOT_NAMES.get(kind.value, kind.value), "steps": k, "status": status.value,
+                "alpha": a[:k], "beta": b[:k], "coef": c[:k], "cnorm": cn.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pned_slots_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

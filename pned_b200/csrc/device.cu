@@ -141,6 +141,8 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
 #pragma unroll
     for (int k = 0; k < K; ++k) red[k][0] = make_double2(0.0, 0.0);
     const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
+    const double hs = a.hsc ? a.hsc[0] : sc;
+    const double shift = a.shift + (a.shiftv ? a.shiftv[0] : 0.0);
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         uint32_t base = tid;
         for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
@@ -158,11 +160,11 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
                 if (!prog.first) {
                     acc[j] = make_double2(0.0, 0.0);
                 } else if (RD) {
-                    const double dd = __ldcs(static_cast<const double *>(a.diag) + sj) - a.shift;
+                    const double dd = __ldcs(static_cast<const double *>(a.diag) + sj) - shift;
                     acc[j] = cscale(dd, v[j]);
                 } else {
                     double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + sj);
-                    dd.x -= a.shift;
+                    dd.x -= shift;
                     acc[j] = cmul(dd, v[j]);
                 }
             }
@@ -205,7 +207,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
 #pragma unroll
         for (int j = 0; j < SPT; ++j) {
             const int64_t e = base | prog.jexp[j];
-            const double2 hv = cscale(sc, acc[j]);
+            const double2 hv = cscale(hs, acc[j]);
             double2 out = hv;
             if (!prog.first) {
                 const double2 w0 = __ldcs(a.W + e);
@@ -368,13 +370,6 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(const double2 *__res
     block_reduce_store<1, kMaxVPT>(red, G, vpt, R, partials);
 }
 
-__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
-{
-    x += 0x9E3779B97F4A7C15ull;
-    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-    return x ^ (x >> 31);
-}
 
 __global__ void __launch_bounds__(kThreads) gaussian_kernel(uint64_t key, int64_t dim, double2 *v, int R, int vpt,
                                                             double2 *partials)
@@ -389,13 +384,7 @@ __global__ void __launch_bounds__(kThreads) gaussian_kernel(uint64_t key, int64_
         for (int j = 0; j < kMaxVPT; ++j) {
             if (j >= vpt) break;
             const int64_t g = base + j;
-            const uint64_t h1 = splitmix64(key ^ uint64_t(2 * g));
-            const uint64_t h2 = splitmix64(key ^ uint64_t(2 * g + 1));
-            const double u1 = (double(h1 >> 11) + 0.5) * 0x1.0p-53;
-            const double u2 = double(h2 >> 11) * 0x1.0p-53;
-            const double rad = sqrt(-log(u1));
-            const double ang = 2.0 * 3.14159265358979323846 * u2;
-            const double2 z = make_double2(rad * cos(ang), rad * sin(ang));
+            const double2 z = gaussian_at(key, g);
             v[g] = z;
             red[0][j].x += z.x * z.x + z.y * z.y;
         }
@@ -435,7 +424,7 @@ int pick_vpt(int R)
 
 // Opts a kernel into more than 48 KB of dynamic shared memory, once per kernel
 // and device (static + dynamic above 48 KB fails to launch without it).
-static cudaError_t allow_dynamic_smem(const void *kern, int device)
+cudaError_t allow_dynamic_smem(const void *kern, int device)
 {
     static std::mutex mu;
     static std::vector<std::pair<const void *, int>> done;
@@ -582,6 +571,10 @@ using namespace pned;
 
 static thread_local int g_device = 0;
 
+namespace pned {
+int current_device() { return g_device; }
+}  // namespace pned
+
 extern "C" int pned_set_device(int device)
 {
     int cnt = 0;
@@ -591,6 +584,44 @@ extern "C" int pned_set_device(int device)
     g_device = device;
     return PNED_OK;
 }
+
+namespace pned {
+
+// Tiled single-vector programs (S = 1/2, n >= 12), one launch per pass.
+void build_tile_programs(pned_model *m)
+{
+    const HostProgram &hp = m->hp;
+    if (hp.q == 2 && hp.n >= 12 && plan_tiles(m->hp, 3, kTileWindowBits, kTileMaxPasses) == PNED_OK) {
+        const HostProgram &h2 = m->hp;
+        for (size_t p = 0; p < h2.passes.size(); ++p) {
+            const HostProgram::TilePass &ps = h2.passes[p];
+            std::unique_ptr<TileProgram> T(new TileProgram());
+            T->n = h2.n;
+            T->jb = ps.jb;
+            T->nin = ps.nin;
+            T->nterms = int(ps.tterms.size());
+            T->ntab = m->ntab;
+            T->nouter = int(ps.outer.size());
+            T->first = p == 0;
+            T->last = p + 1 == h2.passes.size();
+            for (int j = 0; j < (1 << ps.jb); ++j) {
+                uint32_t e = 0;
+                for (int k = 0; k < ps.jb; ++k) if ((j >> k) & 1) e |= 1u << ps.jpos[k];
+                T->jexp[j] = e;
+            }
+            for (int k = 0; k < T->nouter; ++k) T->outer[k] = uint8_t(ps.outer[k]);
+            T->ngroups = int(ps.gxor.size());
+            for (int g = 0; g <= T->ngroups; ++g) T->gstart[g] = uint16_t(ps.gstart[g]);
+            for (int g = 0; g < T->ngroups; ++g) T->gxor[g] = ps.gxor[g];
+            std::copy(ps.tterms.begin(), ps.tterms.end(), T->t);
+            m->tprogs.push_back(std::move(T));
+        }
+        m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << 3) + std::max(1, m->ntab));
+        m->use_tile = true;
+    }
+}
+
+}  // namespace pned
 
 extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
 {
@@ -630,34 +661,7 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g_device);
         m->nsm = nsm;
     }
-    if (hp.q == 2 && hp.n >= 12 && plan_tiles(m->hp, 3, kTileWindowBits, kTileMaxPasses) == PNED_OK) {
-        const HostProgram &h2 = m->hp;
-        for (size_t p = 0; p < h2.passes.size(); ++p) {
-            const HostProgram::TilePass &ps = h2.passes[p];
-            std::unique_ptr<TileProgram> T(new TileProgram());
-            T->n = h2.n;
-            T->jb = ps.jb;
-            T->nin = ps.nin;
-            T->nterms = int(ps.tterms.size());
-            T->ntab = m->ntab;
-            T->nouter = int(ps.outer.size());
-            T->first = p == 0;
-            T->last = p + 1 == h2.passes.size();
-            for (int j = 0; j < (1 << ps.jb); ++j) {
-                uint32_t e = 0;
-                for (int k = 0; k < ps.jb; ++k) if ((j >> k) & 1) e |= 1u << ps.jpos[k];
-                T->jexp[j] = e;
-            }
-            for (int k = 0; k < T->nouter; ++k) T->outer[k] = uint8_t(ps.outer[k]);
-            T->ngroups = int(ps.gxor.size());
-            for (int g = 0; g <= T->ngroups; ++g) T->gstart[g] = uint16_t(ps.gstart[g]);
-            for (int g = 0; g < T->ngroups; ++g) T->gxor[g] = ps.gxor[g];
-            std::copy(ps.tterms.begin(), ps.tterms.end(), T->t);
-            m->tprogs.push_back(std::move(T));
-        }
-        m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << 3) + std::max(1, m->ntab));
-        m->use_tile = true;
-    }
+    build_tile_programs(m.get());
     // coefficient table
     std::vector<double2> tab(std::max<size_t>(1, hp.table.size()));
     for (size_t i = 0; i < hp.table.size(); ++i) tab[i] = make_double2(hp.table[i].real(), hp.table[i].imag());

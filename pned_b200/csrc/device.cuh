@@ -91,6 +91,12 @@ int pick_vpt(int R);
 void session_release(pned_ctx *c);
 
 cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
+// Raises a kernel's dynamic shared memory limit to 200 KB (once per kernel and device).
+cudaError_t allow_dynamic_smem(const void *kern, int device);
+// Device chosen by pned_set_device on this host thread.
+int current_device();
+// Plans the tiled single-vector passes of m->hp (S = 1/2, n >= 12) and sets m->use_tile.
+void build_tile_programs(pned_model *m);
 // Number of partial-sum blocks launch_hv writes for this model, R and grid.
 int hv_partial_blocks(const pned_model *m, int R, int nblocks);
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);
@@ -159,6 +165,27 @@ __device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G
         for (int w = 0; w < nw; ++w) s = cadd(s, sm[w][k][r]);
         partials[((size_t)blockIdx.x * K + k) * R + r] = s;
     }
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// Element g of the seeded complex Gaussian stream (key = splitmix64(seed ^
+// 0x5DEECE66D)): Box-Muller on two counter hashes, sqrt(-ln u1) e^{2 pi i u2}.
+__device__ __forceinline__ double2 gaussian_at(uint64_t key, int64_t g)
+{
+    const uint64_t h1 = splitmix64(key ^ uint64_t(2 * g));
+    const uint64_t h2 = splitmix64(key ^ uint64_t(2 * g + 1));
+    const double u1 = (double(h1 >> 11) + 0.5) * 0x1.0p-53;
+    const double u2 = double(h2 >> 11) * 0x1.0p-53;
+    const double rad = sqrt(-log(u1));
+    const double ang = 2.0 * 3.14159265358979323846 * u2;
+    return make_double2(rad * cos(ang), rad * sin(ang));
 }
 
 // Common epilogue of the H.v kernels: writes W and accumulates the fused sums.

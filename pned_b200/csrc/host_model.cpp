@@ -280,6 +280,47 @@ std::vector<Bond> schedule_bonds(const pned_model_desc *d)
 
 }  // namespace
 
+int eval_tables_on_structure(const HostProgram &S, const pned_model_desc *d, std::vector<cd> &table,
+                             std::vector<cd> &dtab)
+{
+    if (S.q != 2 || d->q_spin != 2 || d->n_sites != S.n || d->n_bonds != S.nbond)
+        return fail(PNED_EINVAL, "slot couplings: lattice differs from the slot batch's structure");
+    std::vector<Bond> bonds = schedule_bonds(d);
+    for (size_t i = 0; i < bonds.size(); ++i)
+        if (bonds[i].s1 != S.dsite1[i] || bonds[i].s2 != S.dsite2[i])
+            return fail(PNED_EINVAL, "slot couplings: bond list differs from the slot batch's structure");
+    const int Q = 4;
+    auto elem = [&](int t, int row, int col) -> cd {
+        const size_t k = size_t(t - 1) * Q * Q + row + size_t(Q) * col;
+        if (d->skip && d->skip[k]) return cd(0, 0);
+        return cd(d->xlocal[k].re, d->xlocal[k].im);
+    };
+    table.assign(S.table.size(), cd(0, 0));
+    for (size_t ti = 0; ti < S.xterms.size(); ++ti) {
+        const XorTerm &term = S.xterms[ti];
+        std::vector<int> deps;
+        for (int k = 0; k < term.nb; ++k) deps.push_back((term.pos4 >> (8 * k)) & 0xff);
+        for (int idx = 0; idx < (1 << term.nb); ++idx) {
+            auto bit = [&](int site) {
+                for (size_t k = 0; k < deps.size(); ++k)
+                    if (deps[k] == site) return (idx >> k) & 1;
+                return 0;
+            };
+            cd c = 0;
+            for (const auto &bf : S.xcontrib[ti]) {
+                const Bond &b = bonds[bf.first];
+                const int st = 2 * bit(b.s2) + bit(b.s1);
+                c += elem(b.t, st ^ bf.second, st);
+            }
+            table[term.tab + idx] = c;
+        }
+    }
+    dtab.clear();
+    for (const Bond &b : bonds)
+        for (int st = 0; st < Q; ++st) dtab.push_back(elem(b.t, st, st));
+    return PNED_OK;
+}
+
 int compile_program(const pned_model_desc *d, HostProgram &P)
 {
     const int n = d->n_sites, q = d->q_spin, Q = q * q;
@@ -307,6 +348,7 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
         if (d->skip && d->skip[k]) return cd(0, 0);
         return cd(d->xlocal[k].re, d->xlocal[k].im);
     };
+    for (const Bond &b : bonds) P.bond_type.push_back(b.t);
     // diagonal tables
     for (const Bond &b : bonds) {
         P.dsite1.push_back(b.s1);
@@ -351,6 +393,9 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
                 std::sort(deps.begin(), deps.end());
                 XorTerm term{};
                 term.xmask = mask;
+                std::vector<std::pair<int, int>> contrib;
+                for (size_t k = i; k < j; ++k) contrib.push_back({cs[k].bond, cs[k].f});
+                P.xcontrib.push_back(contrib);
                 term.nb = uint8_t(deps.size());
                 term.pos4 = 0;
                 for (size_t k = 0; k < deps.size(); ++k) term.pos4 |= uint32_t(deps[k]) << (8 * k);

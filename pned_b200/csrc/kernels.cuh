@@ -79,6 +79,10 @@ struct HvArgs {
     int R;
     int K;                  // 1: alpha; 2: alpha, ||W||^2; 4: + <G|W>, <G|C>
     int *err;               // set to 1 by a kernel whose bounded wait gave up (may be null)
+    // tiled single-vector kernel only (slot batches): per-call scale of the H part
+    // (null: sc) and an extra diagonal shift (null: none)
+    const double *hsc;
+    const double *shiftv;
 };
 
 }  // namespace pned

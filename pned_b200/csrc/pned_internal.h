@@ -68,6 +68,9 @@ struct HostProgram {
     int nbond = 0;
     bool real = true;                    // every coefficient and diagonal entry real
     std::vector<XorTerm> xterms;         // q == 2
+    // per xor term: the (bond index, flip pattern f) contributions summed into its table
+    std::vector<std::vector<std::pair<int, int>>> xcontrib;
+    std::vector<int> bond_type;          // schedule-order bond types (1..9)
     std::vector<RadixTerm> rterms;       // q > 2
     std::vector<cd> table;               // coefficient tables
     // diagonal: per bond (s1, s2) and q*q diagonal values (pair state st)
@@ -91,6 +94,12 @@ struct HostProgram {
 // `window_bits` outer bits of its own tile order (so they are found in L2),
 // the last pass takes what is left.
 int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes);
+
+// Coefficient tables and diagonal tables of `d` evaluated on the term
+// structure of S (same lattice and bonds; q == 2): table[i] for the entries of
+// S.table, dtab as S.dtab.  Terms that `d` lacks get zeros.
+int eval_tables_on_structure(const HostProgram &S, const pned_model_desc *d, std::vector<cd> &table,
+                             std::vector<cd> &dtab);
 
 // Builds the program from a model description (bond order, skip mask and
 // element order follow make_cpu_list2; see model.cpp).
