@@ -122,6 +122,14 @@ int pned_model_create(const pned_model_desc *desc, pned_model **out);
 int pned_model_destroy(pned_model *m);
 /* dim = q^n; n_terms = off-diagonal gather terms per state in the program. */
 int pned_model_info(const pned_model *m, int64_t *dim, int *n_terms, int *real_coefficients);
+/*
+ * Measurement hook (no counterpart in the reference): the single-vector H.v
+ * plan.  tile_passes = launches of the tiled kernel per H.v (0: the flat
+ * gather kernel runs); partner_tiles = distinct out-of-tile flip patterns
+ * summed over the passes (each one a partner-tile read); tile_states =
+ * states per tile.  Any output may be NULL.
+ */
+int pned_model_plan(const pned_model *m, int *tile_passes, int *partner_tiles, int *tile_states);
 
 /* ------------------------------------------------------------------------ */
 /* context: device vectors for R interleaved vectors                         */
@@ -234,6 +242,18 @@ int pned_tps_run(pned_ctx *c, double L, const pned_c128 *v_init, int n_steps, in
 int pned_dsf_run(pned_ctx *c, const pned_c128 *x, const double *qr, int n_steps, double *cnorm, double *salpha,
                  double *sbeta, int ptr_flags);
 
+/*
+ * parallelized_lncv1z (S1/2 Lanczos.f90:183-329), R = 1: replays the Lanczos
+ * chain of v_init (host or device, as in pned_lanczos_run) with the stored
+ * alpha/beta of the first pass and returns x = sum_k coef[k] v_k (coef[0..n_steps-1],
+ * the tridiagonal eigenvector from pned_vec12) normalised, in x_out (host or
+ * device).  As written the reference zeroes v1 before its first product, so
+ * its x is the normalised initial vector, refined afterwards by inverse
+ * iteration (pned_cg_run); this computes the Lanczos eigenvector the routine
+ * sets up.
+ */
+int pned_lanczos_vector(pned_ctx *c, const pned_c128 *v_init, int n_steps, const double *alpha, const double *beta,
+                        const double *coef, pned_c128 *x_out, int ptr_flags);
 /*
  * Inverse iteration with CG (parallelized_inv1z + parallelized_cg1,
  * S1/2 cg.f90:18-196) for chain 0: b_init (normalised, [dim]) and E;

@@ -81,6 +81,7 @@ def lib():
                                          c_dbl_p, c_int_p, c_dbl_p]
         L.oracle_normalization_dsf.argtypes = [C.c_int, C.c_double, C.c_double, c_dbl_p]
         L.oracle_inverse_iteration.argtypes = [vp, C.c_double, vp, vp, C.c_int, C.c_int, c_int_p, c_int_p]
+        L.oracle_lanczos_vector.argtypes = [vp, vp, C.c_int, c_dbl_p, c_dbl_p, c_dbl_p, vp]
         L.oracle_gaussian.argtypes = [C.c_uint64, C.c_int64, C.c_int, vp]
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_num_threads.argtypes = [C.c_int]
@@ -314,6 +315,18 @@ class Model:
         if rc:
             raise RuntimeError("oracle_dsf_chain failed")
         return sa, sb
+
+    def lanczos_vector(self, v1, alpha, beta, coef):
+        """parallelized_lncv1z: x = sum_k coef[k] v_k over the replayed chain, normalised."""
+        x = np.zeros(self.ldim, dtype=np.complex128)
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        rc = lib().oracle_lanczos_vector(self._h, _p(_c128(v1).copy()), len(c), _p(a, C.c_double),
+                                         _p(b, C.c_double), _p(c, C.c_double), _p(x))
+        if rc:
+            raise RuntimeError(f"oracle_lanczos_vector rc={rc}")
+        return x
 
     def inverse_iteration(self, E, b, inv_max=5000, cg_max=500):
         x = np.zeros(self.ldim, dtype=np.complex128)

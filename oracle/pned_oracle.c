@@ -868,6 +868,48 @@ int oracle_lanczos(const omodel *m, cplx *v1, int nsteps, int check_conv, double
 }
 
 /*
+ * Eigenvector by the Lanczos method, parallelized_lncv1z
+ * (S_one_half/Hybrid_TPS_Lanczos.f90:183-329): the chain of the initial
+ * vector is replayed with the alpha/beta stored by the first pass and
+ * x = sum_{k=1..nsteps} coef[k-1] v_k is accumulated (:226-237, :270-309),
+ * then normalised (:312-327).  As written, the reference zeroes v1 before its
+ * first product (:205-214, :238), so its x comes out as the normalised
+ * initial vector, which the following inverse iteration (parallelized_inv1z)
+ * then refines; this restates the recurrence the routine sets up, with v_1 =
+ * the initial vector.
+ */
+int oracle_lanczos_vector(const omodel *m, const cplx *v_init, int nsteps, const double *alpha, const double *beta,
+                          const double *coef, cplx *x)
+{
+    int64_t ldim = m->ldim;
+    cplx *v1 = malloc((size_t)ldim * sizeof(cplx));
+    cplx *v0 = calloc((size_t)ldim, sizeof(cplx));
+    if (!v1 || !v0) { free(v1); free(v0); return OR_ENOMEM; }
+    memcpy(v1, v_init, (size_t)ldim * sizeof(cplx));
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ldim; ++j) x[j] = coef[0] * v1[j];
+    cplx dummy;
+    for (int k = 1; k < nsteps; ++k) {
+        /* v0 = H v_k - beta_{k-1} v_{k-1} (v0 holds -beta_{k-1} v_{k-1}) */
+        oracle_p_mltply_v3(m, v1, v0, 0.0, &dummy);
+        const double a = alpha[k - 1], b = beta[k - 1], c = coef[k];
+#pragma omp parallel for schedule(static)
+        for (int64_t j = 0; j < ldim; ++j) {
+            cplx temp1 = v1[j];
+            cplx temp2 = (v0[j] - a * v1[j]) / b;
+            v0[j] = -b * temp1;
+            v1[j] = temp2;
+            x[j] += c * temp2;
+        }
+    }
+    double dn = sqrt(creal(oracle_inprdct(ldim, x, x)));
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ldim; ++j) x[j] /= dn;
+    free(v1); free(v0);
+    return OR_OK;
+}
+
+/*
  * Diagonal observables of the TPS step (S_one_half/Hybrid_TPS_TPS.f90:128-321,
  * S_arbitrary/Hybrid_TPS9_TPS.f90 twin).  Every observable the reference
  * evaluates has the form

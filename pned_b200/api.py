@@ -195,6 +195,12 @@ class Model:
         check(lib().pned_model_info(h, C.byref(dim), C.byref(nt), C.byref(rc_)))
         self.dim, self.n_terms, self.real = dim.value, nt.value, bool(rc_.value)
 
+    def plan(self) -> dict:
+        """Single-vector H.v plan: tiled-kernel passes, partner tiles, states per tile."""
+        p, g, t = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(lib().pned_model_plan(self._h, C.byref(p), C.byref(g), C.byref(t)))
+        return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
+
     @classmethod
     def from_couplings(cls, cluster, couplings, q=2, tree=0, field=None, tps_L=None, simple=0):
         """Model from a cluster table and coupling slots (+ field, + TPS shift L)."""
@@ -368,6 +374,23 @@ class Context:
         rc = lib().pned_dsf_run(self._h, p, _dp(qr), n_steps, _dp(cn), _dp(sa), _dp(sb), f)
         check(rc)
         return dict(cnorm=cn, salpha=sa.reshape(n_steps, self.R), sbeta=sb.reshape(n_steps + 1, self.R))
+
+    def lanczos_vector(self, v_init, alpha, beta, coef, x_out=None):
+        """parallelized_lncv1z (R = 1): x = sum_k coef[k] v_k over the replayed chain, normalised."""
+        self._check_len(v_init)
+        p, f = _ptr(v_init)
+        if x_out is None:
+            x_out = np.zeros(self.model.dim, dtype=np.complex128) if f == PTR_HOST else \
+                torch.zeros(self.model.dim, dtype=torch.complex128, device=v_init.device)
+        px, fx = _ptr(x_out, writable=True)
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        b = np.ascontiguousarray(beta, dtype=np.float64)
+        c = np.ascontiguousarray(coef, dtype=np.float64)
+        n = len(c)
+        if len(a) < n or len(b) < n:
+            raise ValueError("alpha and beta need at least len(coef) entries")
+        check(lib().pned_lanczos_vector(self._h, p, n, _dp(a), _dp(b), _dp(c), px, _same_flag(f, fx)))
+        return x_out
 
     def cg(self, E: float, b_init, inv_max: int = 5000, cg_max: int = 500, x_out=None):
         """parallelized_inv1z + cg1 (R = 1): returns (x, n_inv, n_cg)."""

@@ -709,6 +709,17 @@ extern "C" int pned_model_destroy(pned_model *m)
     return PNED_OK;
 }
 
+extern "C" int pned_model_plan(const pned_model *m, int *tile_passes, int *partner_tiles, int *tile_states)
+{
+    if (!m) return fail(PNED_EINVAL, "pned_model_plan: null model");
+    int groups = 0;
+    for (const auto &t : m->tprogs) groups += t->ngroups;
+    if (tile_passes) *tile_passes = m->use_tile ? int(m->tprogs.size()) : 0;
+    if (partner_tiles) *partner_tiles = m->use_tile ? groups : 0;
+    if (tile_states) *tile_states = m->use_tile ? kThreads * (1 << 3) : 0;
+    return PNED_OK;
+}
+
 extern "C" int pned_model_info(const pned_model *m, int64_t *dim, int *n_terms, int *real_coef)
 {
     if (!m) return fail(PNED_EINVAL, "pned_model_info: null model");

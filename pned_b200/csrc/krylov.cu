@@ -181,6 +181,33 @@ __global__ void scale_real_kernel(double2 *v, double f, int64_t n)
         v[i] = cscale(f, v[i]);
 }
 
+// Eigenvector pass: v = sc C; x += c v; Pn = W - a v (Pn may be null: accumulate only).
+__global__ void __launch_bounds__(kThreads) lncv_kernel(const double2 *__restrict__ W, const double2 *__restrict__ C,
+                                                        double2 *Pn, double2 *x, const double *__restrict__ sc,
+                                                        double a, double c, int64_t n)
+{
+    const double s = *sc;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = cscale(s, C[i]);
+        const double2 xo = x[i];
+        x[i] = make_double2(fma(c, v.x, xo.x), fma(c, v.y, xo.y));
+        if (Pn) {
+            const double2 w = W[i];
+            Pn[i] = make_double2(w.x - a * v.x, w.y - a * v.y);
+        }
+    }
+}
+
+// sc <- 1/b, pc <- -b sc_old
+__global__ void lncv_scal_kernel(double *sc, double *pc, double b)
+{
+    if (threadIdx.x == 0) {
+        const double old = *sc;
+        *sc = 1.0 / b;
+        *pc = -b * old;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // one step of each kind; buffer roles live in the session
 // ---------------------------------------------------------------------------
@@ -622,6 +649,65 @@ extern "C" int pned_dsf_run(pned_ctx *c, const pned_c128 *x, const double *qr, i
     if (rc) return rc;
     for (int r = 0; r < R; ++r) sbeta[r] = cnorm[r];
     for (size_t i = 0; i < b.size(); ++i) sbeta[R + i] = b[i];
+    return PNED_OK;
+}
+
+// parallelized_lncv1z (S1/2 Lanczos.f90:183-329): the chain of v_init is
+// replayed with the stored alpha/beta, x = sum_k coef[k] v_k, normalised.
+extern "C" int pned_lanczos_vector(pned_ctx *c, const pned_c128 *v_init, int n_steps, const double *alpha,
+                                   const double *beta, const double *coef, pned_c128 *x_out, int flags)
+{
+    if (!c || !v_init || !alpha || !beta || !coef || !x_out || n_steps < 1)
+        return fail(PNED_EINVAL, "pned_lanczos_vector: bad arguments");
+    if (c->R != 1) return fail(PNED_EINVAL, "pned_lanczos_vector: needs a context with R = 1");
+    for (int k = 0; k < n_steps - 1; ++k)
+        if (!(beta[k] > 0.0)) return fail(PNED_EINVAL, "pned_lanczos_vector: beta must be positive");
+    cudaSetDevice(c->m->device);
+    int rc = 0;
+    for (int k = 0; k < 4; ++k)
+        if ((rc = ctx_alloc_buffer(c, k))) return rc;
+    double2 *Cb = c->buf[0], *Pb = c->buf[1], *W = c->buf[2], *x = c->buf[3];
+    const int64_t n = c->m->dim;
+    const size_t bytes = sizeof(double2) * size_t(n);
+    const int nb = c->nblocks;
+    cudaError_t e = cudaMemcpyAsync(Cb, v_init, bytes,
+                                    (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, bytes, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_lanczos_vector: staging");
+    if ((rc = set_slot(c, kSlotSc, 1.0)) || (rc = set_slot(c, kSlotPc, 0.0))) return rc;
+    for (int k = 0; k < n_steps; ++k) {
+        if (k + 1 == n_steps) {
+            lncv_kernel<<<nb, kThreads, 0, c->stream>>>(nullptr, Cb, nullptr, x, slot(c, kSlotSc), 0.0, coef[k], n);
+            e = cudaGetLastError();
+            break;
+        }
+        HvArgs a{};
+        a.C = Cb; a.P = k ? Pb : nullptr; a.W = W;
+        a.sc = slot(c, kSlotSc); a.pc = k ? slot(c, kSlotPc) : nullptr;
+        a.diag = c->m->d_diag; a.shift = 0.0;
+        a.table = c->m->d_table; a.partials = c->partials;
+        a.dim = n; a.R = 1; a.K = 1; a.err = c->flag;
+        e = launch_hv(c->m, a, nb, c->stream);
+        if (e != cudaSuccess) break;
+        lncv_kernel<<<nb, kThreads, 0, c->stream>>>(W, Cb, Pb, x, slot(c, kSlotSc), alpha[k], coef[k], n);
+        lncv_scal_kernel<<<1, 32, 0, c->stream>>>(slot(c, kSlotSc), slot(c, kSlotPc), beta[k]);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) break;
+        std::swap(Cb, Pb);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "pned_lanczos_vector");
+    // normalise
+    double2 xx;
+    e = launch_dot(c, x, x, nullptr, 0, c->sums, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_lanczos_vector: norm");
+    if ((rc = sums_to_host(c, 1))) return rc;
+    xx = c->h_sums[0];
+    scale_real_kernel<<<nb, kThreads, 0, c->stream>>>(x, 1.0 / std::sqrt(xx.x), n);
+    e = cudaMemcpyAsync(x_out, x, bytes, (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_lanczos_vector: result");
     return PNED_OK;
 }
 

@@ -463,11 +463,11 @@ def run_plain(req: Request) -> dict:
         v = torch.empty(m.dim, dtype=torch.complex128, device="cuda")
         ctx.fill_gaussian(req.seed, v)
         r = ctx.lanczos(v, req.gs_steps)
-        e0 = float(api.bisec(r["alpha"][:, 0], r["beta"][:, 0], req.gs_steps, 1)[0])
-        b = torch.empty(m.dim, dtype=torch.complex128, device="cuda")
-        ctx.fill_gaussian(req.seed + 1, b)
-        x = torch.empty(m.dim, dtype=torch.complex128, device="cuda")
-        ctx.cg(e0 - 1e-9, b, inv_max=30, x_out=x)
+        a, b = r["alpha"][:, 0], r["beta"][:, 0]
+        E = api.bisec(a, b, req.gs_steps, 1)
+        e0 = float(E[0])
+        c = api.vec12(a, b, E, req.gs_steps, 1)[0]
+        x = ctx.lanczos_vector(v, a, b, c)
         ctx.close()
         ctxq = api.Context(m, R=req.nq)
         qrs = np.stack([cl.qr(q) for q in range(req.nq)])

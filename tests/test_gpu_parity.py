@@ -226,6 +226,28 @@ def test_dsf_parity():
             assert rel(d1, d2) <= tol_spec, (steps, r, rel(d1, d2))
 
 
+def test_lanczos_vector_parity():
+    """parallelized_lncv1z: the eigenvector pass replays the chain with the stored
+    alpha/beta; x agrees with the oracle to 1e-10 and is an eigenvector."""
+    cl = honeycomb(3, 2)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    v = O.gaussian(3, gm.dim)
+    v /= np.linalg.norm(v)
+    M = 60
+    ref = om.lanczos(v, M)
+    E = P.bisec(ref["alpha"], ref["beta"], M, 1)
+    c = P.vec12(ref["alpha"], ref["beta"], E, M, 1)[0]
+    xr = om.lanczos_vector(v, ref["alpha"], ref["beta"], c)
+    ctx = P.Context(gm, R=1)
+    x = ctx.lanczos_vector(v, ref["alpha"], ref["beta"], c)
+    assert rel(x, xr) <= 1e-10
+    hx = np.zeros_like(x)
+    om.p_mltply_v3(x, hx, 0.0)
+    assert np.linalg.norm(hx - E[0] * x) <= 1e-10
+    xd = ctx.lanczos_vector(torch.from_numpy(v).cuda(), ref["alpha"], ref["beta"], c)
+    assert rel(xd.cpu().numpy(), xr) <= 1e-10
+
+
 def test_cg_inverse_iteration():
     cl = honeycomb(2, 2)
     gm, om = models(cl, 2, 0, KH)
