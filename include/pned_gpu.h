@@ -123,13 +123,29 @@ int pned_model_destroy(pned_model *m);
 /* dim = q^n; n_terms = off-diagonal gather terms per state in the program. */
 int pned_model_info(const pned_model *m, int64_t *dim, int *n_terms, int *real_coefficients);
 /*
- * Measurement hook (no counterpart in the reference): the single-vector H.v
- * plan.  tile_passes = launches of the tiled kernel per H.v (0: the flat
- * gather kernel runs); partner_tiles = distinct out-of-tile flip patterns
- * summed over the passes (each one a partner-tile read); tile_states =
- * states per tile.  Any output may be NULL.
+ * Measurement hook (no counterpart in the reference): the H.v plan for R
+ * vectors.  tile_passes = launches of the tiled kernel per H.v (0: the flat
+ * gather kernel runs, or R > 1 not planned yet); partner_tiles = distinct
+ * out-of-tile flip patterns summed over the passes (each one a partner-tile
+ * read); tile_states = states per tile.  Any output may be NULL.
  */
-int pned_model_plan(const pned_model *m, int *tile_passes, int *partner_tiles, int *tile_states);
+int pned_model_plan(const pned_model *m, int R, int *tile_passes, int *partner_tiles, int *tile_states);
+/*
+ * Tuning hook (no counterpart in the reference): parameters of the tiled H.v
+ * plan for R vectors; any field -1 keeps its default.  row_fixed_bits: low
+ * global bits kept in the tile rows (8 for R = 1 by default: rows are runs
+ * of 256 consecutive states; fewer lets the planner pick tile bits that
+ * leave fewer partner tiles); window_bits: outer bits whose partner tiles a
+ * pass expects in L2; max_passes: 1..4.  Re-plans at once (plan NULL:
+ * defaults); call it between launches, not while other threads launch on the
+ * model.  Used by the autotuner (pned_b200.tune).
+ */
+typedef struct {
+    int32_t row_fixed_bits;
+    int32_t window_bits;
+    int32_t max_passes;
+} pned_tile_plan;
+int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 
 /* ------------------------------------------------------------------------ */
 /* context: device vectors for R interleaved vectors                         */
@@ -364,6 +380,9 @@ int pned_slots_synchronize(pned_slots *s);
  */
 int pned_slots_read(pned_slots *s, int slot, int *kind, int *steps_done, int *status, double *alpha, double *beta,
                     double *coef, double *cnorm);
+/* Tuning and measurement hooks of the batch's tiled H.V (see pned_model_set_plan / pned_model_plan). */
+int pned_slots_set_plan(pned_slots *s, const pned_tile_plan *plan);
+int pned_slots_plan(const pned_slots *s, int *tile_passes, int *partner_tiles, int *tile_states);
 /*
  * Column r of the seeded complex Gaussian [dim][R] start vectors of
  * pned_fill_gaussian (unnormalised), written as a dense [dim] device vector

@@ -303,7 +303,8 @@ class Model:
         qr = np.ascontiguousarray(qr, dtype=np.float64)
         v = np.zeros(self.ldim, dtype=np.complex128)
         cn = np.zeros(1, dtype=np.complex128)
-        lib().oracle_intalv_zz(self._h, _p(qr, C.c_double), _p(_c128(x)), _p(v), _p(cn))
+        xs = _c128(x)   # keep the array alive across the call
+        lib().oracle_intalv_zz(self._h, _p(qr, C.c_double), _p(xs), _p(v), _p(cn))
         return v, complex(cn[0])
 
     def dsf_chain(self, v1, cnorm, nsteps):
@@ -322,7 +323,8 @@ class Model:
         a = np.ascontiguousarray(alpha, dtype=np.float64)
         b = np.ascontiguousarray(beta, dtype=np.float64)
         c = np.ascontiguousarray(coef, dtype=np.float64)
-        rc = lib().oracle_lanczos_vector(self._h, _p(_c128(v1).copy()), len(c), _p(a, C.c_double),
+        v = _c128(v1).copy()   # kept alive across the call
+        rc = lib().oracle_lanczos_vector(self._h, _p(v), len(c), _p(a, C.c_double),
                                          _p(b, C.c_double), _p(c, C.c_double), _p(x))
         if rc:
             raise RuntimeError(f"oracle_lanczos_vector rc={rc}")
@@ -331,6 +333,7 @@ class Model:
     def inverse_iteration(self, E, b, inv_max=5000, cg_max=500):
         x = np.zeros(self.ldim, dtype=np.complex128)
         ni, nc = C.c_int(0), C.c_int(0)
-        lib().oracle_inverse_iteration(self._h, E, _p(_c128(b).copy()), _p(x), inv_max, cg_max, C.byref(ni),
+        bw = _c128(b).copy()   # kept alive across the call
+        lib().oracle_inverse_iteration(self._h, E, _p(bw), _p(x), inv_max, cg_max, C.byref(ni),
                                        C.byref(nc))
         return x, ni.value, nc.value

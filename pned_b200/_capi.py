@@ -30,6 +30,10 @@ class ModelDesc(C.Structure):
     ]
 
 
+class TilePlan(C.Structure):
+    _fields_ = [("row_fixed_bits", C.c_int32), ("window_bits", C.c_int32), ("max_passes", C.c_int32)]
+
+
 class Observable(C.Structure):
     _fields_ = [
         ("n_terms", C.c_int32), ("a", C.POINTER(C.c_int32)), ("b", C.POINTER(C.c_int32)),
@@ -47,7 +51,7 @@ _lib = None
 
 EXPORTS = [
     "pned_abi_version", "pned_last_error", "pned_set_device", "pned_build_xlocal", "pned_tps_transform",
-    "pned_mk_list12", "pned_model_create", "pned_model_destroy", "pned_model_info", "pned_model_plan", "pned_ctx_create",
+    "pned_mk_list12", "pned_model_create", "pned_model_destroy", "pned_model_info", "pned_model_plan", "pned_model_set_plan", "pned_ctx_create",
     "pned_ctx_destroy", "pned_ctx_set_stream", "pned_ctx_synchronize", "pned_ctx_buffer", "pned_ctx_bytes",
     "pned_hv", "pned_inprdct", "pned_calc_beta", "pned_fill_gaussian", "pned_lanczos_run", "pned_tps_run",
     "pned_dsf_run", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
@@ -55,7 +59,7 @@ EXPORTS = [
     "pned_session_end", "pned_session_profile", "pned_hv_noalloc",
     "pned_slots_create", "pned_slots_destroy", "pned_slots_info", "pned_slots_set_stream", "pned_slots_load",
     "pned_slots_load_szq", "pned_slots_load_vector", "pned_slots_release", "pned_slots_step", "pned_slots_query",
-    "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column", "pned_lanczos_vector",
+    "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column", "pned_lanczos_vector", "pned_slots_set_plan", "pned_slots_plan",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -80,7 +84,8 @@ def lib() -> C.CDLL:
     L.pned_model_create.argtypes = [C.POINTER(ModelDesc), C.POINTER(vp)]
     L.pned_model_destroy.argtypes = [vp]
     L.pned_model_info.argtypes = [vp, C.POINTER(i64), ip, ip]
-    L.pned_model_plan.argtypes = [vp, ip, ip, ip]
+    L.pned_model_plan.argtypes = [vp, i32, ip, ip, ip]
+    L.pned_model_set_plan.argtypes = [vp, i32, C.POINTER(TilePlan)]
     L.pned_ctx_create.argtypes = [vp, i32, C.c_size_t, C.POINTER(vp)]
     L.pned_ctx_destroy.argtypes = [vp]
     L.pned_ctx_set_stream.argtypes = [vp, vp]
@@ -121,6 +126,8 @@ def lib() -> C.CDLL:
     L.pned_slots_read.argtypes = [vp, i32, ip, ip, ip, dp, dp, dp, dp]
     L.pned_gaussian_column.argtypes = [i64, i32, i32, C.c_uint64, vp, vp]
     L.pned_lanczos_vector.argtypes = [vp, vp, i32, dp, dp, dp, vp, i32]
+    L.pned_slots_set_plan.argtypes = [vp, C.POINTER(TilePlan)]
+    L.pned_slots_plan.argtypes = [vp, ip, ip, ip]
     _lib = L
     return L
 

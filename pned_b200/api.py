@@ -195,11 +195,17 @@ class Model:
         check(lib().pned_model_info(h, C.byref(dim), C.byref(nt), C.byref(rc_)))
         self.dim, self.n_terms, self.real = dim.value, nt.value, bool(rc_.value)
 
-    def plan(self) -> dict:
-        """Single-vector H.v plan: tiled-kernel passes, partner tiles, states per tile."""
+    def plan(self, R: int = 1) -> dict:
+        """H.v plan for R vectors: tiled-kernel passes, partner tiles, states per tile."""
         p, g, t = C.c_int(0), C.c_int(0), C.c_int(0)
-        check(lib().pned_model_plan(self._h, C.byref(p), C.byref(g), C.byref(t)))
+        check(lib().pned_model_plan(self._h, int(R), C.byref(p), C.byref(g), C.byref(t)))
         return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
+
+    def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1):
+        """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""
+        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes))
+        check(lib().pned_model_set_plan(self._h, int(R), C.byref(tp)))
+        return self.plan(R)
 
     @classmethod
     def from_couplings(cls, cluster, couplings, q=2, tree=0, field=None, tps_L=None, simple=0):
@@ -495,12 +501,14 @@ class SlotBatch:
         check(lib().pned_slots_info(h, C.byref(dim), C.byref(r), C.byref(ms), C.byref(nb)))
         self.dim, self.R, self.max_steps, self.bytes = dim.value, r.value, ms.value, nb.value
         self.n = structure.n
+        self._stream = None
         if stream is not None:
             self.set_stream(stream)
 
     def set_stream(self, stream):
         sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         check(lib().pned_slots_set_stream(self._h, C.c_void_p(sp)))
+        self._stream = stream
 
     def _vec(self, v):
         p, f = _ptr(v)
@@ -541,6 +549,16 @@ class SlotBatch:
 
     def release(self, slot: int):
         check(lib().pned_slots_release(self._h, int(slot)))
+
+    def plan(self) -> dict:
+        p, g, t = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(lib().pned_slots_plan(self._h, C.byref(p), C.byref(g), C.byref(t)))
+        return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
+
+    def set_plan(self, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1) -> dict:
+        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes))
+        check(lib().pned_slots_set_plan(self._h, C.byref(tp)))
+        return self.plan()
 
     def step(self, n: int):
         check(lib().pned_slots_step(self._h, int(n)))

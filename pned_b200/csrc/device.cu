@@ -120,12 +120,13 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
 
 // Tiled single-vector (R = 1) H.v on the S = 1/2 full basis, one pass of a
 // multi-pass program (each pass owns a subset of the flip masks).  A block owns
-// a tile of 256 * 2^JB states: thread t holds states t + 256 j (j < 2^JB),
-// whose global index is base | jexp[j].  The tile is staged in shared memory,
-// so flip masks inside the tile gather from shared memory; the others gather
-// through L1/L2 from the partner tile, two terms at a time so that 2 * 2^JB
-// loads per thread are in flight.  The term decode (coefficient index) is done
-// once per term for the thread's 2^JB states.
+// a tile of 256 * 2^JB states: thread t holds the states of row t (its 8 bits
+// placed on the global bits rowpos[], which start with bits 0..2) and j bits
+// jexp[j] (j < 2^JB), global index base | jexp[j].  The tile is staged in
+// shared memory, so flip masks inside the tile gather from shared memory; the
+// others gather through L1/L2 from the partner tile, 2^JB loads per thread in
+// flight.  The term decode (coefficient index) is done once per term for the
+// thread's 2^JB states.
 template <int JB, bool RC, bool RD, int K>
 __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
 {
@@ -143,8 +144,11 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
     const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
     const double hs = a.hsc ? a.hsc[0] : sc;
     const double shift = a.shift + (a.shiftv ? a.shiftv[0] : 0.0);
+    uint32_t rowbase = 0;   // the thread's row on its global bits
+#pragma unroll
+    for (int k = 0; k < 8; ++k) rowbase |= ((tid >> k) & 1u) << prog.rowpos[k];
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        uint32_t base = tid;
+        uint32_t base = rowbase;
         for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
         double2 acc[SPT];
         {
@@ -231,6 +235,161 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
         }
     }
     block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
+}
+
+// Tiled multi-vector H.V (R > 1 interleaved vectors, S = 1/2 full basis), one
+// pass of a multi-pass program.  G = R / VPT threads share a state; a block
+// owns a tile of NS * SPT states (NS = 256 / G state rows): thread t serves
+// vectors r0 .. r0 + VPT - 1 (r0 = (t mod G) VPT) of row l = t / G, whose j-th
+// state is base | jexp[j] with the bits of l on the global bits rowpos[].  The
+// tile's rows of R values are staged in shared memory ([SPT][NS][R]): in-tile
+// flips gather there, the others through L1/L2 from the partner tile, VPT
+// contiguous values per load.  SLOT: per-vector coefficient tables
+// ([ntab][R]) and real diagonals ([dim][R]).
+template <int VPT, int SPT, bool SLOT, bool RC, bool RD, int K>
+__global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
+{
+    extern __shared__ double2 smem[];
+    const int R = a.R, G = R / VPT, NS = kThreads / G;
+    const int tbits = prog.tbits;
+    const uint32_t tmask = (1u << tbits) - 1u;
+    double2 *s_v = smem;
+    double2 *s_tab = smem + size_t(SPT) * NS * R;
+    const int tabw = SLOT ? R : 1;
+    for (int i = threadIdx.x; i < prog.ntab * tabw; i += blockDim.x) s_tab[i] = a.table[i];
+    const int g = threadIdx.x % G, l = threadIdx.x / G, r0 = g * VPT;
+    const int64_t ntiles = int64_t(1) << prog.nouter;
+    double2 red[K][VPT];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int q = 0; q < VPT; ++q) red[k][q] = make_double2(0.0, 0.0);
+    uint32_t rowbase = 0;   // the thread's row on its global bits
+    for (int k = 0; k < tbits; ++k) rowbase |= ((uint32_t(l) >> k) & 1u) << prog.rowpos[k];
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint32_t base = rowbase;
+        for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
+        double2 acc[SPT][VPT];
+        {
+            double2 v[SPT][VPT];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j)
+#pragma unroll
+                for (int q = 0; q < VPT; ++q) v[j][q] = __ldg(a.C + int64_t(base | prog.jexp[j]) * R + r0 + q);
+            __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+#pragma unroll
+            for (int j = 0; j < SPT; ++j)
+#pragma unroll
+                for (int q = 0; q < VPT; ++q) s_v[(j * NS + l) * R + r0 + q] = v[j][q];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const int64_t sj = base | prog.jexp[j];
+#pragma unroll
+                for (int q = 0; q < VPT; ++q) {
+                    const int r = r0 + q;
+                    if (!prog.first) {
+                        acc[j][q] = make_double2(0.0, 0.0);
+                        continue;
+                    }
+                    const double sh = a.shift + (a.shiftv ? a.shiftv[r] : 0.0);
+                    if (SLOT) {
+                        acc[j][q] = cscale(__ldcs(static_cast<const double *>(a.diag) + sj * R + r) - sh, v[j][q]);
+                    } else if (RD) {
+                        acc[j][q] = cscale(__ldcs(static_cast<const double *>(a.diag) + sj) - sh, v[j][q]);
+                    } else {
+                        double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + sj);
+                        dd.x -= sh;
+                        acc[j][q] = cmul(dd, v[j][q]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // flip masks inside the tile: partners from shared memory
+        for (int t = 0; t < prog.nin; ++t) {
+            const TileTerm T = prog.t[t];
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            const int lp = l ^ int(T.mask & tmask);
+            const uint32_t mhi = T.mask >> tbits;
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const uint32_t idx = T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib;
+                const double2 *ct = s_tab + (T.tab + idx) * tabw + (SLOT ? r0 : 0);
+                const double2 *sv = s_v + ((int(j ^ mhi)) * NS + lp) * R + r0;
+#pragma unroll
+                for (int q = 0; q < VPT; ++q) {
+                    const double2 c = ct[SLOT ? q : 0];
+                    const double2 w = sv[q];
+                    if (RC && !SLOT) { acc[j][q].x = fma(c.x, w.x, acc[j][q].x); acc[j][q].y = fma(c.x, w.y, acc[j][q].y); }
+                    else acc[j][q] = cfma(c, w, acc[j][q]);
+                }
+            }
+        }
+        // flip masks leaving the tile: partners through L1/L2
+        for (int t = prog.nin; t < prog.nterms; ++t) {
+            const TileTerm T = prog.t[t];
+            double2 w0[SPT][VPT];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j)
+#pragma unroll
+                for (int q = 0; q < VPT; ++q)
+                    w0[j][q] = __ldg(a.C + int64_t((base | prog.jexp[j]) ^ T.mask) * R + r0 + q);
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const uint32_t idx = T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib;
+                const double2 *ct = s_tab + (T.tab + idx) * tabw + (SLOT ? r0 : 0);
+#pragma unroll
+                for (int q = 0; q < VPT; ++q) {
+                    const double2 c = ct[SLOT ? q : 0];
+                    if (RC && !SLOT) {
+                        acc[j][q].x = fma(c.x, w0[j][q].x, acc[j][q].x);
+                        acc[j][q].y = fma(c.x, w0[j][q].y, acc[j][q].y);
+                    } else {
+                        acc[j][q] = cfma(c, w0[j][q], acc[j][q]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+#pragma unroll
+            for (int q = 0; q < VPT; ++q) {
+                const int r = r0 + q;
+                const int64_t e = int64_t(base | prog.jexp[j]) * R + r;
+                const double sc = a.sc[r];
+                const double2 hv = cscale(a.hsc ? a.hsc[r] : sc, acc[j][q]);
+                double2 out = hv;
+                if (!prog.first) {
+                    const double2 w0 = __ldcs(a.W + e);
+                    out.x += w0.x;
+                    out.y += w0.y;
+                } else if (a.P) {
+                    const double pc = a.pc[r];
+                    const double2 p = __ldcs(a.P + e);
+                    out.x = fma(pc, p.x, out.x);
+                    out.y = fma(pc, p.y, out.y);
+                }
+                __stcs(a.W + e, out);
+                const double2 vv = cscale(sc, s_v[(j * NS + l) * R + r]);
+                red[0][q] = cadd(red[0][q], cconjmul(vv, hv));
+                if (!prog.last) continue;
+                if (K >= 2) red[1][q].x += out.x * out.x + out.y * out.y;
+                if (K >= 4 && a.G) {
+                    const double2 gv = cscale(a.gsc[r], a.G[e]);
+                    red[2][q] = cadd(red[2][q], cconjmul(gv, out));
+                    red[3][q] = cadd(red[3][q], cconjmul(gv, vv));
+                }
+            }
+        }
+    }
+    block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
 }
 
 // Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by
@@ -503,9 +662,58 @@ static cudaError_t launch_hv_k(const pned_model *m, const HvArgs &a, int nblocks
     }
 }
 
+// Tile set of the multi-vector kernel for R (null: the flat kernel runs).
+static const pned_model::TileSet *find_rtiles(const pned_model *m, int R)
+{
+    if (R < 2) return nullptr;
+    std::lock_guard<std::mutex> lock(const_cast<pned_model *>(m)->rtiles_mu);
+    auto it = m->rtiles.find(R);
+    if (it == m->rtiles.end() || it->second.progs.empty()) return nullptr;
+    return &it->second;
+}
+
+template <int VPT, int SPT, bool SLOT, bool RC, bool RD, int K>
+static cudaError_t launch_rv_t(const pned_model *m, const pned_model::TileSet &ts, const HvArgs &a, int nblocks,
+                               cudaStream_t st)
+{
+    auto kern = hv_tile_rv_kernel<VPT, SPT, SLOT, RC, RD, K>;
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+    if (e != cudaSuccess) return e;
+    const int grid = tile_grid(m, nblocks);
+    const size_t smem = rtile_smem(m, a.R, SLOT);
+    HvArgs b = a;
+    for (size_t p = 0; p < ts.progs.size(); ++p) {
+        b.partials = a.partials + size_t(p) * grid * K * a.R;
+        kern<<<grid, kThreads, smem, st>>>(*ts.progs[p], b);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <int VPT, int SPT, int K>
+static cudaError_t launch_rv_k(const pned_model *m, const pned_model::TileSet &ts, const HvArgs &a, int nblocks,
+                               cudaStream_t st)
+{
+    if (a.slot_tables) return launch_rv_t<VPT, SPT, true, false, true, K>(m, ts, a, nblocks, st);
+    if (m->real_coef && m->real_diag) return launch_rv_t<VPT, SPT, false, true, true, K>(m, ts, a, nblocks, st);
+    if (m->real_diag) return launch_rv_t<VPT, SPT, false, false, true, K>(m, ts, a, nblocks, st);
+    return launch_rv_t<VPT, SPT, false, false, false, K>(m, ts, a, nblocks, st);
+}
+
+template <int K>
+static cudaError_t launch_rv(const pned_model *m, const pned_model::TileSet &ts, const HvArgs &a, int nblocks,
+                             cudaStream_t st)
+{
+    if (ts.vpt == 2 && ts.spt == 4) return launch_rv_k<2, 4, K>(m, ts, a, nblocks, st);
+    if (ts.vpt == 3 && ts.spt == 2) return launch_rv_k<3, 2, K>(m, ts, a, nblocks, st);
+    return cudaErrorInvalidValue;
+}
+
 int hv_partial_blocks(const pned_model *m, int R, int nblocks)
 {
     if (!m->tprogs.empty() && R == 1 && m->use_tile) return int(m->tprogs.size()) * tile_grid(m, nblocks);
+    if (const pned_model::TileSet *ts = find_rtiles(m, R)) return int(ts->progs.size()) * tile_grid(m, nblocks);
     return nblocks;
 }
 
@@ -515,6 +723,11 @@ cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStr
         if (a.K == 1) return launch_tile<1>(m, a, nblocks, st);
         if (a.K == 4) return launch_tile<4>(m, a, nblocks, st);
     }
+    if (const pned_model::TileSet *ts = find_rtiles(m, a.R)) {
+        if (a.K == 1) return launch_rv<1>(m, *ts, a, nblocks, st);
+        if (a.K == 4) return launch_rv<4>(m, *ts, a, nblocks, st);
+    }
+    if (a.slot_tables) return cudaErrorInvalidValue;
     switch (a.K) {
     case 1: return launch_hv_k<1>(m, a, nblocks, st);
     case 4: return launch_hv_k<4>(m, a, nblocks, st);
@@ -587,38 +800,106 @@ extern "C" int pned_set_device(int device)
 
 namespace pned {
 
+// Device programs of a tile plan (one per pass).
+static std::vector<std::unique_ptr<TileProgram>> tile_programs(const HostProgram &h2,
+                                                               const std::vector<HostProgram::TilePass> &passes,
+                                                               int ntab)
+{
+    std::vector<std::unique_ptr<TileProgram>> out;
+    for (size_t p = 0; p < passes.size(); ++p) {
+        const HostProgram::TilePass &ps = passes[p];
+        std::unique_ptr<TileProgram> T(new TileProgram());
+        T->n = h2.n;
+        T->tbits = ps.tbits;
+        T->jb = ps.jb;
+        T->nin = ps.nin;
+        T->nterms = int(ps.tterms.size());
+        T->ntab = ntab;
+        T->nouter = int(ps.outer.size());
+        T->first = p == 0;
+        T->last = p + 1 == passes.size();
+        for (int j = 0; j < (1 << ps.jb); ++j) {
+            uint32_t e = 0;
+            for (int k = 0; k < ps.jb; ++k) if ((j >> k) & 1) e |= 1u << ps.jpos[k];
+            T->jexp[j] = e;
+        }
+        for (int k = 0; k < T->nouter; ++k) T->outer[k] = uint8_t(ps.outer[k]);
+        for (int k = 0; k < 8; ++k) T->rowpos[k] = uint8_t(k < ps.tbits ? ps.rowpos[k] : 0);
+        T->ngroups = int(ps.gxor.size());
+        for (int g = 0; g <= T->ngroups; ++g) T->gstart[g] = uint16_t(ps.gstart[g]);
+        for (int g = 0; g < T->ngroups; ++g) T->gxor[g] = ps.gxor[g];
+        std::copy(ps.tterms.begin(), ps.tterms.end(), T->t);
+        out.push_back(std::move(T));
+    }
+    return out;
+}
+
 // Tiled single-vector programs (S = 1/2, n >= 12), one launch per pass.
 void build_tile_programs(pned_model *m)
 {
+    m->use_tile = false;
+    m->tprogs.clear();
     const HostProgram &hp = m->hp;
-    if (hp.q == 2 && hp.n >= 12 && plan_tiles(m->hp, 3, kTileWindowBits, kTileMaxPasses) == PNED_OK) {
-        const HostProgram &h2 = m->hp;
-        for (size_t p = 0; p < h2.passes.size(); ++p) {
-            const HostProgram::TilePass &ps = h2.passes[p];
-            std::unique_ptr<TileProgram> T(new TileProgram());
-            T->n = h2.n;
-            T->jb = ps.jb;
-            T->nin = ps.nin;
-            T->nterms = int(ps.tterms.size());
-            T->ntab = m->ntab;
-            T->nouter = int(ps.outer.size());
-            T->first = p == 0;
-            T->last = p + 1 == h2.passes.size();
-            for (int j = 0; j < (1 << ps.jb); ++j) {
-                uint32_t e = 0;
-                for (int k = 0; k < ps.jb; ++k) if ((j >> k) & 1) e |= 1u << ps.jpos[k];
-                T->jexp[j] = e;
-            }
-            for (int k = 0; k < T->nouter; ++k) T->outer[k] = uint8_t(ps.outer[k]);
-            T->ngroups = int(ps.gxor.size());
-            for (int g = 0; g <= T->ngroups; ++g) T->gstart[g] = uint16_t(ps.gstart[g]);
-            for (int g = 0; g < T->ngroups; ++g) T->gxor[g] = ps.gxor[g];
-            std::copy(ps.tterms.begin(), ps.tterms.end(), T->t);
-            m->tprogs.push_back(std::move(T));
-        }
+    std::vector<HostProgram::TilePass> passes;
+    const int fixed = m->plan1.row_fixed_bits >= 0 ? m->plan1.row_fixed_bits : 8;
+    const int window = m->plan1.window_bits >= 0 ? m->plan1.window_bits : kTileWindowBits;
+    const int mp = m->plan1.max_passes > 0 ? m->plan1.max_passes : kTileMaxPasses;
+    if (hp.q == 2 && hp.n >= 12 && plan_tiles(hp, 8, 3, fixed, window, mp, passes) == PNED_OK) {
+        m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << 3) + std::max(1, m->ntab));
         m->use_tile = true;
     }
+}
+
+// Tile shape of the multi-vector kernel: VPT vectors and SPT state rows per
+// thread (VPT * SPT <= 8 accumulators), G = R / VPT threads per state.
+static void rtile_shape(int R, int &vpt, int &spt)
+{
+    switch (R) {
+    case 3: case 6: case 12: vpt = 3; spt = 2; break;
+    default: vpt = 2; spt = 4; break;   // 2, 4, 8, 16
+    }
+}
+
+size_t rtile_smem(const pned_model *m, int R, bool slot_tables)
+{
+    int vpt, spt;
+    rtile_shape(R, vpt, spt);
+    const int G = R / vpt;
+    const size_t tile = size_t(kThreads / G) * spt * R;
+    return sizeof(double2) * (tile + size_t(std::max(1, m->ntab)) * (slot_tables ? R : 1));
+}
+
+bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan *plan)
+{
+    const HostProgram &hp = m->hp;
+    if (hp.q != 2 || hp.n < 12 || R < 2 || pick_vpt(R) == 0) return false;
+    if (rtile_smem(m, R, slot_tables) > 200 * 1024) return false;
+    std::lock_guard<std::mutex> lock(m->rtiles_mu);
+    if (m->rtiles.count(R) && !plan) return !m->rtiles[R].progs.empty();
+    pned_model::TileSet &ts = m->rtiles[R];
+    ts.progs.clear();
+    rtile_shape(R, ts.vpt, ts.spt);
+    const int G = R / ts.vpt;
+    int tbits = 8;
+    while ((1 << tbits) > kThreads / G) --tbits;
+    int jb = 0;
+    while ((1 << jb) < ts.spt) ++jb;
+    // L2 window: about 2^21 vector elements of R
+    int lr = 0;
+    while ((1 << lr) < R) ++lr;
+    int window = std::max(4, 21 - lr - tbits - jb);
+    int fixed = tbits;
+    int mp = kTileMaxPasses;
+    if (plan) {
+        if (plan->row_fixed_bits >= 0) fixed = std::min(tbits, plan->row_fixed_bits);
+        if (plan->window_bits >= 0) window = plan->window_bits;
+        if (plan->max_passes > 0) mp = std::min(kTileMaxPasses, plan->max_passes);
+    }
+    std::vector<HostProgram::TilePass> passes;
+    if (plan_tiles(hp, tbits, jb, fixed, window, mp, passes) != PNED_OK) return false;
+    ts.progs = tile_programs(hp, passes, m->ntab);
+    return true;
 }
 
 }  // namespace pned
@@ -709,14 +990,41 @@ extern "C" int pned_model_destroy(pned_model *m)
     return PNED_OK;
 }
 
-extern "C" int pned_model_plan(const pned_model *m, int *tile_passes, int *partner_tiles, int *tile_states)
+extern "C" int pned_model_plan(const pned_model *m, int R, int *tile_passes, int *partner_tiles, int *tile_states)
 {
-    if (!m) return fail(PNED_EINVAL, "pned_model_plan: null model");
-    int groups = 0;
-    for (const auto &t : m->tprogs) groups += t->ngroups;
-    if (tile_passes) *tile_passes = m->use_tile ? int(m->tprogs.size()) : 0;
-    if (partner_tiles) *partner_tiles = m->use_tile ? groups : 0;
-    if (tile_states) *tile_states = m->use_tile ? kThreads * (1 << 3) : 0;
+    if (!m || R < 1) return fail(PNED_EINVAL, "pned_model_plan: bad arguments");
+    int passes = 0, groups = 0, states = 0;
+    if (R == 1 && m->use_tile) {
+        passes = int(m->tprogs.size());
+        for (const auto &t : m->tprogs) groups += t->ngroups;
+        states = kThreads * (1 << 3);
+    } else if (R > 1) {
+        std::lock_guard<std::mutex> lock(const_cast<pned_model *>(m)->rtiles_mu);
+        auto it = m->rtiles.find(R);
+        if (it != m->rtiles.end() && !it->second.progs.empty()) {
+            passes = int(it->second.progs.size());
+            for (const auto &t : it->second.progs) groups += t->ngroups;
+            states = (1 << it->second.progs[0]->tbits) << it->second.progs[0]->jb;
+        }
+    }
+    if (tile_passes) *tile_passes = passes;
+    if (partner_tiles) *partner_tiles = groups;
+    if (tile_states) *tile_states = states;
+    return PNED_OK;
+}
+
+extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan)
+{
+    if (!m || pick_vpt(R) == 0) return fail(PNED_EINVAL, "pned_model_set_plan: bad arguments");
+    if (plan && (plan->max_passes > kTileMaxPasses || plan->window_bits > 30 || plan->row_fixed_bits > 8))
+        return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
+    if (R == 1) {
+        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1};
+        build_tile_programs(m);
+        return PNED_OK;
+    }
+    const pned_tile_plan def{-1, -1, -1};
+    ensure_rtiles(m, R, false, plan ? plan : &def);
     return PNED_OK;
 }
 
@@ -771,7 +1079,9 @@ extern "C" int pned_ctx_create(pned_model *m, int R, size_t budget, pned_ctx **o
     e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
     c->stream = c->own_stream;
-    const size_t pbytes = sizeof(double2) * size_t(c->nblocks) * kMaxK * kMaxR;
+    // tiled kernels write one partial sum per block and pass
+    if (R > 1) ensure_rtiles(m, R, false, nullptr);
+    const size_t pbytes = sizeof(double2) * size_t(c->nblocks) * kTileMaxPasses * kMaxK * kMaxR;
     e = cudaMalloc(&c->partials, pbytes);
     if (e == cudaSuccess) e = cudaMalloc(&c->sums, sizeof(double2) * kMaxK * kMaxR * 4);
     if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(double) * kScalSlots * kMaxR);

@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "kernels.cuh"
@@ -20,6 +22,14 @@ struct pned_model {
     std::vector<std::unique_ptr<pned::TileProgram>> tprogs;   // tiled single-vector passes (q == 2)
     size_t tile_smem = 0;
     bool use_tile = false;   // single-vector H.v uses the tiled kernel
+    // tiled multi-vector passes per R (q == 2): VPT vectors and SPT rows per thread
+    struct TileSet {
+        std::vector<std::unique_ptr<pned::TileProgram>> progs;
+        int vpt = 0, spt = 0;
+    };
+    std::map<int, TileSet> rtiles;
+    std::mutex rtiles_mu;
+    pned_tile_plan plan1{-1, -1, -1};   // single-vector plan parameters (-1: defaults)
     int nsm = 148;
     double2 *d_table = nullptr;
     void *d_diag = nullptr;
@@ -97,6 +107,12 @@ cudaError_t allow_dynamic_smem(const void *kern, int device);
 int current_device();
 // Plans the tiled single-vector passes of m->hp (S = 1/2, n >= 12) and sets m->use_tile.
 void build_tile_programs(pned_model *m);
+// Plans the tiled multi-vector passes for R vectors (S = 1/2, n >= 12, R > 1),
+// once per model and R (again when `plan` is given); returns false when the
+// flat kernel is used instead.
+bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan *plan);
+// Shared memory of the tiled multi-vector kernel for R vectors.
+size_t rtile_smem(const pned_model *m, int R, bool slot_tables);
 // Number of partial-sum blocks launch_hv writes for this model, R and grid.
 int hv_partial_blocks(const pned_model *m, int R, int nblocks);
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);

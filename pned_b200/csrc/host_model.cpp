@@ -463,32 +463,60 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
 // ---------------------------------------------------------------------------
 namespace {
 
-// Tile j-bits (greedy: most masks made in-tile) and outer order (bits most used
-// by out-of-tile masks first) for a set of masks.
-void choose_tile(const std::vector<uint32_t> &masks, int n, int jb, std::vector<int> &jpos, std::vector<int> &outer,
-                 uint32_t &tilemask)
+// Partner tiles a set of masks needs with tile bits `tm`: distinct out-of-tile parts.
+int count_groups(const std::vector<uint32_t> &masks, uint32_t tm)
 {
-    tilemask = 0xffu;
-    jpos.clear();
-    for (int k = 0; k < jb; ++k) {
-        int best = -1, bestc = -1;
-        for (int b = 8; b < n; ++b) {
+    std::vector<uint32_t> parts;
+    for (uint32_t m : masks)
+        if (m & ~tm) parts.push_back(m & ~tm);
+    std::sort(parts.begin(), parts.end());
+    return int(std::unique(parts.begin(), parts.end()) - parts.begin());
+}
+
+// Tile bits for a set of masks: the `fixed` low bits, then tbits + jb - fixed
+// bits chosen to minimise the partner tiles (greedy, then pairwise exchanges
+// while they help); rows take the fixed bits and the lowest chosen ones, the
+// j bits the rest.  Outer order: bits most used by out-of-tile masks first.
+void choose_tile(const std::vector<uint32_t> &masks, int n, int tbits, int jb, int fixed, std::vector<int> &rowpos,
+                 std::vector<int> &jpos, std::vector<int> &outer, uint32_t &tilemask)
+{
+    const int target = tbits + jb;
+    tilemask = (1u << fixed) - 1u;
+    auto usage = [&](int b) {
+        int u = 0;
+        for (uint32_t m : masks) if (m & (1u << b)) ++u;
+        return u;
+    };
+    for (int k = fixed; k < target; ++k) {
+        int best = -1, bestg = 1 << 30, bestu = -1;
+        for (int b = fixed; b < n; ++b) {
             if (tilemask & (1u << b)) continue;
-            const uint32_t tm = tilemask | (1u << b);
-            int cnt = 0, use = 0;
-            for (uint32_t m : masks) {
-                if ((m & ~tm) == 0) ++cnt;
-                if (m & (1u << b)) ++use;
-            }
-            const int score = cnt * 64 + use;
-            if (score > bestc) { bestc = score; best = b; }
+            const int g = count_groups(masks, tilemask | (1u << b));
+            const int u = usage(b);
+            if (g < bestg || (g == bestg && u > bestu)) { bestg = g; bestu = u; best = b; }
         }
-        jpos.push_back(best);
         tilemask |= 1u << best;
     }
-    std::sort(jpos.begin(), jpos.end());
+    int g = count_groups(masks, tilemask);
+    for (int round = 0; round < 16; ++round) {
+        bool better = false;
+        for (int a = fixed; a < n && !better; ++a) {
+            if (!(tilemask & (1u << a))) continue;
+            for (int b = fixed; b < n; ++b) {
+                if (tilemask & (1u << b)) continue;
+                const uint32_t t2 = (tilemask & ~(1u << a)) | (1u << b);
+                const int g2 = count_groups(masks, t2);
+                if (g2 < g) { tilemask = t2; g = g2; better = true; break; }
+            }
+        }
+        if (!better) break;
+    }
+    std::vector<int> chosen;
+    for (int b = 0; b < n; ++b) if (tilemask & (1u << b)) chosen.push_back(b);
+    rowpos.assign(chosen.begin(), chosen.begin() + tbits);
+    jpos.assign(chosen.begin() + tbits, chosen.end());
     std::vector<std::pair<int, int>> ob;
-    for (int b = 8; b < n; ++b) {
+    for (int b = 0; b < n; ++b) {
         if (tilemask & (1u << b)) continue;
         int use = 0;
         for (uint32_t m : masks) if ((m & ~tilemask) && (m & (1u << b))) ++use;
@@ -501,23 +529,26 @@ void choose_tile(const std::vector<uint32_t> &masks, int n, int jb, std::vector<
 
 }  // namespace
 
-int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
+int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bits, int max_passes,
+               std::vector<HostProgram::TilePass> &passes)
 {
-    if (P.q != 2 || jb < 1 || jb > kTileMaxJB || P.n < 8 + jb + 1) return PNED_ENOTSUP;
+    if (P.q != 2 || jb < 0 || jb > kTileMaxJB || tbits < 1 || tbits > 8 || fixed < 0 || fixed > tbits ||
+        P.n < tbits + jb + 1)
+        return PNED_ENOTSUP;
     const int n = P.n;
     std::vector<int> remaining(P.xterms.size());
     for (size_t i = 0; i < remaining.size(); ++i) remaining[i] = int(i);
-    P.passes.clear();
+    passes.clear();
     while (!remaining.empty()) {
         std::vector<uint32_t> rm;
         for (int i : remaining) rm.push_back(P.xterms[i].xmask);
-        std::vector<int> jpos, outer;
+        std::vector<int> rowpos, jpos, outer;
         uint32_t tilemask;
-        choose_tile(rm, n, jb, jpos, outer, tilemask);
+        choose_tile(rm, n, tbits, jb, fixed, rowpos, jpos, outer, tilemask);
         uint32_t nearmask = tilemask;
         for (int k = 0; k < window_bits && k < int(outer.size()); ++k) nearmask |= 1u << outer[k];
         std::vector<int> take, rest;
-        const bool last = int(P.passes.size()) + 1 >= max_passes;
+        const bool last = int(passes.size()) + 1 >= max_passes;
         for (int i : remaining) {
             if (last || (P.xterms[i].xmask & ~nearmask) == 0) take.push_back(i);
             else rest.push_back(i);
@@ -526,14 +557,17 @@ int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
         // re-plan the tile for the masks of this pass only
         std::vector<uint32_t> tm;
         for (int i : take) tm.push_back(P.xterms[i].xmask);
-        choose_tile(tm, n, jb, jpos, outer, tilemask);
+        choose_tile(tm, n, tbits, jb, fixed, rowpos, jpos, outer, tilemask);
         HostProgram::TilePass pass;
+        pass.tbits = tbits;
         pass.jb = jb;
+        pass.rowpos = rowpos;
         for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
         pass.outer = outer;
         auto local = [&](uint32_t m) {
-            uint32_t l = m & 0xffu;
-            for (int k = 0; k < jb; ++k) if (m & (1u << jpos[k])) l |= 1u << (8 + k);
+            uint32_t l = 0;
+            for (int k = 0; k < tbits; ++k) if (m & (1u << rowpos[k])) l |= 1u << k;
+            for (int k = 0; k < jb; ++k) if (m & (1u << jpos[k])) l |= 1u << (tbits + k);
             return l;
         };
         std::vector<TileTerm> in;
@@ -580,19 +614,21 @@ int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes)
         }
         pass.gstart.push_back(int(pass.tterms.size()));
         if (int(pass.gxor.size()) > kTileMaxGroups) return PNED_ENOTSUP;
-        P.passes.push_back(pass);
+        passes.push_back(pass);
         remaining = rest;
     }
-    if (P.passes.empty()) {   // diagonal-only model: one pass with no terms
+    if (passes.empty()) {   // diagonal-only model: one pass with no terms
         HostProgram::TilePass pass;
+        pass.tbits = tbits;
         pass.jb = jb;
-        std::vector<int> jpos, outer;
+        std::vector<int> rowpos, jpos, outer;
         uint32_t tilemask;
-        choose_tile({}, n, jb, jpos, outer, tilemask);
+        choose_tile({}, n, tbits, jb, fixed, rowpos, jpos, outer, tilemask);
+        pass.rowpos = rowpos;
         for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
         pass.outer = outer;
         pass.gstart.push_back(0);
-        P.passes.push_back(pass);
+        passes.push_back(pass);
     }
     return PNED_OK;
 }

@@ -52,9 +52,10 @@ struct RadixProgram {
 
 // Tiled single-vector S = 1/2 program (see TileTerm).
 struct TileProgram {
-    int n, jb, nin, nterms, ntab, nouter;
+    int n, tbits, jb, nin, nterms, ntab, nouter;
     int first, last;                  // pass flags: first adds diagonal and P, last forms the K >= 2 sums
     uint32_t jexp[1 << kTileMaxJB];   // global bits of the thread's j-th state
+    uint8_t rowpos[8];                // row bit k -> global bit rowpos[k]
     uint8_t outer[32];                // tile-id bit k -> global bit outer[k]
     int ngroups;                      // out-of-tile groups, one partner tile each
     uint16_t gstart[kTileMaxGroups + 1];
@@ -83,6 +84,9 @@ struct HvArgs {
     // (null: sc) and an extra diagonal shift (null: none)
     const double *hsc;
     const double *shiftv;
+    // tiled multi-vector kernel only: per-vector coefficient tables ([ntab][R])
+    // and real diagonals ([dim][R]) instead of shared ones
+    int slot_tables;
 };
 
 }  // namespace pned

@@ -78,6 +78,8 @@ struct HostProgram {
     std::vector<cd> dtab;                // [nbond][Q]
     // tiled program (q == 2): one or more passes, each with its own tile plan
     struct TilePass {
+        int tbits = 8;                   // row bits of a tile (state rows of the thread index)
+        std::vector<int> rowpos;         // global bit of row bit k (k < tbits)
         int jb = 0;
         int jpos[kTileMaxJB] = {0, 0, 0};
         std::vector<int> outer;          // outer bit positions, fastest first
@@ -86,14 +88,19 @@ struct HostProgram {
         std::vector<int> gstart;         // out-of-tile group g: terms gstart[g] .. gstart[g+1]-1
         std::vector<uint32_t> gxor;      // partner tile of group g: outer bits flipped by gxor[g]
     };
-    std::vector<TilePass> passes;
 };
 
-// Splits the flip masks into passes for the tiled kernel (q == 2,
-// n >= 8 + jb + 1): each pass takes the masks whose partner tiles lie within
-// `window_bits` outer bits of its own tile order (so they are found in L2),
-// the last pass takes what is left.
-int plan_tiles(HostProgram &P, int jb, int window_bits, int max_passes);
+// Splits the flip masks into passes for the tiled kernels (q == 2,
+// n >= tbits + jb + 1).  A tile holds the states that agree on all bits but
+// its tbits row bits and jb j bits, chosen per pass to minimise the partner
+// tiles; the row bits include the global bits 0..fixed-1, so that a warp's
+// loads come in contiguous segments.  Each pass takes the masks whose partner
+// tiles lie within `window_bits` outer bits of its own tile order (so they are
+// found in L2), the last pass takes what is left.  In-tile terms carry the
+// local xor (row bits, then the j bits from bit tbits); out-of-tile terms the
+// global one.
+int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bits, int max_passes,
+               std::vector<HostProgram::TilePass> &out);
 
 // Coefficient tables and diagonal tables of `d` evaluated on the term
 // structure of S (same lattice and bonds; q == 2): table[i] for the entries of

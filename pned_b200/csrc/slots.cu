@@ -393,12 +393,13 @@ cudaError_t slot_step(pned_slots *S)
     if (S->tile) {
         HvArgs a{};
         a.C = C; a.P = P; a.W = W; a.G = P;
-        a.sc = S->cf + kCfSc; a.pc = S->cf + kCfPc; a.gsc = S->cf + kCfGsc;
-        a.hsc = S->cf + kCfHsc; a.shiftv = S->cf + kCfShift;
+        a.sc = S->cf + kCfSc * R; a.pc = S->cf + kCfPc * R; a.gsc = S->cf + kCfGsc * R;
+        a.hsc = S->cf + kCfHsc * R; a.shiftv = S->cf + kCfShift * R;
         a.diag = S->diag; a.shift = 0.0; a.table = S->table;
-        a.partials = S->partials; a.dim = S->dim; a.R = 1; a.K = 4;
+        a.partials = S->partials; a.dim = S->dim; a.R = R; a.K = 4;
+        a.slot_tables = R > 1;
         e = launch_hv(&S->tm, a, S->nblocks, S->stream);
-        nb_hv = hv_partial_blocks(&S->tm, 1, S->nblocks);
+        nb_hv = hv_partial_blocks(&S->tm, R, S->nblocks);
     } else {
         SlotHvArgs a{};
         a.C = C; a.P = P; a.W = W;
@@ -609,7 +610,7 @@ extern "C" int pned_slots_create(const pned_model_desc *structure, int R, int ma
     if (e == cudaSuccess) e = salloc(S.get(), &S->hist_b, size_t(R) * max_steps);
     if (e == cudaSuccess) e = salloc(S.get(), &S->coef, size_t(R) * max_steps * 5);
     if (e == cudaSuccess) e = salloc(S.get(), &S->vcoef, size_t(R) * max_steps);
-    if (e == cudaSuccess) e = salloc(S.get(), &S->partials, size_t(S->nblocks) * 4 * kMaxR);
+    if (e == cudaSuccess) e = salloc(S.get(), &S->partials, size_t(S->nblocks) * kTileMaxPasses * kMaxK * kMaxR);
     if (e == cudaSuccess) e = salloc(S.get(), &S->sums, size_t(12) * kMaxR);
     if (e == cudaSuccess) e = salloc(S.get(), &S->scratch, size_t(R) * 64 + size_t(R) * S->nbond * 4);
     if (e == cudaSuccess) e = cudaMemcpy(S->s1, hp.dsite1.data(), sizeof(int) * S->nbond, cudaMemcpyHostToDevice);
@@ -627,19 +628,20 @@ extern "C" int pned_slots_create(const pned_model_desc *structure, int R, int ma
         slots_free(S.get());
         return cuda_fail(e, "pned_slots_create");
     }
-    if (R == 1) {
+    {
+        // the batch's table ([ntab][R]) and diagonal ([dim][R]) drive the tiled
+        // kernels through a model that borrows them
         pned_model &m = S->tm;
         m.hp = S->hp;
         m.device = S->device; m.n = S->n; m.q = 2; m.nbond = S->nbond; m.dim = S->dim;
         m.real_coef = false; m.real_diag = true;
         m.ntab = S->ntab; m.nterms = S->xprog->nterms; m.nsm = S->nsm;
         m.d_table = S->table; m.d_diag = S->diag;
-        build_tile_programs(&m);
-        S->tile = m.use_tile;
-        // the tiled passes write more partial sums than the flat grid
-        if (S->tile && size_t(hv_partial_blocks(&m, 1, S->nblocks)) * 4 > size_t(S->nblocks) * 4 * kMaxR) {
-            slots_free(S.get());
-            return fail(PNED_ENOTSUP, "pned_slots_create: tiled partial sums exceed the scratch");
+        if (R == 1) {
+            build_tile_programs(&m);
+            S->tile = m.use_tile;
+        } else {
+            S->tile = ensure_rtiles(&m, R, true, nullptr);
         }
     }
     *out = S.release();
@@ -823,4 +825,38 @@ extern "C" int pned_gaussian_column(int64_t dim, int R, int r, uint64_t seed, pn
         splitmix64_host(seed ^ 0x5DEECE66Dull), dim, R, r, reinterpret_cast<double2 *>(v_dev));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_gaussian_column");
+}
+
+extern "C" int pned_slots_set_plan(pned_slots *S, const pned_tile_plan *plan)
+{
+    if (!S) return fail(PNED_EINVAL, "pned_slots_set_plan: null slot batch");
+    if (!S->tile) return PNED_OK;   // the flat kernel runs: nothing to plan
+    cudaSetDevice(S->device);
+    cudaError_t e = cudaStreamSynchronize(S->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_slots_set_plan");
+    if (S->graph) {   // the captured steps hold the old plan
+        cudaGraphExecDestroy(S->graph);
+        S->graph = nullptr;
+    }
+    const pned_tile_plan def{-1, -1, -1};
+    if (S->R == 1) {
+        S->tm.plan1 = plan ? *plan : def;
+        build_tile_programs(&S->tm);
+        S->tile = S->tm.use_tile;
+    } else {
+        S->tile = ensure_rtiles(&S->tm, S->R, true, plan ? plan : &def);
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_slots_plan(const pned_slots *S, int *tile_passes, int *partner_tiles, int *tile_states)
+{
+    if (!S) return fail(PNED_EINVAL, "pned_slots_plan: null slot batch");
+    if (!S->tile) {
+        if (tile_passes) *tile_passes = 0;
+        if (partner_tiles) *partner_tiles = 0;
+        if (tile_states) *tile_states = 0;
+        return PNED_OK;
+    }
+    return pned_model_plan(&S->tm, S->R, tile_passes, partner_tiles, tile_states);
 }

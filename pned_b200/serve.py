@@ -167,14 +167,18 @@ def dsf_spectra(result: dict, i_range: int = 2000, omega_max: float = 3.0, eta: 
 class GpuLane:
     """Slot batch of one lattice size on its own CUDA stream."""
 
-    def __init__(self, n: int, R: int, max_steps: int, budget: int = 0, n_vectors: int = 1):
+    def __init__(self, n: int, R: int, max_steps: int, budget: int = 0, n_vectors: int = 1, tune: bool = True):
         import torch
         self.torch = torch
         self.n = n
         self.cluster = cluster_for_sites(n)
         self.stream = torch.cuda.Stream()
-        self.batch = api.SlotBatch(api.ModelInput.structure(self.cluster), R, max_steps, hbm_budget=budget,
-                                   stream=self.stream)
+        structure = api.ModelInput.structure(self.cluster)
+        self.batch = api.SlotBatch(structure, R, max_steps, hbm_budget=budget, stream=self.stream)
+        self.tuning = None
+        if tune:
+            from .tune import autotune_slots
+            self.tuning = autotune_slots(self.batch, structure)
         self.R, self.dim = self.batch.R, self.batch.dim
         with torch.cuda.stream(self.stream):
             self.tmp = torch.empty(self.dim, dtype=torch.complex128, device="cuda")
