@@ -187,6 +187,10 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     model, cl = build_model(args.n_sites)
     D = model.dim
+    tuning = None
+    if args.tune:
+        from pned_b200.tune import autotune
+        tuning = autotune(model, 1)
     stream = torch.cuda.Stream(device=dev)
     ctx = P.Context(model, R=1, stream=stream)   # every kernel of the context runs on `stream`
     v = torch.empty(D, dtype=torch.complex128, device=dev)
@@ -265,6 +269,9 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "e2e": e2e,
     }
+    if tuning is not None:
+        line["roofline"]["tuned_plan"] = {"row_fixed_bits": tuning["plan"][0], "window_bits": tuning["plan"][1],
+                                          "max_passes": tuning["plan"][2], "candidates": len(tuning.get("tried", []))}
     if rank == 0 and args.cpu_baseline:
         try:
             cs = CpuSample(args.n_sites, os.cpu_count() or 1, slice_log2=args.ref_slice_log2)
@@ -275,8 +282,182 @@ def run_ours(args, rank, world, local_rank):
             del cs
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
+    if args.batched:
+        del v
+        ctx.close()
+        model.close()
+        torch.cuda.empty_cache()
+        line["batched"] = {"tpq": batched_tpq(dev, args), "dsf": batched_dsf(dev, args)}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _kh(gamma=0.0):
+    from pned_b200 import couplings as CP
+    return CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi), gamma=gamma)
+
+
+def _timed_session(ctx, st, kind, v, warm, steps, L=0.0):
+    """Times `steps` session steps on the context's stream `st` (CUDA events)."""
+    import torch
+    ctx.session_begin(kind, v, warm + steps + 1, L=L)
+    ctx.session_step(warm)
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    ctx.session_step(steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    res = ctx.session_read()
+    ctx.session_end()
+    return e0.elapsed_time(e1) / steps, res
+
+
+def batched_tpq(dev, args):
+    """mTPQ with R = 16 vectors, S=1/2 N=24 honeycomb (3x4), KH + Gamma 0.1 + h 0.05 [111], l = 2:
+    batched steps against the same vectors advanced one at a time."""
+    import torch
+    import pned_b200 as P
+    from pned_b200 import couplings as CP
+    from pned_b200.lattice import cluster_for_sites
+    from pned_b200.tune import autotune
+    cl = cluster_for_sites(24)
+    L = 2.0 * cl.n
+    m = P.Model.from_couplings(cl, _kh(0.1), field=CP.field_111(0.05), tps_L=L)
+    out = {"workload": "mTPQ R=16, S=1/2 KH+Gamma=0.1+h=0.05[111] honeycomb N=24 (3x4), D=2^24, l=2.0 (L=48), "
+                       "complex128, interleaved [2^24][16]", "steps_timed": args.batch_steps}
+    for R in (16, 1):
+        autotune(m, R)
+        st = torch.cuda.Stream(device=dev)
+        ctx = P.Context(m, R=R, stream=st)
+        v = torch.empty(m.dim * R, dtype=torch.complex128, device=dev)
+        ctx.fill_gaussian(SEED, v)
+        ms, res = _timed_session(ctx, st, "tps", v, 3, args.batch_steps, L=L)
+        if R == 16:
+            out.update(ms_per_step=ms, steps_per_s=1000.0 / ms, vector_steps_per_s=16000.0 / ms,
+                       plan=m.plan(16))
+            # E(T) of the first step, averaged over R (coefficient 3 of eval_phys_val: L - alpha1)
+            out["energy_first_step_mean"] = float(res["coef"][0, :, 3].mean())
+        else:
+            out.update(plain_ms_per_vector_step=ms, plain_vector_steps_per_s=1000.0 / ms)
+        ctx.close()
+        del v
+        torch.cuda.empty_cache()
+    out["vs_plain"] = out["vector_steps_per_s"] / out["plain_vector_steps_per_s"]
+    m.close()
+    return out
+
+
+def batched_dsf(dev, args):
+    """DSF: ground state of the N=24 KH cluster, S^z_q at all 12 momenta, 150-step
+    chains for the 12 q in one batched run against one momentum at a time."""
+    import numpy as np
+    import torch
+    import pned_b200 as P
+    from pned_b200.lattice import cluster_for_sites
+    from pned_b200.tune import autotune
+    cl = cluster_for_sites(24)
+    m = P.Model.from_couplings(cl, _kh())
+    ctx1 = P.Context(m, R=1)
+    v = torch.empty(m.dim, dtype=torch.complex128, device=dev)
+    ctx1.fill_gaussian(SEED, v)
+    gs_steps = 120
+    r = ctx1.lanczos(v, gs_steps)
+    a, b = r["alpha"][:, 0], r["beta"][:, 0]
+    E = P.bisec(a, b, gs_steps, 1)
+    c = P.vec12(a, b, E, gs_steps, 1)[0]
+    x = ctx1.lanczos_vector(v, a, b, c)
+    nq = len(cl.q_list)
+    qrs = np.stack([cl.qr(i) for i in range(nq)])
+    steps = 150
+    out = {"workload": f"DSF S^z_q chains, {nq} momenta of the N=24 KH honeycomb (3x4), 150 steps each, "
+                       "from the Lanczos ground state; S(q,w) on 2000 w in [0,3], eta=0.05",
+           "e0": float(E[0]), "momenta": nq}
+    autotune(m, nq)
+    ctxq = P.Context(m, R=nq)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d = ctxq.dsf(x, qrs, steps)
+    t1 = time.perf_counter()
+    out.update(batched_s=t1 - t0, chains_per_s=nq / (t1 - t0), plan=m.plan(nq))
+    sp = [P.exec_renbun(2000, steps + 2, 3.0 / 1999, float(E[0]), 0.05, d["salpha"][:, i], d["sbeta"][:, i])[2]
+          for i in range(nq)]
+    out["spectral_weight_q0"] = float(np.sum(sp[0]) * 3.0 / 1999)
+    ctxq.close()
+    t0 = time.perf_counter()
+    d1 = ctx1.dsf(x, qrs[:1], steps)
+    t1 = time.perf_counter()
+    out.update(plain_chain_s=t1 - t0, plain_chains_per_s=1.0 / (t1 - t0))
+    out["vs_plain"] = out["chains_per_s"] / out["plain_chains_per_s"]
+    out["max_rel_diff_alpha_q0"] = float(np.max(np.abs(d1["salpha"][:12, 0] - d["salpha"][:12, 0]) /
+                                                np.abs(d["salpha"][:12, 0])))
+    ctx1.close()
+    m.close()
+    del x, v
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_serve(args, rank, world, local_rank):
+    """Serving stream (continuous batching) against the plain one-at-a-time path."""
+    import numpy as np
+    import torch
+    import pned_b200 as P
+    from pned_b200 import serve
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    P.lib().pned_set_device(local_rank)
+    reqs = serve.make_stream(args.requests, rate=args.rate, seed=SEED, p30=args.p30)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(0.85 * free)
+    # capacity: the whole stream queued at once, drained as fast as the loop can
+    cap_reqs = [serve.Request(**{**q.__dict__, "arrival": 0.0}) for q in reqs]
+    srv = serve.Server(budget=budget, max_steps=512)
+    with ClockSampler(local_rank) as clk:
+        cap = srv.run(cap_reqs, realtime=True)
+        # latency: Poisson arrivals at `rate`
+        st = srv.run(reqs, realtime=True)
+    srv.close()
+    torch.cuda.empty_cache()
+    capacity = len(cap.results) / cap.makespan_s
+    s = serve.summarize(st, reqs)
+    by = {r["rid"]: r for r in cap.results}
+    k = min(len(reqs), args.plain_sample)
+    tp, diffs = 0.0, []
+    for q in reqs[:k]:
+        t0 = time.perf_counter()
+        p = serve.run_plain(q)
+        tp += time.perf_counter() - t0
+        if "e0" in p:
+            diffs.append(abs(by[q.rid]["e0"] - p["e0"]) / abs(p["e0"]))
+    plain = k / tp
+    kinds = {kd: sum(1 for q in reqs if q.kind == kd) for kd in ("lanczos", "tpq", "dsf")}
+    line = {
+        "metric": "served_solves_per_s", "value": capacity, "unit": "solves/s", "n_gpus": 1,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic request stream (seeded)",
+        "config": {"workload": "Poisson stream of Lanczos E0 (300 steps), mTPQ (R=4, 500 steps), DSF (4 momenta, "
+                               "100 steps) requests, S=1/2 honeycomb N in {18..26} uniform + p30 at N=30, "
+                               "random phi, Gamma, h[111]; HBM-budget admission, co-batching by N",
+                   "requests": len(reqs), "rate_per_s": args.rate, "p30": args.p30, "kinds": kinds,
+                   "hbm_budget_bytes": budget},
+        "capacity": {"solves_per_s": capacity, "makespan_s": cap.makespan_s, "lanes_created": cap.lanes_created,
+                     "slot_occupancy": cap.occupied_slot_steps / max(1, cap.slot_steps),
+                     "peak_bytes": cap.peak_bytes, "note": "all requests queued at t=0"},
+        "latency": {"rate_per_s": args.rate, "solves_per_s": s["solves_per_s"], "p50_s": s["p50_latency_s"],
+                    "p99_s": s["p99_latency_s"], "makespan_s": s["makespan_s"]},
+        "p50_latency_s": s["p50_latency_s"], "p99_latency_s": s["p99_latency_s"],
+        "plain": {"solves_per_s": plain, "sample": k, "mean_s": tp / k,
+                  "max_rel_e0_diff_served_vs_plain": max(diffs) if diffs else None},
+        "vs_plain": capacity / plain,
+        "clocks": clk.summary(),
+        "e2e": {"value": s["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "requests enter and results leave through host memory; start vectors are generated "
+                        "on the device from each request's seed"},
+    }
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -291,6 +472,14 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
+    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve"])
+    ap.add_argument("--no-tune", dest="tune", action="store_false")
+    ap.add_argument("--no-batched", dest="batched", action="store_false")
+    ap.add_argument("--batch-steps", type=int, default=40)
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--p30", type=float, default=0.02)
+    ap.add_argument("--plain-sample", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -307,6 +496,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "serve":
+            run_serve(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -405,6 +405,34 @@ int pned_exec_renbun(int i_range, int s_maxitr, double split, double ene, double
 /* nomalization_DSF (S1/2 DSF.f90:337-351) */
 int pned_normalize_dsf(int i_range, double split, double sq_re, double *dsf);
 
+/* ------------------------------------------------------------------------ */
+/* output chain of mTPQ runs                                                 */
+/* ------------------------------------------------------------------------ */
+/*
+ * The TPQ coefficient file SalphaSbeta_me%05dseed%05d<comp> (dump_alpha_beta_coef,
+ * S1/2 TPS.f90:507-538): Fortran unformatted sequential, five records --
+ * num_data1 (int32), num_data2 (int32), alpha[num_data1], beta[num_data1],
+ * coef[num_data2][num_data1] (column-major coef(k, m)) -- each framed by its
+ * 4-byte length.  The reader returns the sizes; with alpha, beta and coef
+ * non-NULL (capacity1 >= num_data1, coef room for num_data1 * num_data2)
+ * it also fills them.
+ */
+int pned_write_salphasbeta(const char *path, int num_data1, int num_data2, const double *alpha, const double *beta,
+                           const double *coef);
+int pned_read_salphasbeta(const char *path, int *num_data1, int *num_data2, double *alpha, double *beta,
+                          double *coef, int capacity1);
+/*
+ * eval_mpi (S1/2 eval_mpi.f90:236-363, 395-440): canonical averages of n_seeds
+ * mTPQ runs on num_div + 1 temperatures log-spaced in [t_min, t_max].  Per
+ * seed s (arrays [n_seeds][num_data1]): beta = the TPS norms, energy =
+ * coef(:,4) = L - alpha1, hmix = coef(:,5) = Re<k-1|H|k>.  out[num_div+1][5]:
+ * T, E(T) (seed mean), C(T) = dE/dT by the centred difference at
+ * T +- t_delta (t_delta = 1e-4, or 0.9 t_min below that), the seed variance
+ * of E averaged over T +- t_delta, and d2E/dT2.
+ */
+int pned_tpq_thermo(int num_data1, int n_seeds, const double *beta, const double *energy, const double *hmix,
+                    double t_min, double t_max, int num_div, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -337,3 +337,71 @@ class Model:
         lib().oracle_inverse_iteration(self._h, E, _p(bw), _p(x), inv_max, cg_max, C.byref(ni),
                                        C.byref(nc))
         return x, ni.value, nc.value
+
+
+# --------------------------------------------------------------------------- mTPQ output chain (numpy)
+
+def tpq_thermo(beta, energy, hmix, t_min, t_max, num_div):
+    """eval_mpi restated in numpy/Python loops (S_one_half/Hybrid_TPS_eval_mpi.f90:
+    calc_fac :236-281, eval_q :284-313, lsort :315-347, calc_ave :349-363, main
+    loop :395-430); arrays [n_seeds][num_data1]; returns [num_div+1][5]:
+    T, E(T), dE/dT, variance, d2E/dT2."""
+    import math
+    beta = np.atleast_2d(np.asarray(beta, dtype=np.float64))
+    energy = np.atleast_2d(np.asarray(energy, dtype=np.float64))
+    hmix = np.atleast_2d(np.asarray(hmix, dtype=np.float64))
+    nseed, nd1 = beta.shape
+
+    def calc_fac(bt, b):
+        fac1 = [0.0] * (nd1 + 1)
+        fac2 = [0.0] * (nd1 + 1)
+        y, maxfac = 0.0, -1e200
+        for i in range(1, 2 * (nd1 - 1) + 1):
+            m = ((i + 1) >> 1) + 1
+            arg = bt / (2 * i) * b[m - 1]
+            y += math.log(arg) if arg > 0 else -math.inf
+            fac1[m] = y
+            maxfac = max(y, maxfac)
+        for i in range(1, nd1):
+            fac1[i] = math.exp(fac1[i] - maxfac)
+            fac2[i] = fac1[i] * bt * b[i] / (2 * i - 1)
+        fac1[nd1] = math.exp(fac1[nd1] - maxfac)
+        return fac1, fac2
+
+    def eval_q(bt, s):
+        fac1, fac2 = calc_fac(bt, beta[s])
+        t1 = [fac1[i] * energy[s][i - 1] for i in range(1, nd1)]
+        t2 = [fac2[i] * hmix[s][i - 1] for i in range(1, nd1)]
+        z = 0.0
+        for i in range(1, nd1):
+            z = z + fac1[i] + fac2[i]
+        x = 0.0
+        for v in sorted(t1, reverse=True):
+            x += v
+        y = 0.0
+        for v in sorted(t2, reverse=True):
+            y += v
+        return (x + y) / z
+
+    lmin, lmax = math.log(t_min), math.log(t_max)
+    delta = (lmax - lmin) / num_div
+    t_delta = 1e-4 if t_min >= 1e-4 else t_min * 0.9
+    out = np.zeros((num_div + 1, 5))
+    for i1 in range(num_div + 1):
+        t0 = math.exp(lmin + i1 * delta)
+        dat = [0.0] * 9
+        for i2, bt in enumerate((1.0 / (t0 - t_delta), 1.0 / t0, 1.0 / (t0 + t_delta))):
+            tmp = [eval_q(bt, s) for s in range(nseed)]
+            ave = 0.0
+            var = 0.0
+            for v in tmp:
+                ave += v
+                var += v * v
+            ave /= nseed
+            var = var / nseed - ave * ave
+            dat[3 * i2:3 * i2 + 3] = [bt, ave, var]
+        spec = 0.5 * (dat[7] - dat[1]) / t_delta
+        d1 = (dat[4] - dat[1]) / t_delta
+        d2 = (dat[7] - dat[4]) / t_delta
+        out[i1] = [1.0 / dat[3], dat[4], spec, 0.5 * (dat[2] + dat[8]), (d2 - d1) / t_delta]
+    return out

@@ -60,6 +60,7 @@ EXPORTS = [
     "pned_slots_create", "pned_slots_destroy", "pned_slots_info", "pned_slots_set_stream", "pned_slots_load",
     "pned_slots_load_szq", "pned_slots_load_vector", "pned_slots_release", "pned_slots_step", "pned_slots_query",
     "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column", "pned_lanczos_vector", "pned_slots_set_plan", "pned_slots_plan",
+    "pned_write_salphasbeta", "pned_read_salphasbeta", "pned_tpq_thermo",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -128,6 +129,9 @@ def lib() -> C.CDLL:
     L.pned_lanczos_vector.argtypes = [vp, vp, i32, dp, dp, dp, vp, i32]
     L.pned_slots_set_plan.argtypes = [vp, C.POINTER(TilePlan)]
     L.pned_slots_plan.argtypes = [vp, ip, ip, ip]
+    L.pned_write_salphasbeta.argtypes = [C.c_char_p, i32, i32, dp, dp, dp]
+    L.pned_read_salphasbeta.argtypes = [C.c_char_p, ip, ip, dp, dp, dp, i32]
+    L.pned_tpq_thermo.argtypes = [i32, i32, dp, dp, dp, dbl, dbl, i32, dp]
     _lib = L
     return L
 

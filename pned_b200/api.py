@@ -7,6 +7,7 @@ device by the call) or a CUDA torch tensor (device memory: used in place).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -123,6 +124,44 @@ def normalize_dsf(i_range: int, split: float, sq_re: float, dsf):
     d = np.ascontiguousarray(dsf, dtype=np.float64).copy()
     check(lib().pned_normalize_dsf(i_range, split, sq_re, _dp(d)))
     return d
+
+
+# --------------------------------------------------------------------------- mTPQ output chain
+
+
+def write_salphasbeta(path: str, alpha, beta, coef):
+    """dump_alpha_beta_coef: alpha, beta [num_data1], coef [num_data1][num_data2] (written column-major)."""
+    a = np.ascontiguousarray(alpha, dtype=np.float64)
+    b = np.ascontiguousarray(beta, dtype=np.float64)
+    c = np.asfortranarray(np.asarray(coef, dtype=np.float64))
+    n1, n2 = c.shape
+    if a.shape != (n1,) or b.shape != (n1,):
+        raise ValueError("alpha and beta need num_data1 = coef.shape[0] entries")
+    cf = np.ascontiguousarray(c.T)   # coef(k, m) with k fastest
+    check(lib().pned_write_salphasbeta(os.fsencode(path), n1, n2, _dp(a), _dp(b), _dp(cf)))
+
+
+def read_salphasbeta(path: str):
+    """Returns (alpha, beta, coef [num_data1][num_data2]) of a TPQ coefficient file."""
+    n1, n2 = C.c_int(0), C.c_int(0)
+    check(lib().pned_read_salphasbeta(os.fsencode(path), C.byref(n1), C.byref(n2), None, None, None, 0))
+    a, b = np.zeros(n1.value), np.zeros(n1.value)
+    cf = np.zeros(n1.value * n2.value)
+    check(lib().pned_read_salphasbeta(os.fsencode(path), C.byref(n1), C.byref(n2), _dp(a), _dp(b), _dp(cf), n1.value))
+    return a, b, cf.reshape(n2.value, n1.value).T.copy()
+
+
+def tpq_thermo(beta, energy, hmix, t_min: float, t_max: float, num_div: int):
+    """eval_mpi: canonical T, E(T), C(T), var, d2E/dT2 from mTPQ runs ([n_seeds][num_data1] arrays)."""
+    b = np.ascontiguousarray(np.atleast_2d(beta), dtype=np.float64)
+    e = np.ascontiguousarray(np.atleast_2d(energy), dtype=np.float64)
+    h = np.ascontiguousarray(np.atleast_2d(hmix), dtype=np.float64)
+    if not (b.shape == e.shape == h.shape):
+        raise ValueError("beta, energy and hmix need the same [n_seeds][num_data1] shape")
+    out = np.zeros((num_div + 1, 5))
+    check(lib().pned_tpq_thermo(b.shape[1], b.shape[0], _dp(b), _dp(e), _dp(h), float(t_min), float(t_max),
+                                int(num_div), _dp(out)))
+    return out
 
 
 # --------------------------------------------------------------------------- model / context

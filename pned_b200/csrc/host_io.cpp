@@ -1,0 +1,180 @@
+// Host-side output chain of libpned_gpu.so: the reference's TPQ coefficient
+// files (Fortran unformatted sequential records) and the canonical
+// finite-temperature evaluation of mTPQ runs (eval_mpi).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "pned_internal.h"
+
+using namespace pned;
+
+namespace {
+
+// One Fortran unformatted sequential record: 4-byte length, payload, 4-byte length.
+bool put_record(FILE *f, const void *data, size_t bytes)
+{
+    if (bytes > 0x7fffffffu) return false;
+    const int32_t len = int32_t(bytes);
+    return fwrite(&len, 4, 1, f) == 1 && (bytes == 0 || fwrite(data, 1, bytes, f) == bytes) &&
+           fwrite(&len, 4, 1, f) == 1;
+}
+
+// Reads one record into `out` (resized to the record length).
+bool get_record(FILE *f, std::vector<char> &out)
+{
+    int32_t len = 0, tail = 0;
+    if (fread(&len, 4, 1, f) != 1 || len < 0) return false;
+    out.resize(size_t(len));
+    if (len && fread(out.data(), 1, size_t(len), f) != size_t(len)) return false;
+    return fread(&tail, 4, 1, f) == 1 && tail == len;
+}
+
+// calc_fac (S_one_half/Hybrid_TPS_eval_mpi.f90:236-281): log-weights of the
+// mTPQ states at inverse temperature bt, shifted by their maximum; b is the
+// 1-based beta(1..nd1) of one seed.
+void calc_fac(int nd1, const double *b, double bt, std::vector<double> &fac1, std::vector<double> &fac2)
+{
+    fac1.assign(size_t(nd1) + 1, 0.0);
+    fac2.assign(size_t(nd1) + 1, 0.0);
+    double y = 0.0, maxfac = -1e200;
+    for (int i = 1; i <= 2 * (nd1 - 1); ++i) {
+        const int m = ((i + 1) >> 1) + 1;
+        const double z = std::log(bt / double(2 * i) * b[m - 1]);
+        y += z;
+        fac1[m] = y;
+        maxfac = std::max(y, maxfac);
+    }
+    for (int i = 1; i <= nd1 - 1; ++i) {
+        fac1[i] = std::exp(fac1[i] - maxfac);
+        fac2[i] = fac1[i] * bt * b[i] / double(2 * i - 1);
+    }
+    fac1[nd1] = std::exp(fac1[nd1] - maxfac);
+    fac2[nd1] = 0.0;
+}
+
+// Sum of v in descending order (lsort, :315-347, then the ordered sums of eval_q).
+double sorted_sum(std::vector<double> v)
+{
+    std::sort(v.begin(), v.end(), std::greater<double>());
+    double s = 0.0;
+    for (double x : v) s += x;
+    return s;
+}
+
+// eval_q (:284-313): canonical expectation of dat1 (diagonal) and dat2
+// (<k-1|H|k>) terms at bt for one seed.
+double eval_q(int nd1, const double *b, const double *dat1, const double *dat2, double bt)
+{
+    std::vector<double> fac1, fac2;
+    calc_fac(nd1, b, bt, fac1, fac2);
+    std::vector<double> t1(size_t(nd1) - 1), t2(size_t(nd1) - 1);
+    double z = 0.0;
+    for (int i = 1; i <= nd1 - 1; ++i) {
+        t1[i - 1] = fac1[i] * dat1[i - 1];
+        t2[i - 1] = fac2[i] * dat2[i - 1];
+        z = z + fac1[i] + fac2[i];
+    }
+    return (sorted_sum(t1) + sorted_sum(t2)) / z;
+}
+
+}  // namespace
+
+extern "C" int pned_write_salphasbeta(const char *path, int num_data1, int num_data2, const double *alpha,
+                                      const double *beta, const double *coef)
+{
+    if (!path || num_data1 < 1 || num_data2 < 1 || !alpha || !beta || !coef)
+        return fail(PNED_EINVAL, "pned_write_salphasbeta: bad arguments");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_write_salphasbeta: cannot open ") + path);
+    const int32_t n1 = num_data1, n2 = num_data2;
+    bool ok = put_record(f, &n1, 4) && put_record(f, &n2, 4) &&
+              put_record(f, alpha, sizeof(double) * size_t(n1)) && put_record(f, beta, sizeof(double) * size_t(n1)) &&
+              put_record(f, coef, sizeof(double) * size_t(n1) * size_t(n2));
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_write_salphasbeta: write failed");
+}
+
+extern "C" int pned_read_salphasbeta(const char *path, int *num_data1, int *num_data2, double *alpha, double *beta,
+                                     double *coef, int capacity1)
+{
+    if (!path || !num_data1 || !num_data2) return fail(PNED_EINVAL, "pned_read_salphasbeta: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_read_salphasbeta: cannot open ") + path);
+    std::vector<char> r1, r2, ra, rb, rc;
+    bool ok = get_record(f, r1) && r1.size() == 4 && get_record(f, r2) && r2.size() == 4;
+    int32_t n1 = 0, n2 = 0;
+    if (ok) {
+        std::memcpy(&n1, r1.data(), 4);
+        std::memcpy(&n2, r2.data(), 4);
+        ok = n1 > 0 && n2 > 0;
+    }
+    if (ok && alpha && beta && coef) {
+        ok = capacity1 >= n1 && get_record(f, ra) && ra.size() == sizeof(double) * size_t(n1) && get_record(f, rb) &&
+             rb.size() == ra.size() && get_record(f, rc) && rc.size() == sizeof(double) * size_t(n1) * size_t(n2);
+        if (ok) {
+            std::memcpy(alpha, ra.data(), ra.size());
+            std::memcpy(beta, rb.data(), rb.size());
+            std::memcpy(coef, rc.data(), rc.size());
+        }
+    }
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_read_salphasbeta: not a TPQ coefficient file of the expected layout");
+    *num_data1 = n1;
+    *num_data2 = n2;
+    return PNED_OK;
+}
+
+extern "C" int pned_tpq_thermo(int num_data1, int n_seeds, const double *beta, const double *energy,
+                               const double *hmix, double t_min, double t_max, int num_div, double *out)
+{
+    if (num_data1 < 2 || n_seeds < 1 || !beta || !energy || !hmix || !out || num_div < 1 || !(t_min > 0) ||
+        !(t_max >= t_min))
+        return fail(PNED_EINVAL, "pned_tpq_thermo: bad arguments");
+    const double lmax = std::log(t_max), lmin = std::log(t_min);
+    const double delta = (lmax - lmin) / double(num_div);
+    double t_delta = 1e-4;
+    if (t_min < t_delta) t_delta = t_min * 0.9;
+    std::vector<double> tmp(static_cast<size_t>(n_seeds));
+    for (int i1 = 0; i1 <= num_div; ++i1) {
+        const double t0 = std::exp(lmin + double(i1) * delta);
+        double dat[9];
+        for (int i2 = 0; i2 < 3; ++i2) {
+            const double bt = i2 == 0 ? 1.0 / (t0 - t_delta) : (i2 == 1 ? 1.0 / t0 : 1.0 / (t0 + t_delta));
+            for (int s = 0; s < n_seeds; ++s) {
+                const size_t o = size_t(s) * num_data1;
+                tmp[s] = eval_q(num_data1, beta + o, energy + o, hmix + o, bt);
+            }
+            // calc_ave (:349-363)
+            double ave = 0.0, var = 0.0;
+            for (int s = 0; s < n_seeds; ++s) {
+                ave += tmp[s];
+                var += tmp[s] * tmp[s];
+            }
+            ave /= double(n_seeds);
+            var = var / double(n_seeds) - ave * ave;
+            dat[3 * i2] = bt;
+            dat[3 * i2 + 1] = ave;
+            dat[3 * i2 + 2] = var;
+        }
+        // :420-430 (Fortran dat(0:8))
+        const double d_e = 0.5 * (dat[7] - dat[1]);
+        const double spec = d_e / t_delta;
+        const double var_spec = 0.5 * (dat[2] + dat[8]);
+        const double spec_d1 = (dat[4] - dat[1]) / t_delta;
+        const double spec_d2 = (dat[7] - dat[4]) / t_delta;
+        const double del_c = (spec_d2 - spec_d1) / t_delta;
+        double *o = out + size_t(i1) * 5;
+        o[0] = 1.0 / dat[3];
+        o[1] = dat[4];
+        o[2] = spec;
+        o[3] = var_spec;
+        o[4] = del_c;
+    }
+    return PNED_OK;
+}

@@ -242,16 +242,28 @@ class GpuLane:
 # --------------------------------------------------------------------------- scheduler
 
 def default_lane_slots(n: int) -> int:
-    """Slots per lane by lattice size (device memory 56 dim bytes per slot)."""
-    if n >= 30:
-        return 1
-    if n >= 26:
+    """Slots per lane.  Measured on B200: a step of R slots costs R times the
+    single-vector step or more from N = 20 up (the partner-tile reads that
+    bound the H.V scale with R), so larger lattices get single-slot lanes and
+    run side by side instead; at N <= 18 four slots cost 0.7x per slot."""
+    return 4 if n <= 18 else 1
+
+
+def default_max_lanes(n: int) -> int:
+    """Lanes per lattice size that may run side by side (small lattices leave
+    most of the device idle, large ones fill it)."""
+    if n <= 20:
         return 8
-    return 16
+    if n <= 22:
+        return 4
+    if n <= 24:
+        return 2
+    return 1
 
 
 @dataclass
 class _LaneState:
+    n: int
     eng: object
     occ: list
     left: list
@@ -280,14 +292,15 @@ class Server:
     chunk, so that arrivals wait at most about that long for admission."""
 
     def __init__(self, budget: int, lane_factory=None, lane_slots=default_lane_slots, max_steps: int = 512,
-                 chunk_ms: float = 30.0, clock=time.perf_counter, sleep=time.sleep):
+                 chunk_ms: float = 30.0, clock=time.perf_counter, sleep=time.sleep, max_lanes=default_max_lanes):
         self.budget = int(budget)
         self.lane_factory = lane_factory or (lambda n, R, ms: GpuLane(n, R, ms))
         self.lane_slots = lane_slots
+        self.max_lanes = max_lanes
         self.max_steps = max_steps
         self.chunk_ms = chunk_ms
         self.clock, self.sleep = clock, sleep
-        self.lanes: dict = {}
+        self.lanes: list = []
         self.used = 0
         self.clusters: dict = {}
 
@@ -304,23 +317,23 @@ class Server:
         R = self.lane_slots(n)
         need = self._lane_bytes(n, R)
         if self.used + need > self.budget:
-            # free idle lanes (nothing loaded, nothing waiting), oldest first
-            for m, ls in sorted(self.lanes.items(), key=lambda kv: kv[1].idle_since):
+            # free idle lanes (nothing loaded, nothing waiting for their size), oldest first
+            for ls in sorted(self.lanes, key=lambda x: x.idle_since):
                 if self.used + need <= self.budget:
                     break
-                if not ls.busy and all(o is None for o in ls.occ) and not self.waiting[m]:
-                    self._close_lane(m)
+                if not ls.busy and all(o is None for o in ls.occ) and not self.waiting[ls.n]:
+                    self._close_lane(ls)
             if self.used + need > self.budget:
                 return False
         eng = self.lane_factory(n, R, self.max_steps)
-        self.lanes[n] = _LaneState(eng=eng, occ=[None] * eng.R, left=[0] * eng.R, idle_since=now)
+        self.lanes.append(_LaneState(n=n, eng=eng, occ=[None] * eng.R, left=[0] * eng.R, idle_since=now))
         self.used += eng.bytes
         stats.lanes_created += 1
         stats.peak_bytes = max(stats.peak_bytes, self.used)
         return True
 
-    def _close_lane(self, n):
-        ls = self.lanes.pop(n)
+    def _close_lane(self, ls):
+        self.lanes.remove(ls)
         self.used -= ls.eng.bytes
         ls.eng.close()
 
@@ -343,8 +356,8 @@ class Server:
                 jobs_open += 1
                 i += 1
             progressed = False
-            for n in list(self.lanes):
-                ls = self.lanes[n]
+            for ls in list(self.lanes):
+                n = ls.n
                 if ls.busy:
                     if not ls.eng.query():
                         continue
@@ -405,9 +418,13 @@ class Server:
                 for s in active:
                     ls.left[s] -= k
                 progressed = True
-            # lanes for sizes with waiting chains
+            # more lanes for sizes whose waiting chains outnumber their free slots
             for n, q in self.waiting.items():
-                if q and n not in self.lanes:
+                if not q:
+                    continue
+                mine = [ls for ls in self.lanes if ls.n == n]
+                free = sum(o is None for ls in mine for o in ls.occ)
+                if len(q) > free and len(mine) < self.max_lanes(n):
                     if self._open_lane(n, now, stats):
                         progressed = True
             if not progressed:
@@ -417,8 +434,8 @@ class Server:
         return stats
 
     def close(self):
-        for n in list(self.lanes):
-            self._close_lane(n)
+        for ls in list(self.lanes):
+            self._close_lane(ls)
 
 
 def summarize(stats: ServeStats, requests) -> dict:

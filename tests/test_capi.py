@@ -1,6 +1,7 @@
 """CPU-side checks of the C ABI: the library loads, exports every symbol that
 include/pned_gpu.h declares, and its host routines agree bit for bit with the
 oracle's restatement of the reference."""
+import math
 import os
 import re
 
@@ -10,6 +11,7 @@ import pytest
 import pned_b200 as P
 from oracle import oracle as O
 from pned_b200 import couplings as CP
+from pned_b200.lattice import honeycomb
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -94,3 +96,59 @@ def test_errors_are_reported_not_fatal():
         P.bisec(np.zeros(3), np.zeros(3), 3, 5)         # ne > ndim
     with pytest.raises(ValueError):
         P.build_xlocal(2, 0, np.zeros(5))
+
+
+# --------------------------------------------------------------------------- mTPQ output chain
+
+def test_salphasbeta_file_layout_and_round_trip(tmp_path):
+    import struct
+    n1, n2 = 7, 5
+    rng = np.random.default_rng(3)
+    a, b = rng.standard_normal(n1), rng.standard_normal(n1)
+    c = rng.standard_normal((n1, n2))
+    path = str(tmp_path / "SalphaSbeta_me00000seed00001zz")
+    P.api.write_salphasbeta(path, a, b, c)
+
+    def rec(payload):
+        return struct.pack("<i", len(payload)) + payload + struct.pack("<i", len(payload))
+    expect = (rec(struct.pack("<i", n1)) + rec(struct.pack("<i", n2)) + rec(a.astype("<f8").tobytes()) +
+              rec(b.astype("<f8").tobytes()) + rec(np.asfortranarray(c).T.astype("<f8").tobytes()))
+    assert open(path, "rb").read() == expect
+    a2, b2, c2 = P.api.read_salphasbeta(path)
+    assert np.array_equal(a2, a) and np.array_equal(b2, b) and np.array_equal(c2, c)
+    with open(path, "r+b") as f:
+        f.seek(4 + 4 + 4 + 4 + 4 + 4)   # corrupt the first alpha record's length
+        f.write(struct.pack("<i", 3))
+    with pytest.raises(P.PnedError):
+        P.api.read_salphasbeta(path)
+
+
+def test_tpq_thermo_matches_oracle():
+    """eval_mpi on oracle mTPQ runs: the library equals the numpy restatement to
+    1e-12; its E(T) rises with T and tends to the exact ground-state energy at
+    low T.  (Its weights carry bt/(2i) per factor, eval_mpi.f90:249, so at finite
+    T it does not reproduce the exact canonical energy; mirrored as it is.)"""
+    from dense import dense_h
+    cl = honeycomb(3, 2)
+    cpl = CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi))
+    L = 2.0 * cl.n
+    X = O.xlocal(2, 0, cpl)
+    skip, _, pt = O.parity_skip(2, 0, X)
+    Xt = O.tps_explicit(2, cl.nbond, L, X)
+    om = O.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, Xt, skip, pt)
+    steps = 150
+    runs = []
+    for seed in (1, 2):
+        v = O.gaussian(seed, om.ldim)
+        v /= np.linalg.norm(v)
+        runs.append(om.tps(L, v, steps))
+    beta = np.stack([r["beta"] for r in runs])
+    energy = np.stack([r["coef"][:, 3] for r in runs])
+    hmix = np.stack([r["coef"][:, 4] for r in runs])
+    got = P.api.tpq_thermo(beta, energy, hmix, 0.05, 10.0, 12)
+    ref = O.tpq_thermo(beta, energy, hmix, 0.05, 10.0, 12)
+    assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)) <= 1e-12
+    assert np.allclose(got[:, 0], np.exp(np.linspace(math.log(0.05), math.log(10.0), 13)), rtol=1e-12)
+    assert np.all(np.diff(got[:, 1]) > 0) and np.all(got[:, 2] > 0) and np.all(got[:, 3] >= -1e-12)
+    e0 = np.linalg.eigvalsh(dense_h(cl.n, 2, 0, cl.ipair, cl.ibond_type, cpl))[0]
+    assert abs(got[0, 1] - e0) <= 0.02 * abs(e0)

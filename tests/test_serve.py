@@ -80,7 +80,7 @@ def small_stream(n=60, seed=5):
 
 def test_all_requests_complete_with_their_phases():
     reqs = small_stream()
-    srv, lanes = make(budget=1 << 40, lane_slots=lambda n: 4)
+    srv, lanes = make(budget=1 << 40, lane_slots=lambda n: 4, max_lanes=lambda n: 1)
     st = srv.run(reqs, realtime=False)
     assert sorted(r["rid"] for r in st.results) == [q.rid for q in reqs]
     by = {r["rid"]: r for r in st.results}
@@ -104,7 +104,7 @@ def test_all_requests_complete_with_their_phases():
 def test_budget_bounds_the_lanes_held():
     reqs = small_stream(40, seed=9)
     one_lane = 56 * 2 ** 14 * 2 + 32 * 2 ** 14
-    srv, lanes = make(budget=one_lane, lane_slots=lambda n: 2)
+    srv, lanes = make(budget=one_lane, lane_slots=lambda n: 2, max_lanes=lambda n: 1)
     st = srv.run(reqs, realtime=False)
     assert len(st.results) == len(reqs)
     assert st.peak_bytes <= one_lane
@@ -140,3 +140,15 @@ def test_summary_percentiles():
     st = srv.run(reqs, realtime=False)
     s = serve.summarize(st, reqs)
     assert s["requests"] == 20 and s["p99_latency_s"] >= s["p50_latency_s"] >= 0
+
+
+def test_several_lanes_per_size_run_side_by_side():
+    reqs = small_stream(40, seed=21)
+    srv, lanes = make(budget=1 << 40, lane_slots=lambda n: 1, max_lanes=lambda n: 3)
+    st = srv.run(reqs, realtime=False)
+    assert len(st.results) == len(reqs)
+    per_n = {}
+    for e in FakeLane.log:
+        if e[0] == "open":
+            per_n[e[1]] = per_n.get(e[1], 0) + 1
+    assert max(per_n.values()) == 3 and all(v <= 3 for v in per_n.values())
