@@ -188,7 +188,11 @@ def run_ours(args, rank, world, local_rank):
     model, cl = build_model(args.n_sites)
     D = model.dim
     tuning = None
-    if args.tune:
+    if args.plan:
+        f, w, mp, jb = (int(x) for x in args.plan.split(","))
+        model.set_plan(1, f, w, mp, jb)
+        tuning = {"plan": [f, w, mp, jb], "tried": []}
+    elif args.tune:
         from pned_b200.tune import autotune
         tuning = autotune(model, 1)
     stream = torch.cuda.Stream(device=dev)
@@ -270,8 +274,9 @@ def run_ours(args, rank, world, local_rank):
         "e2e": e2e,
     }
     if tuning is not None:
-        line["roofline"]["tuned_plan"] = {"row_fixed_bits": tuning["plan"][0], "window_bits": tuning["plan"][1],
-                                          "max_passes": tuning["plan"][2], "candidates": len(tuning.get("tried", []))}
+        pl = list(tuning["plan"]) + [-1] * (4 - len(tuning["plan"]))
+        line["roofline"]["tuned_plan"] = {"row_fixed_bits": pl[0], "window_bits": pl[1], "max_passes": pl[2],
+                                          "j_bits": pl[3], "candidates": len(tuning.get("tried", []))}
     if rank == 0 and args.cpu_baseline:
         try:
             cs = CpuSample(args.n_sites, os.cpu_count() or 1, slice_log2=args.ref_slice_log2)
@@ -474,6 +479,8 @@ def main():
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
     ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve"])
     ap.add_argument("--no-tune", dest="tune", action="store_false")
+    ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits' "
+                                                 "instead of autotuning (profiling runs)")
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--batch-steps", type=int, default=40)
     ap.add_argument("--requests", type=int, default=200)

@@ -136,14 +136,17 @@ int pned_model_plan(const pned_model *m, int R, int *tile_passes, int *partner_t
  * global bits kept in the tile rows (8 for R = 1 by default: rows are runs
  * of 256 consecutive states; fewer lets the planner pick tile bits that
  * leave fewer partner tiles); window_bits: outer bits whose partner tiles a
- * pass expects in L2; max_passes: 1..4.  Re-plans at once (plan NULL:
- * defaults); call it between launches, not while other threads launch on the
- * model.  Used by the autotuner (pned_b200.tune).
+ * pass expects in L2; max_passes: 1..4; j_bits (R = 1 only): 1..3, states
+ * per thread 2^j_bits (fewer registers, more resident blocks).  Re-plans at
+ * once (plan NULL: defaults); call it between launches, not while other
+ * threads launch on the model.  Used by the autotuner (pned_b200.tune).
  */
 typedef struct {
     int32_t row_fixed_bits;
     int32_t window_bits;
     int32_t max_passes;
+    int32_t j_bits;
+    int32_t l1_carveout;   /* 1 (default): shared-memory carveout sized to the tiles, the rest L1; 0: driver's choice */
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 

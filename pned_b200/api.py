@@ -240,9 +240,10 @@ class Model:
         check(lib().pned_model_plan(self._h, int(R), C.byref(p), C.byref(g), C.byref(t)))
         return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
 
-    def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1):
+    def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
+                 j_bits: int = -1, l1_carveout: int = 1):
         """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""
-        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes))
+        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout))
         check(lib().pned_model_set_plan(self._h, int(R), C.byref(tp)))
         return self.plan(R)
 
@@ -594,8 +595,9 @@ class SlotBatch:
         check(lib().pned_slots_plan(self._h, C.byref(p), C.byref(g), C.byref(t)))
         return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
 
-    def set_plan(self, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1) -> dict:
-        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes))
+    def set_plan(self, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
+                 j_bits: int = -1, l1_carveout: int = 1) -> dict:
+        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout))
         check(lib().pned_slots_set_plan(self._h, C.byref(tp)))
         return self.plan()
 

@@ -127,8 +127,13 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
 // others gather through L1/L2 from the partner tile, 2^JB loads per thread in
 // flight.  The term decode (coefficient index) is done once per term for the
 // thread's 2^JB states.
+// Resident blocks per SM the single-vector tile kernel is built for: fewer
+// rows per thread, fewer registers, more warps to hide the gather latency.
+__host__ __device__ constexpr int tile_blocks_per_sm(int jb) { return jb >= 3 ? 2 : (jb == 2 ? 3 : 4); }
+
 template <int JB, bool RC, bool RD, int K>
-__global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
+__global__ void __launch_bounds__(kThreads, tile_blocks_per_sm(JB))
+    hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
 {
     constexpr int SPT = 1 << JB;
     constexpr int TILE = kThreads * SPT;
@@ -183,9 +188,19 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
                 if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
             const double2 *sv = s_v + (tid ^ (T.mask & 0xffu));
             const uint32_t mhi = T.mask >> 8;
+            if (!T.hasj) {   // one coefficient for all rows of the thread
+                const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 w = sv[kThreads * (j ^ mhi)];
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
-                const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
+                const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
                 const double2 w = sv[kThreads * (j ^ mhi)];
                 if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
                 else acc[j] = cfma(c, w, acc[j]);
@@ -195,15 +210,26 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_kernel(const __grid_const
         for (int t = prog.nin; t < prog.nterms; ++t) {
             const TileTerm T = prog.t[t];
             double2 w0[SPT];
+            // (base | jexp) ^ mask == (base ^ mask) ^ jexp: base has no j bits
+            const uint32_t pbx = base ^ T.mask;
 #pragma unroll
-            for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + ((base | prog.jexp[j]) ^ T.mask));
+            for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + (pbx ^ prog.jexp[j]));
             uint32_t ib = 0;
 #pragma unroll
             for (int d = 0; d < kMaxDeps; ++d)
                 if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            if (!T.hasj) {
+                const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
+                    else acc[j] = cfma(c, w0[j], acc[j]);
+                }
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
-                const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
+                const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
                 if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
                 else acc[j] = cfma(c, w0[j], acc[j]);
             }
@@ -595,16 +621,42 @@ cudaError_t allow_dynamic_smem(const void *kern, int device)
     return e;
 }
 
-static int tile_grid(const pned_model *m, int nblocks) { return std::max(1, std::min(nblocks, 2 * m->nsm)); }
-
-template <bool RC, bool RD, int K>
-static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+// Shared-memory carveout of a kernel: just what `blocks` resident blocks of
+// `smem` dynamic bytes (+ static and reserved bytes) need, so that the rest
+// of the SM's 256 KB stays L1, which catches partner rows re-read by the
+// terms of one partner tile.
+static cudaError_t set_carveout(const void *kern, int device, size_t smem, int blocks)
 {
-    auto kern = hv_tile_kernel<3, RC, RD, K>;
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void *, int>, int>> last;
+    const size_t need = size_t(blocks) * (smem + 9 * 1024);
+    const int pct = int(std::min<size_t>(100, (need * 100 + 228 * 1024 - 1) / (228 * 1024)));
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &l : last)
+        if (l.first.first == kern && l.first.second == device) {
+            if (l.second == pct) return cudaSuccess;
+            l.second = pct;
+            return cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+        }
+    last.push_back({{kern, device}, pct});
+    return cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
+// Persistent grid of the tiled kernels: all resident blocks, which sweep
+// consecutive tiles, so partner tiles on the fast outer bits are found in L2.
+static int tile_grid(const pned_model *m, int nblocks)
+{
+    return std::max(1, std::min(nblocks, tile_blocks_per_sm(m->tile_jb) * m->nsm));
+}
+
+template <int JB, bool RC, bool RD, int K>
+static cudaError_t launch_tile_j(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    auto kern = hv_tile_kernel<JB, RC, RD, K>;
     cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+    if (e == cudaSuccess && m->carveout)
+        e = set_carveout(reinterpret_cast<const void *>(kern), m->device, m->tile_smem, tile_blocks_per_sm(JB));
     if (e != cudaSuccess) return e;
-    // persistent grid (two blocks per SM): the blocks in flight sweep consecutive
-    // tiles, so partner tiles on the fast outer bits are found in L2
     const int grid = tile_grid(m, nblocks);
     HvArgs b = a;
     for (size_t p = 0; p < m->tprogs.size(); ++p) {
@@ -614,6 +666,17 @@ static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nbloc
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+template <bool RC, bool RD, int K>
+static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    switch (m->tile_jb) {
+    case 1: return launch_tile_j<1, RC, RD, K>(m, a, nblocks, st);
+    case 2: return launch_tile_j<2, RC, RD, K>(m, a, nblocks, st);
+    case 3: return launch_tile_j<3, RC, RD, K>(m, a, nblocks, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 template <int K>
@@ -662,6 +725,8 @@ static cudaError_t launch_hv_k(const pned_model *m, const HvArgs &a, int nblocks
     }
 }
 
+static int rtile_grid(const pned_model *m, int nblocks) { return std::max(1, std::min(nblocks, 2 * m->nsm)); }
+
 // Tile set of the multi-vector kernel for R (null: the flat kernel runs).
 static const pned_model::TileSet *find_rtiles(const pned_model *m, int R)
 {
@@ -678,8 +743,10 @@ static cudaError_t launch_rv_t(const pned_model *m, const pned_model::TileSet &t
 {
     auto kern = hv_tile_rv_kernel<VPT, SPT, SLOT, RC, RD, K>;
     cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+    if (e == cudaSuccess && m->carveout)
+        e = set_carveout(reinterpret_cast<const void *>(kern), m->device, rtile_smem(m, a.R, SLOT), 2);
     if (e != cudaSuccess) return e;
-    const int grid = tile_grid(m, nblocks);
+    const int grid = rtile_grid(m, nblocks);
     const size_t smem = rtile_smem(m, a.R, SLOT);
     HvArgs b = a;
     for (size_t p = 0; p < ts.progs.size(); ++p) {
@@ -713,7 +780,7 @@ static cudaError_t launch_rv(const pned_model *m, const pned_model::TileSet &ts,
 int hv_partial_blocks(const pned_model *m, int R, int nblocks)
 {
     if (!m->tprogs.empty() && R == 1 && m->use_tile) return int(m->tprogs.size()) * tile_grid(m, nblocks);
-    if (const pned_model::TileSet *ts = find_rtiles(m, R)) return int(ts->progs.size()) * tile_grid(m, nblocks);
+    if (const pned_model::TileSet *ts = find_rtiles(m, R)) return int(ts->progs.size()) * rtile_grid(m, nblocks);
     return nblocks;
 }
 
@@ -844,9 +911,11 @@ void build_tile_programs(pned_model *m)
     const int fixed = m->plan1.row_fixed_bits >= 0 ? m->plan1.row_fixed_bits : 8;
     const int window = m->plan1.window_bits >= 0 ? m->plan1.window_bits : kTileWindowBits;
     const int mp = m->plan1.max_passes > 0 ? m->plan1.max_passes : kTileMaxPasses;
-    if (hp.q == 2 && hp.n >= 12 && plan_tiles(hp, 8, 3, fixed, window, mp, passes) == PNED_OK) {
+    const int jb = m->plan1.j_bits > 0 ? m->plan1.j_bits : 3;
+    if (hp.q == 2 && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes) == PNED_OK) {
         m->tprogs = tile_programs(hp, passes, m->ntab);
-        m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << 3) + std::max(1, m->ntab));
+        m->tile_jb = jb;
+        m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
         m->use_tile = true;
     }
 }
@@ -997,7 +1066,7 @@ extern "C" int pned_model_plan(const pned_model *m, int R, int *tile_passes, int
     if (R == 1 && m->use_tile) {
         passes = int(m->tprogs.size());
         for (const auto &t : m->tprogs) groups += t->ngroups;
-        states = kThreads * (1 << 3);
+        states = kThreads * (1 << m->tile_jb);
     } else if (R > 1) {
         std::lock_guard<std::mutex> lock(const_cast<pned_model *>(m)->rtiles_mu);
         auto it = m->rtiles.find(R);
@@ -1016,14 +1085,17 @@ extern "C" int pned_model_plan(const pned_model *m, int R, int *tile_passes, int
 extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan)
 {
     if (!m || pick_vpt(R) == 0) return fail(PNED_EINVAL, "pned_model_set_plan: bad arguments");
-    if (plan && (plan->max_passes > kTileMaxPasses || plan->window_bits > 30 || plan->row_fixed_bits > 8))
+    if (plan && (plan->max_passes > kTileMaxPasses || plan->window_bits > 30 || plan->row_fixed_bits > 8 ||
+                 plan->j_bits > kTileMaxJB || plan->j_bits == 0))
         return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
     if (R == 1) {
-        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1};
+        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1};
+        m->carveout = m->plan1.l1_carveout != 0;
         build_tile_programs(m);
         return PNED_OK;
     }
-    const pned_tile_plan def{-1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1};
+    if (plan) m->carveout = plan->l1_carveout != 0;
     ensure_rtiles(m, R, false, plan ? plan : &def);
     return PNED_OK;
 }
