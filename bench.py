@@ -250,6 +250,10 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = load_peaks()
     plan = model.plan()
+    # DRAM traffic of the tiled H.v per state, from the ncu capture of the same
+    # kernel and plan shape at N=26 (6.92 GB per H.v over 2^26 states), scaled
+    # to this basis; an ncu figure passed with --traffic replaces it
+    traffic = args.traffic if args.traffic is not None else (6.92e9 / 2 ** 26 * D if plan["tile_passes"] else None)
     # algorithmic bytes of the H.v in a Lanczos step (all flip masks resolved on
     # chip): read C, read P, write W (16 B each) + real diagonal (8 B)
     bytes_hv = (16 + 16 + 16 + 8) * D
@@ -268,7 +272,16 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": (f"hv_tile_kernel x{plan['tile_passes']} passes (K=1)" if plan["tile_passes"]
                                 else "hv_xor_kernel (K=1)"),
                      "hv_ms": hv_ms, "step_ms_profiled": step_ms, "algorithmic_bytes_per_hv": bytes_hv,
-                     "plan": plan, "traffic": args.traffic},
+                     "plan": plan, "traffic": traffic,
+                     "traffic_source": ("--traffic" if args.traffic is not None else
+                                        "scaled from the N=26 ncu capture (103 B/state)"),
+                     # the accounting that counts every partner-tile read (m of them) as a vector read
+                     "partner_read_accounting": {
+                         "m": plan["partner_tiles"],
+                         "bytes_per_hv": 16 * D * (1 + plan["partner_tiles"]) + 16 * D,
+                         "GBs": (16 * D * (2 + plan["partner_tiles"])) / (hv_ms * 1e-3) / 1e9,
+                         "frac": (16 * D * (2 + plan["partner_tiles"])) / (hv_ms * 1e-3) / 1e9 / peak,
+                         "note": "partner tiles are read from L2, not HBM, so this fraction can exceed 1"}},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
         "e2e": e2e,
@@ -287,12 +300,16 @@ def run_ours(args, rank, world, local_rank):
             del cs
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
-    if args.batched:
+    # the batched and served workloads are one-GPU measurements beside the headline
+    if world == 1 and (args.batched or args.served):
         del v
         ctx.close()
         model.close()
         torch.cuda.empty_cache()
-        line["batched"] = {"tpq": batched_tpq(dev, args), "dsf": batched_dsf(dev, args)}
+        if args.batched:
+            line["batched"] = {"tpq": batched_tpq(dev, args), "dsf": batched_dsf(dev, args)}
+        if args.served:
+            line["served"] = served_section(args, local_rank, args.served_requests, args.served_rate)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -404,25 +421,19 @@ def batched_dsf(dev, args):
     return out
 
 
-def run_serve(args, rank, world, local_rank):
-    """Serving stream (continuous batching) against the plain one-at-a-time path."""
-    import numpy as np
+def served_section(args, local_rank, n_requests, rate):
+    """Serving stream (continuous batching) against the plain one-at-a-time path:
+    capacity (all requests queued at once), p50/p99 latency at `rate`, and the
+    same requests run alone through the plain path."""
     import torch
-    import pned_b200 as P
     from pned_b200 import serve
-    if rank != 0:
-        return
-    torch.cuda.set_device(local_rank)
-    P.lib().pned_set_device(local_rank)
-    reqs = serve.make_stream(args.requests, rate=args.rate, seed=SEED, p30=args.p30)
+    reqs = serve.make_stream(n_requests, rate=rate, seed=SEED, p30=args.p30)
     free, _ = torch.cuda.mem_get_info()
     budget = int(0.85 * free)
-    # capacity: the whole stream queued at once, drained as fast as the loop can
     cap_reqs = [serve.Request(**{**q.__dict__, "arrival": 0.0}) for q in reqs]
     srv = serve.Server(budget=budget, max_steps=512)
     with ClockSampler(local_rank) as clk:
         cap = srv.run(cap_reqs, realtime=True)
-        # latency: Poisson arrivals at `rate`
         st = srv.run(reqs, realtime=True)
     srv.close()
     torch.cuda.empty_cache()
@@ -438,29 +449,46 @@ def run_serve(args, rank, world, local_rank):
         if "e0" in p:
             diffs.append(abs(by[q.rid]["e0"] - p["e0"]) / abs(p["e0"]))
     plain = k / tp
-    kinds = {kd: sum(1 for q in reqs if q.kind == kd) for kd in ("lanczos", "tpq", "dsf")}
-    line = {
-        "metric": "served_solves_per_s", "value": capacity, "unit": "solves/s", "n_gpus": 1,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-        "data": "synthetic request stream (seeded)",
-        "config": {"workload": "Poisson stream of Lanczos E0 (300 steps), mTPQ (R=4, 500 steps), DSF (4 momenta, "
-                               "100 steps) requests, S=1/2 honeycomb N in {18..26} uniform + p30 at N=30, "
-                               "random phi, Gamma, h[111]; HBM-budget admission, co-batching by N",
-                   "requests": len(reqs), "rate_per_s": args.rate, "p30": args.p30, "kinds": kinds,
-                   "hbm_budget_bytes": budget},
-        "capacity": {"solves_per_s": capacity, "makespan_s": cap.makespan_s, "lanes_created": cap.lanes_created,
-                     "slot_occupancy": cap.occupied_slot_steps / max(1, cap.slot_steps),
-                     "peak_bytes": cap.peak_bytes, "note": "all requests queued at t=0"},
-        "latency": {"rate_per_s": args.rate, "solves_per_s": s["solves_per_s"], "p50_s": s["p50_latency_s"],
+    return {
+        "workload": "Poisson stream of Lanczos E0 (300 steps), mTPQ (R=4, 500 steps), DSF (4 momenta, 100 steps) "
+                    "requests, S=1/2 honeycomb N uniform in {18..26} + p30 at N=30, random phi, Gamma, h[111]; "
+                    "HBM-budget admission, co-batching by N",
+        "requests": len(reqs), "kinds": {kd: sum(1 for q in reqs if q.kind == kd) for kd in ("lanczos", "tpq", "dsf")},
+        "sizes": {str(n): sum(1 for q in reqs if q.n == n) for n in sorted({q.n for q in reqs})},
+        "hbm_budget_bytes": budget,
+        "solves_per_s": capacity,
+        "capacity": {"makespan_s": cap.makespan_s, "lanes_created": cap.lanes_created,
+                     "slot_occupancy": cap.occupied_slot_steps / max(1, cap.slot_steps), "peak_bytes": cap.peak_bytes,
+                     "note": "all requests queued at t=0"},
+        "latency": {"rate_per_s": rate, "solves_per_s": s["solves_per_s"], "p50_s": s["p50_latency_s"],
                     "p99_s": s["p99_latency_s"], "makespan_s": s["makespan_s"]},
-        "p50_latency_s": s["p50_latency_s"], "p99_latency_s": s["p99_latency_s"],
         "plain": {"solves_per_s": plain, "sample": k, "mean_s": tp / k,
                   "max_rel_e0_diff_served_vs_plain": max(diffs) if diffs else None},
         "vs_plain": capacity / plain,
         "clocks": clk.summary(),
-        "e2e": {"value": s["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
-                "note": "requests enter and results leave through host memory; start vectors are generated "
-                        "on the device from each request's seed"},
+    }
+
+
+def run_serve(args, rank, world, local_rank):
+    """--workload serve: the serving stream as its own JSON line."""
+    import torch
+    import pned_b200 as P
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    P.lib().pned_set_device(local_rank)
+    sv = served_section(args, local_rank, args.requests, args.rate)
+    line = {
+        "metric": "served_solves_per_s", "value": sv["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic request stream (seeded)",
+        "config": {"workload": sv["workload"], "requests": sv["requests"], "rate_per_s": args.rate,
+                   "p30": args.p30, "kinds": sv["kinds"], "sizes": sv["sizes"]},
+        "p50_latency_s": sv["latency"]["p50_s"], "p99_latency_s": sv["latency"]["p99_s"],
+        "served": sv, "vs_plain": sv["vs_plain"], "clocks": sv["clocks"],
+        "e2e": {"value": sv["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "requests enter and results leave through host memory; start vectors are generated on "
+                        "the device from each request's seed"},
     }
     print(json.dumps(line), flush=True)
 
@@ -487,6 +515,9 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--p30", type=float, default=0.02)
     ap.add_argument("--plain-sample", type=int, default=200)
+    ap.add_argument("--no-served", dest="served", action="store_false")
+    ap.add_argument("--served-requests", type=int, default=40)
+    ap.add_argument("--served-rate", type=float, default=1.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
