@@ -421,6 +421,63 @@ def batched_dsf(dev, args):
     return out
 
 
+def run_s1(args, rank, world, local_rank):
+    """--workload s1: S=1 Kitaev-Heisenberg (mixed radix, base 3) on the 18-site honeycomb
+    (3x3), K=-1, J=0.2, D=3^18: batched mTPQ with R=4 vectors (l=3.0, L=54) and a
+    Lanczos E0 run; K timed steps of each after W warm-up steps."""
+    import torch
+    import pned_b200 as P
+    from pned_b200 import couplings as CP
+    from pned_b200.lattice import cluster_for_sites
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    P.lib().pned_set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cl = cluster_for_sites(18)
+    cpl = CP.kitaev_heisenberg(0.2, -1.0)
+    L = 3.0 * cl.n
+    out = {}
+    with ClockSampler(local_rank) as clk:
+        m = P.Model.from_couplings(cl, cpl, q=3, tree=1, tps_L=L)
+        st = torch.cuda.Stream(device=dev)
+        ctx = P.Context(m, R=4, stream=st)
+        v = torch.empty(m.dim * 4, dtype=torch.complex128, device=dev)
+        ctx.fill_gaussian(SEED, v)
+        ms_tpq, res = _timed_session(ctx, st, "tps", v, args.warmup, args.steps, L=L)
+        out["tpq"] = {"ms_per_step": ms_tpq, "steps_per_s": 1000.0 / ms_tpq, "vector_steps_per_s": 4000.0 / ms_tpq,
+                      "energy_first_step_mean": float(res["coef"][0, :, 3].mean())}
+        ctx.close()
+        m.close()
+        del v
+        torch.cuda.empty_cache()
+        m = P.Model.from_couplings(cl, cpl, q=3, tree=1)
+        ctx = P.Context(m, R=1, stream=st)
+        v = torch.empty(m.dim, dtype=torch.complex128, device=dev)
+        ctx.fill_gaussian(SEED, v)
+        ms_l, res = _timed_session(ctx, st, "lanczos", v, args.warmup, args.steps)
+        a, b = res["alpha"][:, 0], res["beta"][:, 0]
+        out["lanczos"] = {"ms_per_step": ms_l, "steps_per_s": 1000.0 / ms_l,
+                          "e0_after_steps": float(P.bisec(a, b, len(a), 1)[0])}
+        D = m.dim
+        ctx.close()
+        m.close()
+    line = {
+        "metric": "s1_tpq_steps_per_s_N18", "value": out["tpq"]["steps_per_s"], "unit": "steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["tpq"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded complex Gaussian start vectors)",
+        "config": {"workload": "S=1 KH honeycomb N=18 (3x3), K=-1, J=0.2, base-3 basis D=3^18, complex128; "
+                               "mTPQ R=4, l=3.0 (L=54), and a Lanczos E0 chain", "dim": D, "R": 4},
+        "tpq": out["tpq"], "lanczos": out["lanczos"],
+        "roofline": {"bound": "hbm", "kernel": "hv_radix_kernel",
+                     "achieved": 56 * D * 4 / (out["tpq"]["ms_per_step"] * 1e-3) / 1e9,
+                     "unit": "GB/s", "note": "whole TPS step over 56 B per state and vector"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def served_section(args, local_rank, n_requests, rate):
     """Serving stream (continuous batching) against the plain one-at-a-time path:
     capacity (all requests queued at once), p50/p99 latency at `rate`, and the
@@ -505,7 +562,7 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
-    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve"])
+    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1"])
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits' "
                                                  "instead of autotuning (profiling runs)")
@@ -536,6 +593,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "serve":
             run_serve(args, rank, world, local_rank)
+        elif args.workload == "s1":
+            run_s1(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -115,8 +115,9 @@ typedef struct {
  * mixed-radix offsets with coefficient tables) and uploads it to the current
  * device.  Replaces set_parallel_bits + make_cpu_list2 + mk_list12
  * (S1/2 MPIlib.f90:74-84, 104-341; parallel.f90:452-578) for one GPU.
- * This build runs the full basis (parity_type != 0); parity_type == 0
- * returns PNED_ENOTSUP.
+ * parity_type == 0 selects the Sz-conserving sector of digit sum total_sz
+ * (mk_list12 order; vectors have the sector dimension, index = the
+ * reference's list1 order); its diagonal must be real.
  */
 int pned_model_create(const pned_model_desc *desc, pned_model **out);
 int pned_model_destroy(pned_model *m);

@@ -29,10 +29,12 @@ int cuda_fail(cudaError_t e, const char *what)
 // Diagonal d(s) = sum_b X_b[st_b(s), st_b(s)] over all bonds (set-up, once).
 template <bool RD>
 __global__ void diag_kernel(int64_t dim, int n, int q, int nbond, const int *__restrict__ s1,
-                            const int *__restrict__ s2, const double2 *__restrict__ dtab, void *out)
+                            const int *__restrict__ s2, const double2 *__restrict__ dtab, void *out,
+                            const int64_t *__restrict__ list1)
 {
     const int Q = q * q;
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < dim; s += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < dim; l += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = list1 ? list1[l] : l;   // sector index -> state
         double2 acc = make_double2(0.0, 0.0);
         if (q == 2) {
             for (int b = 0; b < nbond; ++b) {
@@ -46,15 +48,15 @@ __global__ void diag_kernel(int64_t dim, int n, int q, int nbond, const int *__r
                 acc = cadd(acc, dtab[b * Q + st]);
             }
         }
-        if (RD) static_cast<double *>(out)[s] = acc.x;
-        else static_cast<double2 *>(out)[s] = acc;
+        if (RD) static_cast<double *>(out)[l] = acc.x;
+        else static_cast<double2 *>(out)[l] = acc;
     }
 }
 
 // Gathered H.v on the S = 1/2 full basis:
 //   W[s,r] = pc_r P[s,r] + sc_r * ( (d(s) - shift) C[s,r] + sum_t c_t(s) C[s ^ m_t, r] )
 // with fused per-vector sums: alpha = <v|Hv>, ||W||^2, <G|W>, <G|v> (v = sc C).
-template <int VPT, bool RC, bool RD, int K>
+template <int VPT, bool RC, bool RD, int K, bool SECTOR>
 __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant__ XorProgram prog, const HvArgs a)
 {
     extern __shared__ double2 s_tab[];
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
     for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
          it += (int64_t)gridDim.x * blockDim.x) {
         const int64_t s = it / G;
-        const uint32_t su = uint32_t(s);
+        const uint32_t su = SECTOR ? uint32_t(a.list1[s]) : uint32_t(s);
         double2 v[VPT], acc[VPT];
         const double2 *cs = a.C + s * R + r0;
 #pragma unroll
@@ -101,7 +103,9 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
             for (int k = 0; k < kMaxDeps; ++k)
                 if (k < T.nb) idx |= ((su >> ((T.pos4 >> (8 * k)) & 0xffu)) & 1u) << k;
             const double2 c = s_tab[T.tab + idx];
-            const double2 *ps = a.C + int64_t(su ^ T.xmask) * R + r0;
+            // in the sector, zero elements (the reference's skip mask) leave it: no partner
+            if (SECTOR && c.x == 0.0 && c.y == 0.0) continue;
+            const double2 *ps = a.C + (SECTOR ? lin_index(a, su ^ T.xmask) : int64_t(su ^ T.xmask)) * R + r0;
 #pragma unroll
             for (int j = 0; j < VPT; ++j) {
                 const double2 w = __ldg(ps + j);
@@ -420,7 +424,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
 
 // Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by
 // the two bond digits; zero coefficients (target digit out of range) skip the load.
-template <int VPT, bool RC, bool RD, int K>
+template <int VPT, bool RC, bool RD, int K, bool SECTOR>
 __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constant__ RadixProgram prog, const HvArgs a,
                                                             int q)
 {
@@ -460,13 +464,14 @@ __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constan
 #pragma unroll
             for (int j = 0; j < VPT; ++j) acc[j] = cmul(dd, v[j]);
         }
-        const uint64_t digits = pack_digits(s, prog.n, q);
+        const int64_t st = SECTOR ? a.list1[s] : s;
+        const uint64_t digits = pack_digits(st, prog.n, q);
         for (int t = 0; t < prog.nterms; ++t) {
             const RadixTerm T = prog.t[t];
             const int idx = digit_at(digits, T.s1) + q * digit_at(digits, T.s2);
             const double2 c = s_tab[T.tab + idx];
             if (c.x == 0.0 && c.y == 0.0) continue;
-            const double2 *ps = a.C + (s + T.offset) * R + r0;
+            const double2 *ps = a.C + (SECTOR ? lin_index(a, uint64_t(st + T.offset)) : s + T.offset) * R + r0;
 #pragma unroll
             for (int j = 0; j < VPT; ++j) {
                 const double2 w = __ldg(ps + j);
@@ -687,17 +692,17 @@ static cudaError_t launch_tile(const pned_model *m, const HvArgs &a, int nblocks
     return launch_tile_t<false, false, K>(m, a, nblocks, st);
 }
 
-template <int VPT, bool RC, bool RD, int K>
+template <int VPT, bool RC, bool RD, int K, bool SECTOR = false>
 static cudaError_t launch_hv_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
     const size_t smem = sizeof(double2) * std::max(1, m->ntab);
     if (m->q == 2) {
-        auto kern = hv_xor_kernel<VPT, RC, RD, K>;
+        auto kern = hv_xor_kernel<VPT, RC, RD, K, SECTOR>;
         cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
         if (e != cudaSuccess) return e;
         kern<<<nblocks, kThreads, smem, st>>>(*m->xprog, a);
     } else {
-        auto kern = hv_radix_kernel<VPT, RC, RD, K>;
+        auto kern = hv_radix_kernel<VPT, RC, RD, K, SECTOR>;
         cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
         if (e != cudaSuccess) return e;
         kern<<<nblocks, kThreads, smem, st>>>(*m->rprog, a, m->q);
@@ -708,6 +713,14 @@ static cudaError_t launch_hv_t(const pned_model *m, const HvArgs &a, int nblocks
 template <int VPT, int K>
 static cudaError_t launch_hv_v(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
+    if (m->hp.sector) {   // Sz sector: complex coefficients, real diagonal
+        HvArgs b = a;
+        b.list1 = m->d_list1;
+        b.lin_lo = m->d_lin_lo;
+        b.lin_hi = m->d_lin_hi;
+        b.lin_mod = m->lin_mod;
+        return launch_hv_t<VPT, false, true, K, true>(m, b, nblocks, st);
+    }
     if (m->real_coef && m->real_diag) return launch_hv_t<VPT, true, true, K>(m, a, nblocks, st);
     if (m->real_diag) return launch_hv_t<VPT, false, true, K>(m, a, nblocks, st);
     return launch_hv_t<VPT, false, false, K>(m, a, nblocks, st);
@@ -912,7 +925,7 @@ void build_tile_programs(pned_model *m)
     const int window = m->plan1.window_bits >= 0 ? m->plan1.window_bits : kTileWindowBits;
     const int mp = m->plan1.max_passes > 0 ? m->plan1.max_passes : kTileMaxPasses;
     const int jb = m->plan1.j_bits > 0 ? m->plan1.j_bits : 3;
-    if (hp.q == 2 && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes) == PNED_OK) {
+    if (hp.q == 2 && !hp.sector && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes) == PNED_OK) {
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
         m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
@@ -942,7 +955,7 @@ size_t rtile_smem(const pned_model *m, int R, bool slot_tables)
 bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan *plan)
 {
     const HostProgram &hp = m->hp;
-    if (hp.q != 2 || hp.n < 12 || R < 2 || pick_vpt(R) == 0) return false;
+    if (hp.q != 2 || hp.sector || hp.n < 12 || R < 2 || pick_vpt(R) == 0) return false;
     if (rtile_smem(m, R, slot_tables) > 200 * 1024) return false;
     std::lock_guard<std::mutex> lock(m->rtiles_mu);
     if (m->rtiles.count(R) && !plan) return !m->rtiles[R].progs.empty();
@@ -1011,7 +1024,28 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g_device);
         m->nsm = nsm;
     }
-    build_tile_programs(m.get());
+    if (hp.sector) {
+        if (!m->real_diag)
+            return fail(PNED_ENOTSUP, "pned_model_create: the sector basis needs a real diagonal");
+        int64_t mod = 1;
+        for (int i = 0; i < hp.ihf; ++i) mod *= hp.q;
+        m->lin_mod = mod;
+        e = cudaMalloc(&m->d_list1, sizeof(int64_t) * hp.list1.size());
+        if (e == cudaSuccess) e = cudaMalloc(&m->d_lin_lo, sizeof(int64_t) * hp.lin_lo.size());
+        if (e == cudaSuccess) e = cudaMalloc(&m->d_lin_hi, sizeof(int64_t) * hp.lin_hi.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(m->d_list1, hp.list1.data(), sizeof(int64_t) * hp.list1.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(m->d_lin_lo, hp.lin_lo.data(), sizeof(int64_t) * hp.lin_lo.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(m->d_lin_hi, hp.lin_hi.data(), sizeof(int64_t) * hp.lin_hi.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(m->d_list1); cudaFree(m->d_lin_lo); cudaFree(m->d_lin_hi);
+            return cuda_fail(e, "pned_model_create: sector tables");
+        }
+    } else {
+        build_tile_programs(m.get());
+    }
     // coefficient table
     std::vector<double2> tab(std::max<size_t>(1, hp.table.size()));
     for (size_t i = 0; i < hp.table.size(); ++i) tab[i] = make_double2(hp.table[i].real(), hp.table[i].imag());
@@ -1037,8 +1071,10 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
     if (e == cudaSuccess) {
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
-        if (m->real_diag) diag_kernel<true><<<nsm * 8, kThreads>>>(m->dim, hp.n, hp.q, hp.nbond, ds1, ds2, dt, m->d_diag);
-        else diag_kernel<false><<<nsm * 8, kThreads>>>(m->dim, hp.n, hp.q, hp.nbond, ds1, ds2, dt, m->d_diag);
+        if (m->real_diag)
+            diag_kernel<true><<<nsm * 8, kThreads>>>(m->dim, hp.n, hp.q, hp.nbond, ds1, ds2, dt, m->d_diag, m->d_list1);
+        else
+            diag_kernel<false><<<nsm * 8, kThreads>>>(m->dim, hp.n, hp.q, hp.nbond, ds1, ds2, dt, m->d_diag, m->d_list1);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }
@@ -1055,6 +1091,9 @@ extern "C" int pned_model_destroy(pned_model *m)
     cudaSetDevice(m->device);
     cudaFree(m->d_table);
     cudaFree(m->d_diag);
+    cudaFree(m->d_list1);
+    cudaFree(m->d_lin_lo);
+    cudaFree(m->d_lin_hi);
     delete m;
     return PNED_OK;
 }

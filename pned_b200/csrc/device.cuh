@@ -35,6 +35,9 @@ struct pned_model {
     int nsm = 148;
     double2 *d_table = nullptr;
     void *d_diag = nullptr;
+    // Sz sector: index -> state and the Lin tables
+    int64_t *d_list1 = nullptr, *d_lin_lo = nullptr, *d_lin_hi = nullptr;
+    int64_t lin_mod = 0;
 };
 
 namespace pned {

@@ -336,12 +336,30 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
         if (d->bond_type[i] < 1 || d->bond_type[i] > 9) return fail(PNED_EINVAL, "pned_model_create: bond type");
         if (d->ipair[2 * i] == d->ipair[2 * i + 1]) return fail(PNED_EINVAL, "pned_model_create: bond on one site");
     }
-    if (d->parity_type == 0)
-        return fail(PNED_ENOTSUP, "pned_model_create: the Sz-sector basis (parity_type == 0) is not built yet");
     P = HostProgram{};
     P.n = n; P.q = q; P.nbond = d->n_bonds;
     P.dim = 1;
     for (int i = 0; i < n; ++i) P.dim *= q;
+    if (d->parity_type == 0) {
+        // Sz-conserving sector: mk_list12 (S1/2 parallel.f90:452-578, Sa :366-486)
+        if (n > 40) return fail(PNED_ENOTSUP, "pned_model_create: sector basis above 40 sites");
+        int64_t ldim = 0;
+        int rc = pned_mk_list12(n, q, 0, d->total_sz, &ldim, nullptr, nullptr, nullptr);
+        if (rc) return rc;
+        if (ldim < 1) return fail(PNED_EINVAL, "pned_model_create: empty Sz sector");
+        const int ihf0 = n / 2, ihf = (n + 1) / 2;
+        int64_t nA = 1, nB = 1;
+        for (int i = 0; i < ihf; ++i) nA *= q;
+        for (int i = 0; i < ihf0; ++i) nB *= q;
+        P.list1.resize(size_t(ldim));
+        P.lin_lo.resize(size_t(std::max(nA, nB)));
+        P.lin_hi.resize(size_t(std::max(nA, nB)));
+        rc = pned_mk_list12(n, q, 0, d->total_sz, &ldim, P.list1.data(), P.lin_lo.data(), P.lin_hi.data());
+        if (rc) return rc;
+        P.sector = true;
+        P.ihf = ihf;
+        P.dim = ldim;
+    }
     std::vector<Bond> bonds = schedule_bonds(d);
     auto elem = [&](int t, int row, int col) -> cd {
         const size_t k = size_t(t - 1) * Q * Q + row + size_t(Q) * col;

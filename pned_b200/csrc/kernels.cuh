@@ -87,6 +87,18 @@ struct HvArgs {
     // tiled multi-vector kernel only: per-vector coefficient tables ([ntab][R])
     // and real diagonals ([dim][R]) instead of shared ones
     int slot_tables;
+    // Sz sector (set by launch_hv from the model): index -> state, and the Lin
+    // tables, state -> index = lin_lo[state mod lin_mod] + lin_hi[state / lin_mod] - 1
+    const int64_t *list1;
+    const int64_t *lin_lo;
+    const int64_t *lin_hi;
+    int64_t lin_mod;
 };
+
+// Sector index of a state (the reference's list_lib lookup).
+__device__ __forceinline__ int64_t lin_index(const HvArgs &a, uint64_t st)
+{
+    return a.lin_lo[st % uint64_t(a.lin_mod)] + a.lin_hi[st / uint64_t(a.lin_mod)] - 1;
+}
 
 }  // namespace pned

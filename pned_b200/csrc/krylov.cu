@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kThreads) obs_kernel(const double2 *__restrict
                                                        int64_t dim, int R, int vpt, int n, int nterm,
                                                        const int *__restrict__ ta, const int *__restrict__ tb,
                                                        const double2 *__restrict__ tc, const double2 *__restrict__ T,
-                                                       double2 *partials)
+                                                       double2 *partials, const int64_t *__restrict__ list1)
 {
     double2 red[2][kMaxVPT];
     for (int k = 0; k < 2; ++k)
@@ -87,10 +87,11 @@ __global__ void __launch_bounds__(kThreads) obs_kernel(const double2 *__restrict
     for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * Gs;
          it += (int64_t)gridDim.x * blockDim.x) {
         const int64_t st = it / Gs;
+        const int64_t state = list1 ? list1[st] : st;   // sector index -> state
         double2 w = make_double2(0.0, 0.0);
         for (int t = 0; t < nterm; ++t) {
-            const int i = ta[t] >= n ? 0 : int((st >> ta[t]) & 1);
-            const int k = tb[t] >= n ? 0 : int((st >> tb[t]) & 1);
+            const int i = ta[t] >= n ? 0 : int((state >> ta[t]) & 1);
+            const int k = tb[t] >= n ? 0 : int((state >> tb[t]) & 1);
             w = cfma(tc[t], T[2 * i + k], w);
         }
         const int64_t base = st * R + r0;
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(kThreads) obs_kernel(const double2 *__restrict
 // S^z_q start vectors: C[s, r] = sum_j (d_j(s) - S) e^{i qr[r, j]} x[s].
 __global__ void __launch_bounds__(kThreads) szq_kernel(const double2 *__restrict__ x, const double2 *__restrict__ ph,
                                                        int64_t dim, int R, int vpt, int n, int q, double2 *C,
-                                                       double2 *partials)
+                                                       double2 *partials, const int64_t *__restrict__ list1)
 {
     double2 red[1][kMaxVPT];
     for (int j = 0; j < kMaxVPT; ++j) red[0][j] = make_double2(0.0, 0.0);
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(kThreads) szq_kernel(const double2 *__restrict
         const int64_t st = it / Gs;
         double2 w[kMaxVPT];
         for (int j = 0; j < kMaxVPT; ++j) w[j] = make_double2(0.0, 0.0);
-        int64_t y = st;
+        int64_t y = list1 ? list1[st] : st;   // sector index -> state
         for (int site = 0; site < n; ++site) {
             int64_t dj;
             if (q == 2) { dj = y & 1; y >>= 1; }
@@ -275,7 +276,7 @@ static cudaError_t tps_step(pned_ctx *c, Session &S, bool first)
         obs_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(c->buf[S.b0], first ? nullptr : c->buf[S.b2],
                                                           slot(c, kSlotSc), slot(c, kSlotGsc), c->m->dim, R,
                                                           pick_vpt(R), c->m->n, ob.n, ob.a, ob.b, ob.c, ob.T,
-                                                          c->partials);
+                                                          c->partials, c->m->d_list1);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, 2 * R, S.d_osum + 2 * o * R, c->stream);
     }
@@ -421,7 +422,7 @@ extern "C" int pned_session_begin_dsf(pned_ctx *c, const pned_c128 *x, const dou
     if (e == cudaSuccess) e = cudaMemcpyAsync(dph, ph.data(), sizeof(double2) * ph.size(), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) {
         szq_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(dx, dph, c->m->dim, R, pick_vpt(R), n, c->m->q,
-                                                          c->buf[S.b0], c->partials);
+                                                          c->buf[S.b0], c->partials, c->m->d_list1);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, c->sums, c->stream);

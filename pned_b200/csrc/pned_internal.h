@@ -64,7 +64,12 @@ constexpr int kTileMaxGroups = 64;    // partner tiles per pass
 
 struct HostProgram {
     int n = 0, q = 2;
-    int64_t dim = 0;
+    int64_t dim = 0;                     // basis size: q^n, or the sector size
+    // Sz sector (parity_type == 0): sector index -> state, and the Lin tables
+    // (index = lin_lo[state mod q^ihf] + lin_hi[state / q^ihf] - 1)
+    bool sector = false;
+    int ihf = 0;
+    std::vector<int64_t> list1, lin_lo, lin_hi;
     int nbond = 0;
     bool real = true;                    // every coefficient and diagonal entry real
     std::vector<XorTerm> xterms;         // q == 2

@@ -248,6 +248,57 @@ def test_lanczos_vector_parity():
     assert rel(xd.cpu().numpy(), xr) <= 1e-10
 
 
+SECTOR_CASES = [
+    # (L1, L2, q, tree, R): pure Heisenberg (Sz conserved, parity_type == 0), Sz = 0 sector
+    (3, 2, 2, 0, 1),
+    (3, 2, 2, 0, 4),
+    (2, 4, 2, 1, 2),
+    (3, 1, 3, 1, 1),
+    (2, 2, 3, 1, 3),
+]
+
+
+@pytest.mark.parametrize("case", SECTOR_CASES, ids=[f"{c[0]}x{c[1]}q{c[2]}t{c[3]}R{c[4]}" for c in SECTOR_CASES])
+def test_sector_hv_and_lanczos(case):
+    """Sz-sector basis (mk_list12 order, Lin-table partner lookup): H.v to 1e-12 against
+    the oracle's sector p_mltply_v3; Lanczos E0 equals the sector's oracle E0 and the
+    full-basis ground-state energy (the Heisenberg ground state has Sz = 0)."""
+    L1, L2, q, tree, R = case
+    cl = honeycomb(L1, L2)
+    cpl = CP.kitaev_heisenberg(1.0, 0.0)
+    X, skip, pt = P.build_xlocal(q, tree, cpl)
+    assert pt == 0
+    gm = P.Model(cl.n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt)
+    om = O.Model(cl.n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt)
+    assert gm.dim == om.ldim and gm.dim < q ** cl.n
+    list1, _, _ = P.mk_list12(cl.n, q, 0, cl.n // 2 * (q - 1))
+    assert len(list1) == gm.dim
+    ctx = P.Context(gm, R=R)
+    rng = np.random.default_rng(5)
+    D = gm.dim
+    v1 = (rng.standard_normal((D, R)) + 1j * rng.standard_normal((D, R))).astype(np.complex128)
+    v0 = (0.3 * rng.standard_normal((D, R))).astype(np.complex128)
+    w = np.ascontiguousarray(v0).reshape(-1).copy()
+    pr = ctx.p_mltply_v3(np.ascontiguousarray(v1).reshape(-1), w, 0.03125)
+    w = w.reshape(D, R)
+    for r in range(R):
+        ref = np.ascontiguousarray(v0[:, r]).copy()
+        prr = om.p_mltply_v3(np.ascontiguousarray(v1[:, r]), ref, 0.03125)
+        assert rel(w[:, r], ref) <= 1e-12
+        assert abs(pr[r] - prr) <= 1e-12 * abs(prr)
+    v = O.gaussian(7, D)
+    v /= np.linalg.norm(v)
+    steps = min(60, D - 1)
+    out = P.Context(gm, R=1).lanczos(v, steps)
+    ref = om.lanczos(v, steps)
+    assert abs(out["ene"][0] - ref["ene"][0]) <= 1e-10 * abs(ref["ene"][0])
+    full = P.Model(cl.n, q, tree, cl.ipair, cl.ibond_type, X, skip, 1)
+    vf = O.gaussian(8, full.dim)
+    vf /= np.linalg.norm(vf)
+    ef = P.Context(full, R=1).lanczos(vf, 120)["ene"][0]
+    assert abs(out["ene"][0] - ef) <= 1e-8 * abs(ef)
+
+
 def test_cg_inverse_iteration():
     cl = honeycomb(2, 2)
     gm, om = models(cl, 2, 0, KH)
