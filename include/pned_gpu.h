@@ -323,6 +323,21 @@ int pned_session_end(pned_ctx *c);
  * the H.v kernel and around the whole step; returns their mean durations.
  */
 int pned_session_profile(pned_ctx *c, int n_steps, double *hv_ms, double *step_ms);
+/*
+ * Checkpoint / restart of a session (the role of interval_dump /
+ * interval_dump_read, S1/2 output.f90:50-211: a long run stops and resumes
+ * later).  save waits for the session's steps and writes its state -- kind,
+ * steps done, device scalars, alpha/beta (and TPS coefficients) so far, and
+ * its three vectors -- to `path` (sections framed by 8-byte lengths).  load
+ * starts the same session on a context of the same basis and R from such a
+ * file, with room for max_steps steps in all (at least the saved count);
+ * steps taken after a load continue the saved run exactly.  Sessions with
+ * observables are not checkpointed (PNED_ENOTSUP).
+ */
+int pned_session_save(pned_ctx *c, const char *path);
+int pned_session_load(pned_ctx *c, const char *path, int max_steps);
+/* The context's session: kind (0 = none), steps enqueued, max_steps, TPS coefficients per step. */
+int pned_session_info(const pned_ctx *c, int *kind, int *steps_done, int *max_steps, int *n_coef);
 
 /* ------------------------------------------------------------------------ */
 /* slot batches: continuous batching of chains with different couplings      */

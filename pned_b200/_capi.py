@@ -61,7 +61,8 @@ EXPORTS = [
     "pned_slots_create", "pned_slots_destroy", "pned_slots_info", "pned_slots_set_stream", "pned_slots_load",
     "pned_slots_load_szq", "pned_slots_load_vector", "pned_slots_release", "pned_slots_step", "pned_slots_query",
     "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column", "pned_lanczos_vector", "pned_slots_set_plan", "pned_slots_plan",
-    "pned_write_salphasbeta", "pned_read_salphasbeta", "pned_tpq_thermo",
+    "pned_write_salphasbeta", "pned_read_salphasbeta", "pned_tpq_thermo", "pned_session_save",
+    "pned_session_load", "pned_session_info",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -133,6 +134,9 @@ def lib() -> C.CDLL:
     L.pned_write_salphasbeta.argtypes = [C.c_char_p, i32, i32, dp, dp, dp]
     L.pned_read_salphasbeta.argtypes = [C.c_char_p, ip, ip, dp, dp, dp, i32]
     L.pned_tpq_thermo.argtypes = [i32, i32, dp, dp, dp, dbl, dbl, i32, dp]
+    L.pned_session_save.argtypes = [vp, C.c_char_p]
+    L.pned_session_load.argtypes = [vp, C.c_char_p, i32]
+    L.pned_session_info.argtypes = [vp, ip, ip, ip, ip]
     _lib = L
     return L
 

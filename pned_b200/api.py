@@ -503,6 +503,18 @@ class Context:
         check(lib().pned_session_vector(self._h, C.byref(p), _dp(sc)))
         return p.value, sc
 
+    def session_save(self, path: str):
+        """Checkpoint of the running session (waits for its enqueued steps)."""
+        check(lib().pned_session_save(self._h, os.fsencode(path)))
+
+    def session_load(self, path: str, max_steps: int = 0):
+        """Resumes a checkpointed session on this context (same basis and R)."""
+        check(lib().pned_session_load(self._h, os.fsencode(path), int(max_steps)))
+        kind, done, ms, nc = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        check(lib().pned_session_info(self._h, C.byref(kind), C.byref(done), C.byref(ms), C.byref(nc)))
+        names = {_capi.SESSION_LANCZOS: "lanczos", _capi.SESSION_TPS: "tps", _capi.SESSION_DSF: "dsf"}
+        self._sess = {"kind": names[kind.value], "max_steps": ms.value, "nobs": max(0, (nc.value - 5) // 2)}
+
     def session_end(self):
         check(lib().pned_session_end(self._h))
         self._sess = None

@@ -6,7 +6,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "device.cuh"
@@ -789,5 +791,165 @@ extern "C" int pned_cg_run(pned_ctx *c, double E, const pned_c128 *b_init, int i
     if (e != cudaSuccess) return cuda_fail(e, "pned_cg_run: result");
     if (n_inv) *n_inv = itr_inv;
     if (n_cg) *n_cg = total_cg;
+    return PNED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// session checkpoint / restart (the role of interval_dump / interval_dump_read,
+// S1/2 output.f90:50-211: Krylov arrays and vectors to a file, resumed later)
+// ---------------------------------------------------------------------------
+namespace pned {
+namespace {
+
+constexpr uint32_t kCkptMagic = 0x54504B43u;   // "CKPT"
+constexpr int32_t kCkptVersion = 1;
+
+// A section: 8-byte length, payload (vectors exceed the 4-byte Fortran record length).
+bool ck_put(FILE *f, const void *p, uint64_t n)
+{
+    return fwrite(&n, 8, 1, f) == 1 && (n == 0 || fwrite(p, 1, size_t(n), f) == size_t(n));
+}
+
+bool ck_get(FILE *f, void *p, uint64_t n)
+{
+    uint64_t m = 0;
+    return fread(&m, 8, 1, f) == 1 && m == n && (n == 0 || fread(p, 1, size_t(n), f) == size_t(n));
+}
+
+// Device vector to file (or back) through a bounded host buffer.
+bool ck_put_dev(FILE *f, const double2 *d, uint64_t bytes, cudaStream_t st)
+{
+    if (fwrite(&bytes, 8, 1, f) != 1) return false;
+    const uint64_t chunk = uint64_t(1) << 28;
+    std::vector<char> h(size_t(std::min(bytes, chunk)));
+    for (uint64_t o = 0; o < bytes; o += chunk) {
+        const size_t n = size_t(std::min(chunk, bytes - o));
+        if (cudaMemcpyAsync(h.data(), reinterpret_cast<const char *>(d) + o, n, cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess || fwrite(h.data(), 1, n, f) != n)
+            return false;
+    }
+    return true;
+}
+
+bool ck_get_dev(FILE *f, double2 *d, uint64_t bytes, cudaStream_t st)
+{
+    uint64_t m = 0;
+    if (fread(&m, 8, 1, f) != 1 || m != bytes) return false;
+    const uint64_t chunk = uint64_t(1) << 28;
+    std::vector<char> h(size_t(std::min(bytes, chunk)));
+    for (uint64_t o = 0; o < bytes; o += chunk) {
+        const size_t n = size_t(std::min(chunk, bytes - o));
+        if (fread(h.data(), 1, n, f) != n ||
+            cudaMemcpyAsync(reinterpret_cast<char *>(d) + o, h.data(), n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return false;
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace pned
+
+extern "C" int pned_session_save(pned_ctx *c, const char *path)
+{
+    if (!c || !path) return fail(PNED_EINVAL, "pned_session_save: bad arguments");
+    Session &S = c->sess;
+    if (!S.kind) return fail(PNED_EINVAL, "pned_session_save: no session");
+    if (S.nobs) return fail(PNED_ENOTSUP, "pned_session_save: sessions with observables are not checkpointed");
+    cudaSetDevice(c->m->device);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_save");
+    const int R = c->R, k = S.enqueued;
+    const size_t nh = size_t(k) * R;
+    std::vector<double> scal(size_t(kScalSlots) * kMaxR), a(nh), b(nh), cf(nh * std::max(1, S.ncoef));
+    int32_t counters[2] = {0, 0};
+    e = cudaMemcpy(scal.data(), c->scal, sizeof(double) * scal.size(), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && nh) e = cudaMemcpy(a.data(), S.d_alpha, sizeof(double) * nh, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && nh) e = cudaMemcpy(b.data(), S.d_beta, sizeof(double) * nh, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && nh && S.d_coef)
+        e = cudaMemcpy(cf.data(), S.d_coef, sizeof(double) * nh * S.ncoef, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(counters, S.d_counter, sizeof(int32_t) * 2, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_save: reading the session");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_session_save: cannot open ") + path);
+    const int64_t dim = c->m->dim;
+    int32_t hdr[10] = {int32_t(kCkptMagic), kCkptVersion, S.kind, R, k, S.max_steps, S.ncoef, S.b0, S.b1, S.b2};
+    bool ok = ck_put(f, hdr, sizeof(hdr)) && ck_put(f, &dim, 8) && ck_put(f, &S.L, 8) &&
+              ck_put(f, counters, sizeof(counters)) && ck_put(f, scal.data(), sizeof(double) * scal.size()) &&
+              ck_put(f, a.data(), sizeof(double) * nh) && ck_put(f, b.data(), sizeof(double) * nh) &&
+              ck_put(f, cf.data(), sizeof(double) * (S.d_coef ? nh * S.ncoef : 0));
+    const uint64_t vb = sizeof(double2) * uint64_t(dim) * R;
+    for (int r : {S.b0, S.b1, S.b2})
+        if (ok) ok = ck_put_dev(f, c->buf[r], vb, c->stream);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_session_save: write failed");
+}
+
+extern "C" int pned_session_load(pned_ctx *c, const char *path, int max_steps)
+{
+    if (!c || !path) return fail(PNED_EINVAL, "pned_session_load: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_session_load: cannot open ") + path);
+    int32_t hdr[10];
+    int64_t dim = 0;
+    double L = 0.0;
+    int32_t counters[2];
+    bool ok = ck_get(f, hdr, sizeof(hdr)) && hdr[0] == int32_t(kCkptMagic) && hdr[1] == kCkptVersion &&
+              ck_get(f, &dim, 8) && ck_get(f, &L, 8) && ck_get(f, counters, sizeof(counters));
+    if (!ok) { std::fclose(f); return fail(PNED_EINVAL, "pned_session_load: not a session checkpoint"); }
+    const int kind = hdr[2], R = hdr[3], k = hdr[4], ncoef = hdr[6];
+    if (R != c->R || dim != c->m->dim) {
+        std::fclose(f);
+        return fail(PNED_EINVAL, "pned_session_load: checkpoint of another basis size or vector count");
+    }
+    if (max_steps < k) max_steps = hdr[5];
+    cudaSetDevice(c->m->device);
+    int rc = session_common_begin(c, kind, std::max(max_steps, k));
+    if (rc) { std::fclose(f); return rc; }
+    cudaError_t e0 = cudaStreamSynchronize(c->stream);   // the begin's resets land before the restores
+    if (e0 != cudaSuccess) { std::fclose(f); session_release(c); return cuda_fail(e0, "pned_session_load"); }
+    Session &S = c->sess;
+    S.L = L;
+    S.ncoef = ncoef;
+    S.b0 = hdr[7]; S.b1 = hdr[8]; S.b2 = hdr[9];
+    const size_t nh = size_t(k) * R;
+    std::vector<double> scal(size_t(kScalSlots) * kMaxR), a(nh), b(nh), cf(kind == PNED_SESSION_TPS ? nh * ncoef : 0);
+    if (kind == PNED_SESSION_TPS) {
+        S.d_coef = sess_alloc<double>(S, size_t(S.max_steps) * R * ncoef);
+        S.d_osum = sess_alloc<double2>(S, size_t(2) * R);
+        if (!S.d_coef || !S.d_osum) { std::fclose(f); session_release(c); return fail(PNED_ENOMEM, "session"); }
+    }
+    ok = ck_get(f, scal.data(), sizeof(double) * scal.size()) && ck_get(f, a.data(), sizeof(double) * nh) &&
+         ck_get(f, b.data(), sizeof(double) * nh) && ck_get(f, cf.data(), sizeof(double) * cf.size());
+    cudaError_t e = cudaSuccess;
+    if (ok) {
+        e = cudaMemcpy(c->scal, scal.data(), sizeof(double) * scal.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && nh) e = cudaMemcpy(S.d_alpha, a.data(), sizeof(double) * nh, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && nh) e = cudaMemcpy(S.d_beta, b.data(), sizeof(double) * nh, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !cf.empty())
+            e = cudaMemcpy(S.d_coef, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(S.d_counter, counters, sizeof(int32_t) * 2, cudaMemcpyHostToDevice);
+    }
+    const uint64_t vb = sizeof(double2) * uint64_t(dim) * R;
+    for (int r : {S.b0, S.b1, S.b2})
+        if (ok && e == cudaSuccess) ok = ck_get_dev(f, c->buf[r], vb, c->stream);
+    std::fclose(f);
+    if (!ok || e != cudaSuccess) {
+        session_release(c);
+        return e != cudaSuccess ? cuda_fail(e, "pned_session_load") : fail(PNED_EINVAL, "pned_session_load: short file");
+    }
+    S.enqueued = k;
+    return PNED_OK;
+}
+
+extern "C" int pned_session_info(const pned_ctx *c, int *kind, int *steps_done, int *max_steps, int *n_coef)
+{
+    if (!c) return fail(PNED_EINVAL, "pned_session_info: null context");
+    const Session &S = c->sess;
+    if (kind) *kind = S.kind;
+    if (steps_done) *steps_done = S.enqueued;
+    if (max_steps) *max_steps = S.max_steps;
+    if (n_coef) *n_coef = S.ncoef;
     return PNED_OK;
 }

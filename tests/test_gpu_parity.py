@@ -299,6 +299,39 @@ def test_sector_hv_and_lanczos(case):
     assert abs(out["ene"][0] - ef) <= 1e-8 * abs(ef)
 
 
+@pytest.mark.parametrize("kind", ["lanczos", "tps"])
+def test_session_checkpoint_resumes_exactly(kind, tmp_path):
+    """A session saved after 9 steps and loaded into a fresh context continues
+    exactly as the uninterrupted run (the role of interval_dump / _read)."""
+    cl = honeycomb(3, 2)
+    L = 2.0 * cl.n
+    R = 2
+    gm, _ = models(cl, 2, 0, KHGH, FIELD, tps_L=L if kind == "tps" else None)
+    V = O.gaussian(41, gm.dim, R).reshape(gm.dim, R)
+    V /= np.linalg.norm(V, axis=0)
+    v = np.ascontiguousarray(V).reshape(-1)
+    a = P.Context(gm, R=R)
+    a.session_begin(kind, v, 25, L=L)
+    a.session_step(20)
+    full = a.session_read()
+    a.session_end()
+    b = P.Context(gm, R=R)
+    b.session_begin(kind, v, 25, L=L)
+    b.session_step(9)
+    path = str(tmp_path / "session.ckpt")
+    b.session_save(path)
+    b.session_end()
+    c = P.Context(gm, R=R)
+    c.session_load(path, 25)
+    c.session_step(11)
+    resumed = c.session_read()
+    assert np.array_equal(resumed["alpha"], full["alpha"]) and np.array_equal(resumed["beta"], full["beta"])
+    if kind == "tps":
+        assert np.array_equal(resumed["coef"], full["coef"])
+    with pytest.raises(P.PnedError):
+        P.Context(gm, R=1).session_load(path, 25)
+
+
 def test_cg_inverse_iteration():
     cl = honeycomb(2, 2)
     gm, om = models(cl, 2, 0, KH)
