@@ -156,6 +156,20 @@ class CpuSample:
         return (time.perf_counter() - t0) * self.scale
 
 
+def replica_aggregate(ms_local: float, steps: int, world: int, device="cuda"):
+    """Whole-job figure of independent replicas: the slowest rank's time (max
+    over ranks, after a barrier) and all ranks' steps over it."""
+    ms = float(ms_local)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms, world * steps / (ms * 1e-3)
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference CPU algorithm, timed on the host cores."""
     if rank != 0:
@@ -217,12 +231,7 @@ def run_ours(args, rank, world, local_rank):
         ctx.session_step(args.steps)
         end.record(stream)
         torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms, value = replica_aggregate(start.elapsed_time(end), args.steps, world, device=dev)
     res = ctx.session_read()
     # --- per-kernel timing for the roofline (CUDA events on the context's stream)
     hv_ms, step_ms = ctx.session_profile(args.profile_steps)
@@ -260,7 +269,6 @@ def run_ours(args, rank, world, local_rank):
     achieved = bytes_hv / (hv_ms * 1e-3) / 1e9
     # kernels per step: the H.v launches (one per tile pass), finish, residual, finish, epilogue
     launches_per_step = max(1, plan["tile_passes"]) + 4
-    value = world * args.steps / (ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -451,6 +451,20 @@ int pned_read_salphasbeta(const char *path, int *num_data1, int *num_data2, doub
  */
 int pned_tpq_thermo(int num_data1, int n_seeds, const double *beta, const double *energy, const double *hmix,
                     double t_min, double t_max, int num_div, double *out);
+/*
+ * The ground-state vector file basisme%05d (readwrite_vec_data, S1/2
+ * output.f90:12-36): two records, the energy e (double) and x[ll] (complex);
+ * records above 2^31 bytes (ll > 2^27) would need Fortran subrecords and are
+ * refused (PNED_ENOTSUP).
+ */
+int pned_write_vec_data(const char *path, double e, const pned_c128 *x, int64_t ll);
+int pned_read_vec_data(const char *path, double *e, pned_c128 *x, int64_t ll);
+/* SalphaSbeta_q%05dme%05d<comp> (dump_alpha_beta, S1/2 DSF.f90:353-379): sq, salpha[s_maxitr], sbeta[s_maxitr]. */
+int pned_write_dsf_alpha_beta(const char *path, pned_c128 sq, const double *salpha, const double *sbeta, int s_maxitr);
+int pned_read_dsf_alpha_beta(const char *path, pned_c128 *sq, double *salpha, double *sbeta, int s_maxitr);
+/* Appends one momentum's block of the text spectrum (write_dsf_res, S1/2 output.f90:246-264). */
+int pned_append_dsf_res(const char *path, double sq_re, const double *q2, const double *w, const double *dsf,
+                        const int *conv, int ll);
 
 #ifdef __cplusplus
 }

@@ -62,7 +62,8 @@ EXPORTS = [
     "pned_slots_load_szq", "pned_slots_load_vector", "pned_slots_release", "pned_slots_step", "pned_slots_query",
     "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column", "pned_lanczos_vector", "pned_slots_set_plan", "pned_slots_plan",
     "pned_write_salphasbeta", "pned_read_salphasbeta", "pned_tpq_thermo", "pned_session_save",
-    "pned_session_load", "pned_session_info",
+    "pned_session_load", "pned_session_info", "pned_write_vec_data", "pned_read_vec_data",
+    "pned_write_dsf_alpha_beta", "pned_read_dsf_alpha_beta", "pned_append_dsf_res",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -137,6 +138,11 @@ def lib() -> C.CDLL:
     L.pned_session_save.argtypes = [vp, C.c_char_p]
     L.pned_session_load.argtypes = [vp, C.c_char_p, i32]
     L.pned_session_info.argtypes = [vp, ip, ip, ip, ip]
+    L.pned_write_vec_data.argtypes = [C.c_char_p, dbl, vp, i64]
+    L.pned_read_vec_data.argtypes = [C.c_char_p, dp, vp, i64]
+    L.pned_write_dsf_alpha_beta.argtypes = [C.c_char_p, c128, dp, dp, i32]
+    L.pned_read_dsf_alpha_beta.argtypes = [C.c_char_p, C.POINTER(c128), dp, dp, i32]
+    L.pned_append_dsf_res.argtypes = [C.c_char_p, dbl, dp, dp, dp, ip, i32]
     _lib = L
     return L
 

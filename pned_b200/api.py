@@ -164,6 +164,44 @@ def tpq_thermo(beta, energy, hmix, t_min: float, t_max: float, num_div: int):
     return out
 
 
+def write_vec_data(path: str, e: float, x):
+    """readwrite_vec_data (write): the energy and the vector x (complex128, host)."""
+    xs = np.ascontiguousarray(x, dtype=np.complex128)
+    check(lib().pned_write_vec_data(os.fsencode(path), float(e), C.c_void_p(xs.ctypes.data), xs.size))
+
+
+def read_vec_data(path: str, ll: int):
+    e = C.c_double(0.0)
+    x = np.zeros(int(ll), dtype=np.complex128)
+    check(lib().pned_read_vec_data(os.fsencode(path), C.byref(e), C.c_void_p(x.ctypes.data), int(ll)))
+    return e.value, x
+
+
+def write_dsf_alpha_beta(path: str, sq: complex, salpha, sbeta):
+    a = np.ascontiguousarray(salpha, dtype=np.float64)
+    b = np.ascontiguousarray(sbeta, dtype=np.float64)
+    if a.shape != b.shape:
+        raise ValueError("salpha and sbeta need the same length (s_maxitr)")
+    check(lib().pned_write_dsf_alpha_beta(os.fsencode(path), _capi.c128(complex(sq).real, complex(sq).imag),
+                                          _dp(a), _dp(b), a.size))
+
+
+def read_dsf_alpha_beta(path: str, s_maxitr: int):
+    sq = _capi.c128(0.0, 0.0)
+    a, b = np.zeros(int(s_maxitr)), np.zeros(int(s_maxitr))
+    check(lib().pned_read_dsf_alpha_beta(os.fsencode(path), C.byref(sq), _dp(a), _dp(b), int(s_maxitr)))
+    return complex(sq.re, sq.im), a, b
+
+
+def append_dsf_res(path: str, sq_re: float, q, w, dsf, conv):
+    q2 = np.ascontiguousarray(q, dtype=np.float64)[:2].copy()
+    w_ = np.ascontiguousarray(w, dtype=np.float64)
+    d_ = np.ascontiguousarray(dsf, dtype=np.float64)
+    c_ = np.ascontiguousarray(conv, dtype=np.int32)
+    check(lib().pned_append_dsf_res(os.fsencode(path), float(sq_re), _dp(q2), _dp(w_), _dp(d_),
+                                    c_.ctypes.data_as(C.POINTER(C.c_int)), w_.size))
+
+
 # --------------------------------------------------------------------------- model / context
 
 

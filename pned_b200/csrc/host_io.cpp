@@ -178,3 +178,78 @@ extern "C" int pned_tpq_thermo(int num_data1, int n_seeds, const double *beta, c
     }
     return PNED_OK;
 }
+
+// ---------------------------------------------------------------------------
+// the reference's other output files
+// ---------------------------------------------------------------------------
+extern "C" int pned_write_vec_data(const char *path, double e, const pned_c128 *x, int64_t ll)
+{
+    if (!path || !x || ll < 1) return fail(PNED_EINVAL, "pned_write_vec_data: bad arguments");
+    if (uint64_t(ll) * 16 > 0x7fffffffu)
+        return fail(PNED_ENOTSUP, "pned_write_vec_data: vectors above 2^31 bytes need Fortran subrecords");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_write_vec_data: cannot open ") + path);
+    bool ok = put_record(f, &e, 8) && put_record(f, x, size_t(ll) * 16);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_write_vec_data: write failed");
+}
+
+extern "C" int pned_read_vec_data(const char *path, double *e, pned_c128 *x, int64_t ll)
+{
+    if (!path || !e || !x || ll < 1) return fail(PNED_EINVAL, "pned_read_vec_data: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_read_vec_data: cannot open ") + path);
+    std::vector<char> r1, r2;
+    const bool ok = get_record(f, r1) && r1.size() == 8 && get_record(f, r2) && r2.size() == size_t(ll) * 16;
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_read_vec_data: not a vector file of this length");
+    std::memcpy(e, r1.data(), 8);
+    std::memcpy(x, r2.data(), r2.size());
+    return PNED_OK;
+}
+
+extern "C" int pned_write_dsf_alpha_beta(const char *path, pned_c128 sq, const double *salpha, const double *sbeta,
+                                         int s_maxitr)
+{
+    if (!path || !salpha || !sbeta || s_maxitr < 1) return fail(PNED_EINVAL, "pned_write_dsf_alpha_beta: bad arguments");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_write_dsf_alpha_beta: cannot open ") + path);
+    bool ok = put_record(f, &sq, 16) && put_record(f, salpha, sizeof(double) * size_t(s_maxitr)) &&
+              put_record(f, sbeta, sizeof(double) * size_t(s_maxitr));
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_write_dsf_alpha_beta: write failed");
+}
+
+extern "C" int pned_read_dsf_alpha_beta(const char *path, pned_c128 *sq, double *salpha, double *sbeta, int s_maxitr)
+{
+    if (!path || !sq || !salpha || !sbeta || s_maxitr < 1)
+        return fail(PNED_EINVAL, "pned_read_dsf_alpha_beta: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_read_dsf_alpha_beta: cannot open ") + path);
+    std::vector<char> r1, r2, r3;
+    const size_t n = sizeof(double) * size_t(s_maxitr);
+    const bool ok = get_record(f, r1) && r1.size() == 16 && get_record(f, r2) && r2.size() == n && get_record(f, r3) &&
+                    r3.size() == n;
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_read_dsf_alpha_beta: not a DSF coefficient file of this length");
+    std::memcpy(sq, r1.data(), 16);
+    std::memcpy(salpha, r2.data(), n);
+    std::memcpy(sbeta, r3.data(), n);
+    return PNED_OK;
+}
+
+extern "C" int pned_append_dsf_res(const char *path, double sq_re, const double *q2, const double *w, const double *dsf,
+                                   const int *conv, int ll)
+{
+    if (!path || !q2 || !w || !dsf || !conv || ll < 1) return fail(PNED_EINVAL, "pned_append_dsf_res: bad arguments");
+    FILE *f = std::fopen(path, "a");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_append_dsf_res: cannot open ") + path);
+    // write_dsf_res (S1/2 output.f90:246-264): '(A,F25.18)', then '(2F18.10,2F25.16,I5)' per
+    // point, then four list-directed empty records (a single blank each)
+    bool ok = std::fprintf(f, "#        %25.18f\n", sq_re) > 0;
+    for (int k = 0; k < ll && ok; ++k)
+        ok = std::fprintf(f, "%18.10f%18.10f%25.16f%25.16f%5d\n", q2[0], q2[1], w[k], dsf[k], conv[k]) > 0;
+    for (int k = 0; k < 4 && ok; ++k) ok = std::fputs(" \n", f) >= 0;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_append_dsf_res: write failed");
+}

@@ -152,3 +152,50 @@ def test_tpq_thermo_matches_oracle():
     assert np.all(np.diff(got[:, 1]) > 0) and np.all(got[:, 2] > 0) and np.all(got[:, 3] >= -1e-12)
     e0 = np.linalg.eigvalsh(dense_h(cl.n, 2, 0, cl.ipair, cl.ibond_type, cpl))[0]
     assert abs(got[0, 1] - e0) <= 0.02 * abs(e0)
+
+
+def test_vector_and_dsf_files_layout(tmp_path):
+    import struct
+
+    def rec(payload):
+        return struct.pack("<i", len(payload)) + payload + struct.pack("<i", len(payload))
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(37) + 1j * rng.standard_normal(37)
+    p = str(tmp_path / "basisme00000")
+    P.api.write_vec_data(p, -3.25, x)
+    assert open(p, "rb").read() == rec(struct.pack("<d", -3.25)) + rec(x.astype("<c16").tobytes())
+    e, x2 = P.api.read_vec_data(p, 37)
+    assert e == -3.25 and np.array_equal(x2, x)
+    with pytest.raises(P.PnedError):
+        P.api.read_vec_data(p, 36)
+    sa, sb = rng.standard_normal(12), rng.standard_normal(12)
+    q = str(tmp_path / "SalphaSbeta_q00003me00000zz")
+    P.api.write_dsf_alpha_beta(q, 0.5 - 0.25j, sa, sb)
+    assert open(q, "rb").read() == (rec(struct.pack("<dd", 0.5, -0.25)) + rec(sa.astype("<f8").tobytes()) +
+                                    rec(sb.astype("<f8").tobytes()))
+    sq, sa2, sb2 = P.api.read_dsf_alpha_beta(q, 12)
+    assert sq == 0.5 - 0.25j and np.array_equal(sa2, sa) and np.array_equal(sb2, sb)
+
+
+def test_dsf_res_text_block(tmp_path):
+    p = str(tmp_path / "dsf_res_zz")
+    P.api.append_dsf_res(p, 0.75, [0.5, -1.25], [0.0, 1.5], [2.0, 0.125], [3, 4])
+    P.api.append_dsf_res(p, 0.5, [0.0, 0.0], [0.25], [1.0], [1])
+    lines = open(p).read().split("\n")
+    assert lines[0] == "#        " + "%25.18f" % 0.75
+    assert lines[1] == "%18.10f%18.10f%25.16f%25.16f%5d" % (0.5, -1.25, 0.0, 2.0, 3)
+    assert lines[2] == "%18.10f%18.10f%25.16f%25.16f%5d" % (0.5, -1.25, 1.5, 0.125, 4)
+    assert lines[3:7] == [" "] * 4 and lines[7].startswith("#")
+
+
+def test_rejects_bad_arguments():
+    with pytest.raises(ValueError):
+        P.build_xlocal(2, 0, np.zeros(5))
+    with pytest.raises(P.PnedError):
+        P.api.tpq_thermo(np.ones((1, 4)), np.ones((1, 4)), np.ones((1, 4)), -1.0, 2.0, 4)
+    with pytest.raises(P.PnedError):
+        P.api.read_salphasbeta("/nonexistent/file")
+    with pytest.raises(P.PnedError):
+        P.mk_list12(0, 2, 0, 0)
+    with pytest.raises(P.PnedError):
+        P.bisec(np.ones(3), np.ones(3), 0, 1)

@@ -332,6 +332,17 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
         P.Context(gm, R=1).session_load(path, 25)
 
 
+def test_lanczos_breakdown_is_reported():
+    """A start vector that is an eigenvector makes beta vanish after one step: the
+    run returns PNED_EBREAKDOWN (the reference stops with #(E07), Lanczos.f90:126-130)."""
+    X, skip, _ = P.build_xlocal(2, 0, CP.kitaev_heisenberg(1.0, 0.0))
+    m = P.Model(2, 2, 0, np.array([1, 2]), np.array([3]), X, skip, 1)
+    singlet = np.array([0, 1, -1, 0], dtype=np.complex128) / np.sqrt(2.0)
+    with pytest.raises(P.PnedError) as ei:
+        P.Context(m, R=1).lanczos(singlet, 5)
+    assert ei.value.code == 4
+
+
 def test_cg_inverse_iteration():
     cl = honeycomb(2, 2)
     gm, om = models(cl, 2, 0, KH)
