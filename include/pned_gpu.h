@@ -148,6 +148,7 @@ typedef struct {
     int32_t max_passes;
     int32_t j_bits;
     int32_t l1_carveout;   /* 1 (default): shared-memory carveout sized to the tiles, the rest L1; 0: driver's choice */
+    int32_t stage_partner_tiles; /* R = 1, j_bits 3: 1 copies each partner tile into shared memory once (cp.async) */
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 

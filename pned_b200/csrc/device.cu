@@ -267,6 +267,156 @@ __global__ void __launch_bounds__(kThreads, tile_blocks_per_sm(JB))
     block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
 }
 
+// cp.async (Ampere-style asynchronous global -> shared copies, 16 bytes a thread).
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Single-vector tiled H.v with staged partner tiles: the same tiles and
+// passes as hv_tile_kernel, but each partner tile (the terms of one group) is
+// copied into shared memory once with cp.async, two buffers deep (group g + 1
+// loads while group g is computed), and all terms of the group gather from
+// there.  L2 sends each partner tile once instead of once per term, and the
+// copies in flight hold no registers.
+template <bool RC, bool RD, int K>
+__global__ void __launch_bounds__(kThreads, 2)
+    hv_tile_stage_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
+{
+    constexpr int SPT = 8;
+    constexpr int TILE = kThreads * SPT;
+    extern __shared__ double2 smem[];
+    double2 *s_v = smem;              // own tile
+    double2 *s_p = smem + TILE;       // two partner-tile buffers
+    double2 *s_tab = smem + 3 * TILE;
+    for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
+    const uint32_t tid = threadIdx.x;
+    const int64_t ntiles = int64_t(1) << prog.nouter;
+    double2 red[K][1];
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k][0] = make_double2(0.0, 0.0);
+    const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
+    const double hs = a.hsc ? a.hsc[0] : sc;
+    const double shift = a.shift + (a.shiftv ? a.shiftv[0] : 0.0);
+    uint32_t rowbase = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) rowbase |= ((tid >> k) & 1u) << prog.rowpos[k];
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint32_t base = rowbase;
+        for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
+        double2 acc[SPT];
+        {
+            double2 v[SPT];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) v[j] = __ldg(a.C + (base | prog.jexp[j]));
+            __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) s_v[tid + kThreads * j] = v[j];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const uint32_t sj = base | prog.jexp[j];
+                if (!prog.first) {
+                    acc[j] = make_double2(0.0, 0.0);
+                } else if (RD) {
+                    acc[j] = cscale(__ldcs(static_cast<const double *>(a.diag) + sj) - shift, v[j]);
+                } else {
+                    double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + sj);
+                    dd.x -= shift;
+                    acc[j] = cmul(dd, v[j]);
+                }
+            }
+        }
+        // the first partner tile loads while the in-tile terms run
+        if (prog.ngroups > 0) {
+            const uint32_t pb = base ^ prog.gxor[0];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) cp_async16(s_p + tid + kThreads * j, a.C + (pb | prog.jexp[j]));
+            cp_async_commit();
+        }
+        __syncthreads();
+        for (int t = 0; t < prog.nin; ++t) {
+            const TileTerm T = prog.t[t];
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            const double2 *sv = s_v + (tid ^ (T.mask & 0xffu));
+            const uint32_t mhi = T.mask >> 8;
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
+                const double2 w = sv[kThreads * (j ^ mhi)];
+                if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                else acc[j] = cfma(c, w, acc[j]);
+            }
+        }
+        for (int g = 0; g < prog.ngroups; ++g) {
+            double2 *buf = s_p + (g & 1) * TILE;
+            if (g + 1 < prog.ngroups) {
+                // its buffer was released by the barrier that ended group g - 1
+                const uint32_t pb = base ^ prog.gxor[g + 1];
+                double2 *nb = s_p + ((g + 1) & 1) * TILE;
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) cp_async16(nb + tid + kThreads * j, a.C + (pb | prog.jexp[j]));
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();   // group g's tile has landed for every thread
+            for (int t = prog.gstart[g]; t < prog.gstart[g + 1]; ++t) {
+                const TileTerm T = prog.t[t];
+                uint32_t ib = 0;
+#pragma unroll
+                for (int d = 0; d < kMaxDeps; ++d)
+                    if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+                const double2 *sv = buf + (tid ^ (T.lmask & 0xffu));
+                const uint32_t mhi = T.lmask >> 8;
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
+                    const double2 w = sv[kThreads * (j ^ mhi)];
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+            }
+            __syncthreads();   // every thread is done with buf before it is refilled
+        }
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            const int64_t e = base | prog.jexp[j];
+            const double2 hv = cscale(hs, acc[j]);
+            double2 out = hv;
+            if (!prog.first) {
+                const double2 w0 = __ldcs(a.W + e);
+                out.x += w0.x;
+                out.y += w0.y;
+            } else if (a.P) {
+                const double2 p = __ldcs(a.P + e);
+                out.x = fma(pc, p.x, out.x);
+                out.y = fma(pc, p.y, out.y);
+            }
+            __stcs(a.W + e, out);
+            const double2 vv = cscale(sc, s_v[tid + kThreads * j]);
+            red[0][0] = cadd(red[0][0], cconjmul(vv, hv));
+            if (!prog.last) continue;
+            if (K >= 2) red[1][0].x += out.x * out.x + out.y * out.y;
+            if (K >= 4 && a.G) {
+                const double2 gv = cscale(gs, a.G[e]);
+                red[2][0] = cadd(red[2][0], cconjmul(gv, out));
+                red[3][0] = cadd(red[3][0], cconjmul(gv, vv));
+            }
+        }
+    }
+    block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
+}
+
 // Tiled multi-vector H.V (R > 1 interleaved vectors, S = 1/2 full basis), one
 // pass of a multi-pass program.  G = R / VPT threads share a state; a block
 // owns a tile of NS * SPT states (NS = 256 / G state rows): thread t serves
@@ -674,8 +824,28 @@ static cudaError_t launch_tile_j(const pned_model *m, const HvArgs &a, int nbloc
 }
 
 template <bool RC, bool RD, int K>
+static cudaError_t launch_tile_stage(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    auto kern = hv_tile_stage_kernel<RC, RD, K>;
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+    const size_t smem = sizeof(double2) * (size_t(3) * kThreads * 8 + std::max(1, m->ntab));
+    if (e == cudaSuccess && m->carveout) e = set_carveout(reinterpret_cast<const void *>(kern), m->device, smem, 2);
+    if (e != cudaSuccess) return e;
+    const int grid = tile_grid(m, nblocks);
+    HvArgs b = a;
+    for (size_t p = 0; p < m->tprogs.size(); ++p) {
+        b.partials = a.partials + size_t(p) * grid * K * a.R;
+        kern<<<grid, kThreads, smem, st>>>(*m->tprogs[p], b);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <bool RC, bool RD, int K>
 static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
+    if (m->tile_stage && m->tile_jb == 3) return launch_tile_stage<RC, RD, K>(m, a, nblocks, st);
     switch (m->tile_jb) {
     case 1: return launch_tile_j<1, RC, RD, K>(m, a, nblocks, st);
     case 2: return launch_tile_j<2, RC, RD, K>(m, a, nblocks, st);
@@ -928,6 +1098,7 @@ void build_tile_programs(pned_model *m)
     if (hp.q == 2 && !hp.sector && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes) == PNED_OK) {
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
+        m->tile_stage = m->plan1.stage_partner_tiles > 0;
         m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
         m->use_tile = true;
     }
@@ -1128,12 +1299,12 @@ extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *p
                  plan->j_bits > kTileMaxJB || plan->j_bits == 0))
         return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
     if (R == 1) {
-        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1};
+        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1};
         m->carveout = m->plan1.l1_carveout != 0;
         build_tile_programs(m);
         return PNED_OK;
     }
-    const pned_tile_plan def{-1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1};
     if (plan) m->carveout = plan->l1_carveout != 0;
     ensure_rtiles(m, R, false, plan ? plan : &def);
     return PNED_OK;

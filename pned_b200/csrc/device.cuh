@@ -29,9 +29,10 @@ struct pned_model {
     };
     std::map<int, TileSet> rtiles;
     std::mutex rtiles_mu;
-    pned_tile_plan plan1{-1, -1, -1, -1, -1};   // single-vector plan parameters (-1: defaults)
+    pned_tile_plan plan1{-1, -1, -1, -1, -1, -1};   // single-vector plan parameters (-1: defaults)
     int tile_jb = 3;                        // j bits (rows per thread 2^jb) of the single-vector tiles
     bool carveout = true;                   // size the shared-memory carveout to the tiles (rest L1)
+    bool tile_stage = false;                // single-vector: partner tiles staged in shared memory
     int nsm = 148;
     double2 *d_table = nullptr;
     void *d_diag = nullptr;

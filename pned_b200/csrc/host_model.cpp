@@ -614,6 +614,7 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
                 in.push_back(q);
             } else {
                 q.mask = t.xmask;
+                q.lmask = local(t.xmask & tilemask);
                 out.push_back({t.xmask & ~tilemask, q});
             }
         }

@@ -56,6 +56,7 @@ struct TileTerm {
     uint16_t tab;    // coefficient table offset
     uint8_t nb;      // number of dependency bits
     uint8_t hasj;    // 1 if a dependency bit is a j-bit
+    uint32_t lmask;  // out-of-tile: local xor of the mask's in-tile part (the offset inside the partner tile)
 };
 constexpr int kTileMaxJB = 3;
 constexpr int kTileWindowBits = 10;   // outer bits whose partner tiles stay in L2 during a sweep

@@ -332,6 +332,31 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
         P.Context(gm, R=1).session_load(path, 25)
 
 
+@pytest.mark.parametrize("plan", [(8, 10, 4, 3, 1, 1), (5, 10, 2, 3, 1, 1), (3, 8, 1, 3, 1, 1), (5, 12, 2, 2, 1, 0),
+                                  (5, 12, 2, 1, 0, 0)])
+def test_tile_plans_agree_with_oracle(plan):
+    """Every tile plan the autotuner may pick (rows kept, window, passes, rows per
+    thread, carveout, staged partner tiles) gives the oracle's H.v to 1e-12."""
+    cl = honeycomb(2, 4)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    got = gm.set_plan(1, *plan)
+    assert got["tile_passes"] >= 1
+    ctx = P.Context(gm, R=1)
+    rng = np.random.default_rng(23)
+    v1 = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
+    v0 = 0.1 * rng.standard_normal(gm.dim) + 0j
+    w = v0.copy()
+    pr = ctx.p_mltply_v3(v1, w, 0.0625)
+    ref = v0.copy()
+    prr = om.p_mltply_v3(v1, ref, 0.0625)
+    assert rel(w, ref) <= 1e-12 and abs(pr[0] - prr) <= 1e-12 * abs(prr)
+    v = O.gaussian(9, gm.dim)
+    v /= np.linalg.norm(v)
+    out = ctx.lanczos(v, 30)
+    refl = om.lanczos(v, 30)
+    assert rel(out["alpha"][:12, 0], refl["alpha"][:12]) <= 1e-10
+
+
 def test_lanczos_breakdown_is_reported():
     """A start vector that is an eigenvector makes beta vanish after one step: the
     run returns PNED_EBREAKDOWN (the reference stops with #(E07), Lanczos.f90:126-130)."""
