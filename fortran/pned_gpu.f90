@@ -8,6 +8,8 @@ module pned_gpu
   implicit none
   private
   public :: pned_gpu_init, pned_gpu_finalize, p_mltply_v3_gpu, calc_vec_inprdct_gpu, pned_lanczos_run_f
+  public :: pned_lncv1_f, pned_inv1_f, pned_tps_run_f, pned_dump_alpha_beta_coef_f
+  public :: pned_lanczos_begin_f, pned_steps_f, pned_lanczos_read_f, pned_interval_dump_f, pned_interval_dump_read_f
 
   type, bind(C) :: pned_model_desc
     integer(c_int32_t) :: n_sites, q_spin, tree, n_bonds
@@ -52,6 +54,70 @@ module pned_gpu
       integer(c_int), value :: nsteps, check_conv, flags
       real(c_double), intent(out) :: alpha(*), beta(*), ene(8)
       integer(c_int), intent(out) :: done
+    end function
+    integer(c_int) function pned_lanczos_vector(c, v, nsteps, alpha, beta, coef, x, flags) &
+        bind(C, name="pned_lanczos_vector")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c
+      complex(c_double_complex), intent(in) :: v(*)
+      integer(c_int), value :: nsteps, flags
+      real(c_double), intent(in) :: alpha(*), beta(*), coef(*)
+      complex(c_double_complex), intent(out) :: x(*)
+    end function
+    integer(c_int) function pned_cg_run(c, e, b, inv_max, cg_max, x, n_inv, n_cg, flags) bind(C, name="pned_cg_run")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c
+      real(c_double), value :: e
+      complex(c_double_complex), intent(in) :: b(*)
+      integer(c_int), value :: inv_max, cg_max, flags
+      complex(c_double_complex), intent(out) :: x(*)
+      integer(c_int), intent(out) :: n_inv, n_cg
+    end function
+    integer(c_int) function pned_tps_run(c, L, v, nsteps, nobs, obs, alpha, beta, coef, flags) &
+        bind(C, name="pned_tps_run")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c, obs
+      real(c_double), value :: L
+      complex(c_double_complex), intent(in) :: v(*)
+      integer(c_int), value :: nsteps, nobs, flags
+      real(c_double), intent(out) :: alpha(*), beta(*), coef(*)
+    end function
+    integer(c_int) function pned_write_salphasbeta(path, n1, n2, alpha, beta, coef) &
+        bind(C, name="pned_write_salphasbeta")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), value :: n1, n2
+      real(c_double), intent(in) :: alpha(*), beta(*), coef(*)
+    end function
+    integer(c_int) function pned_session_begin(c, kind, v, max_steps, L, nobs, obs, flags) &
+        bind(C, name="pned_session_begin")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c, obs
+      integer(c_int), value :: kind, max_steps, nobs, flags
+      complex(c_double_complex), intent(in) :: v(*)
+      real(c_double), value :: L
+    end function
+    integer(c_int) function pned_session_step(c, nsteps) bind(C, name="pned_session_step")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: c
+      integer(c_int), value :: nsteps
+    end function
+    integer(c_int) function pned_session_read(c, alpha, beta, coef, done, status) bind(C, name="pned_session_read")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: c, coef
+      real(c_double), intent(out) :: alpha(*), beta(*)
+      integer(c_int), intent(out) :: done, status
+    end function
+    integer(c_int) function pned_session_save(c, path) bind(C, name="pned_session_save")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: c
+      character(kind=c_char), intent(in) :: path(*)
+    end function
+    integer(c_int) function pned_session_load(c, path, max_steps) bind(C, name="pned_session_load")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: c
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), value :: max_steps
     end function
     integer(c_int) function pned_ctx_destroy(c) bind(C, name="pned_ctx_destroy")
       import :: c_int, c_ptr
@@ -126,6 +192,88 @@ contains
     if (rc /= 0) stop 'pned_lanczos_run failed'
     itr = done
   end subroutine pned_lanczos_run_f
+
+  !! parallelized_lncv1z: eigenvector x = sum_k coef(k) v_k from the stored alpha/beta of the first pass.
+  subroutine pned_lncv1_f(v, nsteps, alpha, beta, coef, x)
+    complex(kind(0d0)), intent(in) :: v(:)
+    integer, intent(in) :: nsteps
+    double precision, intent(in) :: alpha(:), beta(:), coef(:)
+    complex(kind(0d0)), intent(out) :: x(:)
+    if (pned_lanczos_vector(g_ctx, v, int(nsteps, c_int), alpha, beta, coef, x, 0_c_int) /= 0) &
+        stop 'pned_lanczos_vector failed'
+  end subroutine pned_lncv1_f
+
+  !! parallelized_inv1 (inverse iteration with CG) for eigenvalue e from b.
+  subroutine pned_inv1_f(e, b, x, inv_max, cg_max)
+    double precision, intent(in) :: e
+    complex(kind(0d0)), intent(in) :: b(:)
+    complex(kind(0d0)), intent(out) :: x(:)
+    integer, intent(in) :: inv_max, cg_max
+    integer(c_int) :: ni, nc
+    if (pned_cg_run(g_ctx, real(e, c_double), b, int(inv_max, c_int), int(cg_max, c_int), x, ni, nc, 0_c_int) /= 0) &
+        stop 'pned_cg_run failed'
+  end subroutine pned_inv1_f
+
+  !! parallelized_TPSz for one seed on the model given to pned_gpu_init after
+  !! change_to_TPS_hamiltonian (L = localHam_max); coef(nsteps, 5) as eval_phys_val.
+  subroutine pned_tps_run_f(L, v, nsteps, alpha, beta, coef)
+    double precision, intent(in) :: L
+    complex(kind(0d0)), intent(in) :: v(:)
+    integer, intent(in) :: nsteps
+    double precision, intent(out) :: alpha(:), beta(:), coef(:, :)
+    double precision, allocatable :: c_row(:)
+    integer :: k, m
+    allocate(c_row(5 * nsteps))
+    if (pned_tps_run(g_ctx, real(L, c_double), v, int(nsteps, c_int), 0_c_int, c_null_ptr, alpha, beta, c_row, &
+                     0_c_int) /= 0) stop 'pned_tps_run failed'
+    do k = 1, nsteps
+      do m = 1, 5
+        coef(k, m) = c_row(5 * (k - 1) + m)
+      end do
+    end do
+    deallocate(c_row)
+  end subroutine pned_tps_run_f
+
+  !! dump_alpha_beta_coef: SalphaSbeta file in the reference's layout.
+  subroutine pned_dump_alpha_beta_coef_f(filename, alpha, beta, coef)
+    character(len=*), intent(in) :: filename
+    double precision, intent(in) :: alpha(:), beta(:), coef(:, :)
+    if (pned_write_salphasbeta(trim(filename) // c_null_char, int(size(alpha), c_int), int(size(coef, 2), c_int), &
+                               alpha, beta, coef) /= 0) stop 'pned_write_salphasbeta failed'
+  end subroutine pned_dump_alpha_beta_coef_f
+
+  !! Lanczos run in steps that can stop and resume (interval_dump / interval_dump_read).
+  subroutine pned_lanczos_begin_f(v, max_steps)
+    complex(kind(0d0)), intent(in) :: v(:)
+    integer, intent(in) :: max_steps
+    if (pned_session_begin(g_ctx, 1_c_int, v, int(max_steps, c_int), 0d0, 0_c_int, c_null_ptr, 0_c_int) /= 0) &
+        stop 'pned_session_begin failed'
+  end subroutine pned_lanczos_begin_f
+
+  subroutine pned_steps_f(nsteps)
+    integer, intent(in) :: nsteps
+    if (pned_session_step(g_ctx, int(nsteps, c_int)) /= 0) stop 'pned_session_step failed'
+  end subroutine pned_steps_f
+
+  subroutine pned_lanczos_read_f(alpha, beta, done)
+    double precision, intent(out) :: alpha(:), beta(:)
+    integer, intent(out) :: done
+    integer(c_int) :: d, st
+    if (pned_session_read(g_ctx, alpha, beta, c_null_ptr, d, st) /= 0) stop 'pned_session_read failed'
+    done = d
+  end subroutine pned_lanczos_read_f
+
+  subroutine pned_interval_dump_f(filename)
+    character(len=*), intent(in) :: filename
+    if (pned_session_save(g_ctx, trim(filename) // c_null_char) /= 0) stop 'pned_session_save failed'
+  end subroutine pned_interval_dump_f
+
+  subroutine pned_interval_dump_read_f(filename, max_steps)
+    character(len=*), intent(in) :: filename
+    integer, intent(in) :: max_steps
+    if (pned_session_load(g_ctx, trim(filename) // c_null_char, int(max_steps, c_int)) /= 0) &
+        stop 'pned_session_load failed'
+  end subroutine pned_interval_dump_read_f
 
   subroutine pned_gpu_finalize()
     integer(c_int) :: rc
