@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
 
 // Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by
 // the two bond digits; zero coefficients (target digit out of range) skip the load.
-template <int VPT, bool RC, bool RD, int K, bool SECTOR>
+template <int VPT, bool RC, bool RD, int K, bool SECTOR, bool I32>
 __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constant__ RadixProgram prog, const HvArgs a,
                                                             int q)
 {
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constan
     }
     for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
          it += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = it / G;
+        const int64_t s = G == 1 ? it : it / G;
         double2 v[VPT], acc[VPT];
         const double2 *cs = a.C + s * R + r0;
 #pragma unroll
@@ -616,12 +616,16 @@ __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constan
         }
         const int64_t st = SECTOR ? a.list1[s] : s;
         const uint64_t digits = pack_digits(st, prog.n, q);
+        // terms come bond by bond: the pair state of a bond is decoded once for its offsets
         for (int t = 0; t < prog.nterms; ++t) {
             const RadixTerm T = prog.t[t];
-            const int idx = digit_at(digits, T.s1) + q * digit_at(digits, T.s2);
-            const double2 c = s_tab[T.tab + idx];
-            if (c.x == 0.0 && c.y == 0.0) continue;
-            const double2 *ps = a.C + (SECTOR ? lin_index(a, uint64_t(st + T.offset)) : s + T.offset) * R + r0;
+            const int pair = digit_at(digits, T.s1) + q * digit_at(digits, T.s2);
+            const double2 c = s_tab[T.tab + pair];
+            if (RC ? c.x == 0.0 : (c.x == 0.0 && c.y == 0.0)) continue;
+            const double2 *ps;
+            if (SECTOR) ps = a.C + lin_index(a, uint64_t(st + T.offset)) * R + r0;
+            else if (I32) ps = a.C + (uint32_t(uint32_t(s) + uint32_t(T.offset)) * uint32_t(R) + uint32_t(r0));
+            else ps = a.C + (s + T.offset) * R + r0;
 #pragma unroll
             for (int j = 0; j < VPT; ++j) {
                 const double2 w = __ldg(ps + j);
@@ -871,8 +875,15 @@ static cudaError_t launch_hv_t(const pned_model *m, const HvArgs &a, int nblocks
         cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
         if (e != cudaSuccess) return e;
         kern<<<nblocks, kThreads, smem, st>>>(*m->xprog, a);
+    } else if (!SECTOR && uint64_t(m->dim) * uint64_t(a.R) < (uint64_t(1) << 31)) {
+        // element indices fit 32 bits (partners stay inside the basis: offsets
+        // are only applied where the coefficient, i.e. the target digit, is valid)
+        auto kern = hv_radix_kernel<VPT, RC, RD, K, SECTOR, true>;
+        cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+        if (e != cudaSuccess) return e;
+        kern<<<nblocks, kThreads, smem, st>>>(*m->rprog, a, m->q);
     } else {
-        auto kern = hv_radix_kernel<VPT, RC, RD, K, SECTOR>;
+        auto kern = hv_radix_kernel<VPT, RC, RD, K, SECTOR, false>;
         cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
         if (e != cudaSuccess) return e;
         kern<<<nblocks, kThreads, smem, st>>>(*m->rprog, a, m->q);
