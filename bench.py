@@ -116,6 +116,10 @@ def build_model(n_sites=30, R=1):
     return P.Model.from_couplings(cl, cpl), cl
 
 
+# single-vector tile kernel by partner-tile staging mode of the plan
+TILE_KERNELS = {0: "hv_tile_kernel", 1: "hv_tile_stage_kernel", 2: "hv_tile_bulk_kernel"}
+
+
 class CpuSample:
     """Reference CPU algorithm on a bounded sample of the workload: one Lanczos
     step's p_mltply_v3 restricted to 2^slice_log2 output states (all bond x
@@ -204,9 +208,9 @@ def run_ours(args, rank, world, local_rank):
     D = model.dim
     tuning = None
     if args.plan:
-        f, w, mp, jb = (int(x) for x in args.plan.split(","))
-        model.set_plan(1, f, w, mp, jb)
-        tuning = {"plan": [f, w, mp, jb], "tried": []}
+        plan = [int(x) for x in args.plan.split(",")]
+        model.set_plan(1, *plan)
+        tuning = {"plan": plan, "tried": []}
     elif args.tune:
         from pned_b200.tune import autotune
         tuning = autotune(model, 1)
@@ -278,7 +282,8 @@ def run_ours(args, rank, world, local_rank):
         "e0_after_warmup_plus_steps": e0,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "kernel": (f"hv_tile_kernel x{plan['tile_passes']} passes (K=1)" if plan["tile_passes"]
+                     "kernel": (f"{TILE_KERNELS.get(plan.get('staging', 0), 'hv_tile_kernel')} "
+                                f"x{plan['tile_passes']} passes (K=1)" if plan["tile_passes"]
                                 else "hv_xor_kernel (K=1)"),
                      "hv_ms": hv_ms, "step_ms_profiled": step_ms, "algorithmic_bytes_per_hv": bytes_hv,
                      "plan": plan, "traffic": traffic,
@@ -575,7 +580,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
     ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1"])
     ap.add_argument("--no-tune", dest="tune", action="store_false")
-    ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits' "
+    ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits[,l1_carveout[,stage]]' "
                                                  "instead of autotuning (profiling runs)")
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--batch-steps", type=int, default=40)

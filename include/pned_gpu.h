@@ -148,9 +148,18 @@ typedef struct {
     int32_t max_passes;
     int32_t j_bits;
     int32_t l1_carveout;   /* 1 (default): shared-memory carveout sized to the tiles, the rest L1; 0: driver's choice */
-    int32_t stage_partner_tiles; /* R = 1, j_bits 3: 1 copies each partner tile into shared memory once (cp.async) */
+    int32_t stage_partner_tiles; /* R = 1, j_bits 3: 1 copies each partner tile into shared memory once
+                                    (cp.async); 2 streams own and partner tiles with bulk copies (TMA engine)
+                                    through a ring of 32 KB shared-memory stages, one block per SM; 2 needs
+                                    tile rows that keep >= 3 low global bits, else the plan uses 0 */
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
+/*
+ * Measurement hook (no counterpart in the reference): the partner-tile
+ * staging the single-vector plan actually runs (0 gathered through L1/L2,
+ * 1 cp.async, 2 bulk copies) and, for 2, the number of ring stages.
+ */
+int pned_model_tile_staging(const pned_model *m, int *mode, int *ring_stages);
 
 /* ------------------------------------------------------------------------ */
 /* context: device vectors for R interleaved vectors                         */

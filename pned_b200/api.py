@@ -27,10 +27,16 @@ def _is_dev(x) -> bool:
 
 
 def _ptr(x, writable=False):
-    """(pointer, flag) for a numpy array or a CUDA tensor of complex128."""
+    """(pointer, flag) for a numpy array or a CUDA tensor of complex128.
+
+    A CUDA tensor may still be being written by torch's current stream (a
+    fill, a copy, a random draw), while the library works on its own stream
+    (a context's or a batch's non-blocking stream); the current stream is
+    therefore waited for before the pointer is handed over."""
     if _is_dev(x):
         if x.dtype != torch.complex128 or not x.is_contiguous():
             raise TypeError("device vectors must be contiguous complex128 CUDA tensors")
+        torch.cuda.current_stream(x.device).synchronize()
         return C.c_void_p(x.data_ptr()), PTR_DEVICE
     if not isinstance(x, np.ndarray) or x.dtype != np.complex128 or not x.flags["C_CONTIGUOUS"]:
         raise TypeError("host vectors must be C-contiguous complex128 numpy arrays")
@@ -276,7 +282,12 @@ class Model:
         """H.v plan for R vectors: tiled-kernel passes, partner tiles, states per tile."""
         p, g, t = C.c_int(0), C.c_int(0), C.c_int(0)
         check(lib().pned_model_plan(self._h, int(R), C.byref(p), C.byref(g), C.byref(t)))
-        return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
+        out = {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
+        if R == 1:
+            md, ns = C.c_int(0), C.c_int(0)
+            check(lib().pned_model_tile_staging(self._h, C.byref(md), C.byref(ns)))
+            out["staging"], out["ring_stages"] = md.value, ns.value
+        return out
 
     def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
                  j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0):

@@ -32,7 +32,9 @@ struct pned_model {
     pned_tile_plan plan1{-1, -1, -1, -1, -1, -1};   // single-vector plan parameters (-1: defaults)
     int tile_jb = 3;                        // j bits (rows per thread 2^jb) of the single-vector tiles
     bool carveout = true;                   // size the shared-memory carveout to the tiles (rest L1)
-    bool tile_stage = false;                // single-vector: partner tiles staged in shared memory
+    int tile_stage = 0;                     // single-vector partner tiles: 0 gathered through L1/L2,
+                                            // 1 staged in shared memory (cp.async), 2 streamed by bulk copies
+    int bulk_stages = 0;                    // shared-memory stages of the bulk-copy pipeline
     int nsm = 148;
     double2 *d_table = nullptr;
     void *d_diag = nullptr;

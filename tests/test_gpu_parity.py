@@ -333,14 +333,18 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
 
 
 @pytest.mark.parametrize("plan", [(8, 10, 4, 3, 1, 1), (5, 10, 2, 3, 1, 1), (3, 8, 1, 3, 1, 1), (5, 12, 2, 2, 1, 0),
-                                  (5, 12, 2, 1, 0, 0)])
+                                  (5, 12, 2, 1, 0, 0), (8, 10, 4, 3, 1, 2), (5, 10, 2, 3, 1, 2), (3, 8, 1, 3, 1, 2),
+                                  (5, 6, 3, 3, 1, 2)])
 def test_tile_plans_agree_with_oracle(plan):
     """Every tile plan the autotuner may pick (rows kept, window, passes, rows per
-    thread, carveout, staged partner tiles) gives the oracle's H.v to 1e-12."""
+    thread, carveout, staged or bulk-streamed partner tiles) gives the oracle's
+    H.v to 1e-12."""
     cl = honeycomb(2, 4)
     gm, om = models(cl, 2, 0, KHGH, FIELD)
     got = gm.set_plan(1, *plan)
     assert got["tile_passes"] >= 1
+    if plan[5] == 2:
+        assert got["staging"] == 2 and got["ring_stages"] >= 2
     ctx = P.Context(gm, R=1)
     rng = np.random.default_rng(23)
     v1 = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
@@ -355,6 +359,56 @@ def test_tile_plans_agree_with_oracle(plan):
     out = ctx.lanczos(v, 30)
     refl = om.lanczos(v, 30)
     assert rel(out["alpha"][:12, 0], refl["alpha"][:12]) <= 1e-10
+
+
+@pytest.mark.parametrize("plan", [(5, 10, 2, 3), (8, 12, 1, 3), (3, 8, 3, 3)])
+def test_bulk_streamed_tiles_match_gathered_tiles(plan):
+    """N = 24 (8192 tiles, many per block, so the stage ring wraps across tiles):
+    streaming the tiles with bulk copies gives the same W bit for bit as
+    gathering the partner rows through L1/L2 with the same plan, and the same
+    Lanczos coefficients to the summation order of the block sums."""
+    cl = honeycomb(3, 4)
+    gm, _ = models(cl, 2, 0, KHGH, FIELD)
+    rng = np.random.default_rng(77)
+    v1 = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
+    v0 = 0.1 * (rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim))
+    v = O.gaussian(5, gm.dim)
+    v /= np.linalg.norm(v)
+    out = {}
+    for stage in (0, 2):
+        got = gm.set_plan(1, *plan, 1, stage)
+        assert got["staging"] == stage
+        ctx = P.Context(gm, R=1)
+        w = v0.copy()
+        pr = ctx.p_mltply_v3(v1, w, 0.0625)
+        run = ctx.lanczos(v, 20)
+        out[stage] = (w, pr, run["alpha"][:, 0], run["beta"][:, 0])
+        ctx.close()
+    assert np.array_equal(out[0][0], out[2][0])
+    assert abs(out[0][1][0] - out[2][1][0]) <= 1e-12 * abs(out[0][1][0])
+    assert rel(out[0][2], out[2][2]) <= 1e-12 and rel(out[0][3], out[2][3]) <= 1e-12
+    gm.set_plan(1)
+
+
+def test_torch_tensors_written_just_before_the_call_are_ready():
+    """The context runs on its own stream; a CUDA tensor that torch is still
+    writing on its current stream (here behind a 10 ms GPU sleep) must be
+    complete before the library reads or accumulates into it."""
+    cl = honeycomb(3, 4)
+    gm, _ = models(cl, 2, 0, KHGH, FIELD)
+    ctx = P.Context(gm, R=1)
+    rng = np.random.default_rng(5)
+    v1h = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
+    wh = np.full(gm.dim, 0.5 + 0.25j)
+    ctx.p_mltply_v3(v1h, wh)
+    v1 = torch.from_numpy(v1h).cuda()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        torch.cuda._sleep(20_000_000)
+        w = torch.full_like(v1, 0.5 + 0.25j)
+        ctx.p_mltply_v3(v1, w)
+        assert np.array_equal(w.cpu().numpy(), wh)
+    ctx.close()
 
 
 def test_lanczos_breakdown_is_reported():
