@@ -29,6 +29,13 @@ struct pned_model {
     };
     std::map<int, TileSet> rtiles;
     std::mutex rtiles_mu;
+    // tiled mixed-radix passes per R (q > 2, full basis; guarded by rtiles_mu)
+    struct QTileSet {
+        std::vector<std::unique_ptr<pned::QTileProgram>> progs;
+        int vpt = 0;
+        size_t smem = 0;
+    };
+    std::map<int, QTileSet> qtiles;
     pned_tile_plan plan1{-1, -1, -1, -1, -1, -1};   // single-vector plan parameters (-1: defaults)
     int tile_jb = 3;                        // j bits (rows per thread 2^jb) of the single-vector tiles
     bool carveout = true;                   // size the shared-memory carveout to the tiles (rest L1)
@@ -121,6 +128,7 @@ void build_tile_programs(pned_model *m);
 bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan *plan);
 // Shared memory of the tiled multi-vector kernel for R vectors.
 size_t rtile_smem(const pned_model *m, int R, bool slot_tables);
+bool ensure_qtiles(pned_model *m, int R);
 // Number of partial-sum blocks launch_hv writes for this model, R and grid.
 int hv_partial_blocks(const pned_model *m, int R, int nblocks);
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);

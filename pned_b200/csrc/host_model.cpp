@@ -466,6 +466,7 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
                         P.table.push_back(v);
                     }
                     P.rterms.push_back(t);
+                    P.rdelta.push_back({d1, d2});
                 }
         }
         if (P.rterms.size() > size_t(kMaxTerms)) return fail(PNED_ENOTSUP, "pned_model_create: too many terms");
@@ -647,6 +648,99 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
         for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
         pass.outer = outer;
         pass.gstart.push_back(0);
+        passes.push_back(pass);
+    }
+    return PNED_OK;
+}
+
+}  // namespace pned
+
+// ---------------------------------------------------------------------------
+// Tile planner for the mixed-radix kernel (q > 2)
+// ---------------------------------------------------------------------------
+namespace pned {
+
+int plan_qtiles(const HostProgram &P, int k, int low, std::vector<QTilePass> &passes)
+{
+    passes.clear();
+    const int n = P.n, q = P.q;
+    if (q <= 2 || P.sector || k < 2 || k > kQTileMaxSites || k > n) return PNED_ENOTSUP;
+    // bonds (site pairs) of the terms
+    std::vector<std::pair<int, int>> bonds;
+    for (const RadixTerm &t : P.rterms) {
+        std::pair<int, int> b{std::min<int>(t.s1, t.s2), std::max<int>(t.s1, t.s2)};
+        if (std::find(bonds.begin(), bonds.end(), b) == bonds.end()) bonds.push_back(b);
+    }
+    std::vector<char> covered(bonds.size(), 0);
+    size_t left = bonds.size();
+    auto touching = [&](int x) {
+        int c = 0;
+        for (size_t i = 0; i < bonds.size(); ++i)
+            if (!covered[i] && (bonds[i].first == x || bonds[i].second == x)) ++c;
+        return c;
+    };
+    while (left > 0) {
+        if (int(passes.size()) >= kQTileMaxPasses) return PNED_ENOTSUP;
+        // seed: the uncovered bond whose sites touch the most uncovered bonds
+        size_t seed = 0;
+        int best = -1;
+        for (size_t i = 0; i < bonds.size(); ++i) {
+            if (covered[i]) continue;
+            const int c = touching(bonds[i].first) + touching(bonds[i].second);
+            if (c > best) { best = c; seed = i; }
+        }
+        // the `low` lowest sites are in every tile: runs of q^low consecutive states
+        std::vector<int> S;
+        for (int x = 0; x < low && x < k; ++x) S.push_back(x);
+        for (int x : {bonds[seed].first, bonds[seed].second})
+            if (int(S.size()) < k && std::find(S.begin(), S.end(), x) == S.end()) S.push_back(x);
+        auto in = [&](int x) { return std::find(S.begin(), S.end(), x) != S.end(); };
+        while (int(S.size()) < k) {
+            int bx = -1, bg = -1, bt = -1;
+            for (int x = 0; x < n; ++x) {
+                if (in(x)) continue;
+                int g = 0;
+                for (size_t i = 0; i < bonds.size(); ++i) {
+                    if (covered[i]) continue;
+                    const int a = bonds[i].first, b = bonds[i].second;
+                    if ((a == x && (b == x || in(b))) || (b == x && in(a))) ++g;
+                }
+                const int t = touching(x);
+                if (g > bg || (g == bg && t > bt)) { bx = x; bg = g; bt = t; }
+            }
+            S.push_back(bx);
+        }
+        std::sort(S.begin(), S.end());
+        QTilePass pass;
+        pass.sites = S;
+        for (int x = 0; x < n; ++x)
+            if (!in(x)) pass.outer.push_back(x);
+        std::vector<int64_t> lpw(S.size() + 1, 1);
+        for (size_t i = 1; i <= S.size(); ++i) lpw[i] = lpw[i - 1] * q;
+        auto pos = [&](int x) { return int(std::find(S.begin(), S.end(), x) - S.begin()); };
+        std::vector<char> take(bonds.size(), 0);
+        for (size_t i = 0; i < bonds.size(); ++i)
+            if (!covered[i] && in(bonds[i].first) && in(bonds[i].second)) take[i] = 1;
+        for (size_t t = 0; t < P.rterms.size(); ++t) {
+            const RadixTerm &T = P.rterms[t];
+            std::pair<int, int> b{std::min<int>(T.s1, T.s2), std::max<int>(T.s1, T.s2)};
+            const size_t bi = size_t(std::find(bonds.begin(), bonds.end(), b) - bonds.begin());
+            if (!take[bi]) continue;
+            QTileTerm qt{};
+            qt.ls1 = uint8_t(pos(T.s1));
+            qt.ls2 = uint8_t(pos(T.s2));
+            qt.loff = int32_t(P.rdelta[t].first * lpw[qt.ls1] + P.rdelta[t].second * lpw[qt.ls2]);
+            qt.tab = T.tab;
+            pass.terms.push_back(qt);
+        }
+        for (size_t i = 0; i < bonds.size(); ++i)
+            if (take[i]) { covered[i] = 1; --left; }
+        passes.push_back(pass);
+    }
+    if (passes.empty()) {   // diagonal-only model: one pass, no terms
+        QTilePass pass;
+        for (int x = 0; x < k; ++x) pass.sites.push_back(x);
+        for (int x = k; x < n; ++x) pass.outer.push_back(x);
         passes.push_back(pass);
     }
     return PNED_OK;

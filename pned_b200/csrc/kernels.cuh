@@ -50,6 +50,19 @@ struct RadixProgram {
     RadixTerm t[kMaxTerms];
 };
 
+// Tiled mixed-radix pass (see QTileTerm): a tile is the q^k states with
+// fixed outer digits; tile t's outer digits are t written in base q over
+// outer[] (fastest first).
+constexpr int kQTileMaxTab = 768;   // coefficient entries of one pass (its terms' tables only)
+struct QTileProgram {
+    int q, k, nt, nouter, nterms, ntab, first, last;
+    int64_t ntiles;
+    uint32_t spow[kQTileMaxSites];  // q^site of tile site i (q^n < 2^32)
+    uint32_t opow[32];              // q^site of outer site i
+    QTileTerm t[kMaxTerms];
+    double2 tab[kQTileMaxTab];      // the pass's coefficient tables
+};
+
 // Tiled single-vector S = 1/2 program (see TileTerm).
 struct TileProgram {
     int n, tbits, jb, nin, nterms, ntab, nouter;

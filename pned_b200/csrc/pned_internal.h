@@ -58,10 +58,26 @@ struct TileTerm {
     uint8_t hasj;    // 1 if a dependency bit is a j-bit
     uint32_t lmask;  // out-of-tile: local xor of the mask's in-tile part (the offset inside the partner tile)
 };
+// Tiled mixed-radix (q > 2) pass: the states that agree on all digits but
+// those of the k tile sites form a tile of q^k states, staged in shared
+// memory; a pass applies the terms of its bonds (both sites in the tile).
+constexpr int kQTileMaxSites = 16;
+constexpr int kQTileMaxPasses = 16;
+struct QTileTerm {
+    int32_t loff;    // partner offset inside the tile (local index)
+    uint8_t ls1, ls2;   // local digit positions of the bond's sites
+    uint16_t tab;    // coefficient table offset (q^2 entries by pair state)
+};
 constexpr int kTileMaxJB = 3;
 constexpr int kTileWindowBits = 10;   // outer bits whose partner tiles stay in L2 during a sweep
 constexpr int kTileMaxPasses = 4;
 constexpr int kTileMaxGroups = 64;    // partner tiles per pass
+
+struct QTilePass {
+    std::vector<int> sites;              // tile sites, ascending: local digit k is site sites[k]
+    std::vector<int> outer;              // the other sites, ascending
+    std::vector<QTileTerm> terms;
+};
 
 struct HostProgram {
     int n = 0, q = 2;
@@ -78,6 +94,7 @@ struct HostProgram {
     std::vector<std::vector<std::pair<int, int>>> xcontrib;
     std::vector<int> bond_type;          // schedule-order bond types (1..9)
     std::vector<RadixTerm> rterms;       // q > 2
+    std::vector<std::pair<int, int>> rdelta;   // per radix term: digit changes (d1, d2) of sites s1, s2
     std::vector<cd> table;               // coefficient tables
     // diagonal: per bond (s1, s2) and q*q diagonal values (pair state st)
     std::vector<int> dsite1, dsite2;
@@ -105,6 +122,11 @@ struct HostProgram {
 // found in L2), the last pass takes what is left.  In-tile terms carry the
 // local xor (row bits, then the j bits from bit tbits); out-of-tile terms the
 // global one.
+// Covers the bonds of a mixed-radix (q > 2, full basis) program with passes
+// of k-site tiles, greedily: each pass takes the uncovered bonds inside a
+// site set grown from the most connected uncovered bond (plus the `low`
+// lowest sites, kept in every tile for contiguous runs of states).
+int plan_qtiles(const HostProgram &P, int k, int low, std::vector<QTilePass> &passes);
 int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bits, int max_passes,
                std::vector<HostProgram::TilePass> &out);
 

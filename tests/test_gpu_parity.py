@@ -77,6 +77,62 @@ def test_hv_parity(case):
         assert abs(pr[r] - prr) <= 1e-12 * abs(prr)
 
 
+QTILE_CASES = [
+    # (L1, L2, q, tree, couplings, field, R): 12 and 8 sites, tiled mixed-radix passes
+    (3, 2, 3, 1, CP.kitaev_heisenberg(0.2, -1.0), None, 1),
+    (3, 2, 3, 1, CP.kitaev_heisenberg(0.2, -1.0, gamma=0.1), FIELD, 4),
+    (3, 2, 3, 1, CP.kitaev_heisenberg(0.2, -1.0), FIELD, 16),
+    (2, 2, 4, 1, CP.kitaev_heisenberg(0.5, 0.3, gamma=-0.2), FIELD, 2),
+]
+
+
+@pytest.mark.parametrize("case", QTILE_CASES, ids=[f"{c[0]}x{c[1]}q{c[2]}R{c[6]}" for c in QTILE_CASES])
+def test_radix_tiles_parity(case):
+    """S >= 1 on 8-12 sites runs the tiled mixed-radix kernel (several passes of
+    q^k-state tiles in shared memory); H.V and prdct match the oracle."""
+    L1, L2, q, tree, cpl, fld, R = case
+    cl = honeycomb(L1, L2)
+    gm, om = models(cl, q, tree, cpl, fld)
+    ctx = P.Context(gm, R=R)
+    plan = gm.plan(R)
+    assert plan["tile_passes"] >= 2 and plan["tile_states"] >= q ** 4
+    rng = np.random.default_rng(29)
+    D = gm.dim
+    v1 = (rng.standard_normal((D, R)) + 1j * rng.standard_normal((D, R))).astype(np.complex128)
+    v0 = (0.2 * rng.standard_normal((D, R)) + 0.1j * rng.standard_normal((D, R))).astype(np.complex128)
+    w = np.ascontiguousarray(v0).reshape(-1).copy()
+    pr = ctx.p_mltply_v3(np.ascontiguousarray(v1).reshape(-1), w, 0.0625)
+    w = w.reshape(D, R)
+    for r in range(R):
+        ref = np.ascontiguousarray(v0[:, r]).copy()
+        prr = om.p_mltply_v3(np.ascontiguousarray(v1[:, r]), ref, 0.0625)
+        assert rel(w[:, r], ref) <= 1e-12
+        assert abs(pr[r] - prr) <= 1e-12 * abs(prr)
+
+
+def test_radix_tiles_tps_and_lanczos():
+    """S = 1, 12 sites: the TPS loop (K = 4 sums in the last pass) and a Lanczos
+    chain through the tiled mixed-radix passes follow the oracle."""
+    cl = honeycomb(3, 2)
+    cpl = CP.kitaev_heisenberg(0.2, -1.0, gamma=0.1)
+    L = 3.0 * cl.n
+    gm, om = models(cl, 3, 1, cpl, FIELD, tps_L=L)
+    R = 4
+    V = O.gaussian(11, gm.dim, R).reshape(gm.dim, R)
+    V /= np.linalg.norm(V, axis=0)
+    out = P.Context(gm, R=R).tps(L, np.ascontiguousarray(V).reshape(-1), 25)
+    for r in range(R):
+        ref = om.tps(L, np.ascontiguousarray(V[:, r]), 25)
+        assert rel(out["alpha"][:, r], ref["alpha"]) <= 1e-10
+        assert rel(out["beta"][:, r], ref["beta"]) <= 1e-10
+        assert rel(out["coef"][:, r, :5], ref["coef"][:, :5]) <= 1e-10
+    gl, ol = models(cl, 3, 1, cpl, FIELD)
+    v = np.ascontiguousarray(V[:, 0])
+    run = P.Context(gl, R=1).lanczos(v, 30)
+    refl = ol.lanczos(v, 30)
+    assert rel(run["alpha"][:12, 0], refl["alpha"][:12]) <= 1e-10
+
+
 def test_hv_device_pointers_and_dots():
     cl = honeycomb(2, 4)
     gm, om = models(cl, 2, 0, KHGH, FIELD)
