@@ -475,6 +475,13 @@ int pned_read_dsf_alpha_beta(const char *path, pned_c128 *sq, double *salpha, do
 /* Appends one momentum's block of the text spectrum (write_dsf_res, S1/2 output.f90:246-264). */
 int pned_append_dsf_res(const char *path, double sq_re, const double *q2, const double *w, const double *dsf,
                         const int *conv, int ll);
+/* Appends the DSF driver's sq.txt line for momentum iq (S1/2 DSF.f90:490-492; Sa DSF.f90:578-580):
+ * ' q = ', iq, q(1), q(2), Re sq in '(A,I3,2F12.6,F25.18)'. */
+int pned_append_sq(const char *path, int iq, double q1, double q2, double norm_re);
+/* vec_q%05dme%05d<comp> (dump_alpha_beta / read_alpha_beta2, S1/2 DSF.f90:374-379, 399-405):
+ * records indx (int32), v1 [ll], v2 [ll]; vectors above 2^31 bytes are refused. */
+int pned_write_dsf_vectors(const char *path, int indx, const pned_c128 *v1, const pned_c128 *v2, int64_t ll);
+int pned_read_dsf_vectors(const char *path, int *indx, pned_c128 *v1, pned_c128 *v2, int64_t ll);
 
 #ifdef __cplusplus
 }

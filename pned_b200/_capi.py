@@ -63,7 +63,8 @@ EXPORTS = [
     "pned_slots_synchronize", "pned_slots_read", "pned_gaussian_column", "pned_lanczos_vector", "pned_slots_set_plan", "pned_slots_plan",
     "pned_write_salphasbeta", "pned_read_salphasbeta", "pned_tpq_thermo", "pned_session_save",
     "pned_session_load", "pned_session_info", "pned_write_vec_data", "pned_read_vec_data",
-    "pned_write_dsf_alpha_beta", "pned_read_dsf_alpha_beta", "pned_append_dsf_res",
+    "pned_write_dsf_alpha_beta", "pned_read_dsf_alpha_beta", "pned_append_dsf_res", "pned_append_sq",
+    "pned_write_dsf_vectors", "pned_read_dsf_vectors",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -144,6 +145,9 @@ def lib() -> C.CDLL:
     L.pned_write_dsf_alpha_beta.argtypes = [C.c_char_p, c128, dp, dp, i32]
     L.pned_read_dsf_alpha_beta.argtypes = [C.c_char_p, C.POINTER(c128), dp, dp, i32]
     L.pned_append_dsf_res.argtypes = [C.c_char_p, dbl, dp, dp, dp, ip, i32]
+    L.pned_append_sq.argtypes = [C.c_char_p, i32, dbl, dbl, dbl]
+    L.pned_write_dsf_vectors.argtypes = [C.c_char_p, i32, vp, vp, i64]
+    L.pned_read_dsf_vectors.argtypes = [C.c_char_p, ip, vp, vp, i64]
     _lib = L
     return L
 

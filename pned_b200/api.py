@@ -208,6 +208,30 @@ def append_dsf_res(path: str, sq_re: float, q, w, dsf, conv):
                                     c_.ctypes.data_as(C.POINTER(C.c_int)), w_.size))
 
 
+def append_sq(path: str, iq: int, q, norm_re: float):
+    """The DSF driver's sq.txt line for momentum iq (q: the two components)."""
+    check(lib().pned_append_sq(os.fsencode(path), int(iq), float(q[0]), float(q[1]), float(norm_re)))
+
+
+def write_dsf_vectors(path: str, indx: int, v1, v2):
+    """vec_q... file of a DSF chain (step index, the two Lanczos vectors)."""
+    a = np.ascontiguousarray(v1, dtype=np.complex128)
+    b = np.ascontiguousarray(v2, dtype=np.complex128)
+    if a.shape != b.shape:
+        raise ValueError("v1 and v2 need the same length")
+    check(lib().pned_write_dsf_vectors(os.fsencode(path), int(indx), C.c_void_p(a.ctypes.data),
+                                       C.c_void_p(b.ctypes.data), a.size))
+
+
+def read_dsf_vectors(path: str, ll: int):
+    i = C.c_int(0)
+    a = np.zeros(int(ll), dtype=np.complex128)
+    b = np.zeros(int(ll), dtype=np.complex128)
+    check(lib().pned_read_dsf_vectors(os.fsencode(path), C.byref(i), C.c_void_p(a.ctypes.data),
+                                      C.c_void_p(b.ctypes.data), int(ll)))
+    return i.value, a, b
+
+
 # --------------------------------------------------------------------------- model / context
 
 

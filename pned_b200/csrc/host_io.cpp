@@ -253,3 +253,46 @@ extern "C" int pned_append_dsf_res(const char *path, double sq_re, const double 
     ok = (std::fclose(f) == 0) && ok;
     return ok ? PNED_OK : fail(PNED_EINVAL, "pned_append_dsf_res: write failed");
 }
+
+extern "C" int pned_append_sq(const char *path, int iq, double q1, double q2, double norm_re)
+{
+    if (!path) return fail(PNED_EINVAL, "pned_append_sq: null path");
+    FILE *f = std::fopen(path, "a");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_append_sq: cannot open ") + path);
+    // the DSF driver's sq.txt line (S1/2 DSF.f90:490-492): '(A,I3,2F12.6,F25.18)'
+    bool ok = std::fprintf(f, " q = %3d%12.6f%12.6f%25.18f\n", iq, q1, q2, norm_re) > 0;
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_append_sq: write failed");
+}
+
+extern "C" int pned_write_dsf_vectors(const char *path, int indx, const pned_c128 *v1, const pned_c128 *v2, int64_t ll)
+{
+    if (!path || !v1 || !v2 || ll < 1) return fail(PNED_EINVAL, "pned_write_dsf_vectors: bad arguments");
+    if (uint64_t(ll) * 16 > 0x7fffffffu)
+        return fail(PNED_ENOTSUP, "pned_write_dsf_vectors: vectors above 2^31 bytes need Fortran subrecords");
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_write_dsf_vectors: cannot open ") + path);
+    const int32_t i4 = indx;
+    bool ok = put_record(f, &i4, 4) && put_record(f, v1, size_t(ll) * 16) && put_record(f, v2, size_t(ll) * 16);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_write_dsf_vectors: write failed");
+}
+
+extern "C" int pned_read_dsf_vectors(const char *path, int *indx, pned_c128 *v1, pned_c128 *v2, int64_t ll)
+{
+    if (!path || !indx || !v1 || !v2 || ll < 1) return fail(PNED_EINVAL, "pned_read_dsf_vectors: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_read_dsf_vectors: cannot open ") + path);
+    std::vector<char> r1, r2, r3;
+    const size_t n = size_t(ll) * 16;
+    const bool ok = get_record(f, r1) && r1.size() == 4 && get_record(f, r2) && r2.size() == n &&
+                    get_record(f, r3) && r3.size() == n;
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_read_dsf_vectors: not a DSF vector file of this length");
+    int32_t i4 = 0;
+    std::memcpy(&i4, r1.data(), 4);
+    *indx = i4;
+    std::memcpy(v1, r2.data(), n);
+    std::memcpy(v2, r3.data(), n);
+    return PNED_OK;
+}

@@ -177,6 +177,30 @@ def test_vector_and_dsf_files_layout(tmp_path):
     assert sq == 0.5 - 0.25j and np.array_equal(sa2, sa) and np.array_equal(sb2, sb)
 
 
+def test_dsf_vectors_file_and_sq_line(tmp_path):
+    import struct
+
+    def rec(payload):
+        return struct.pack("<i", len(payload)) + payload + struct.pack("<i", len(payload))
+    rng = np.random.default_rng(12)
+    v1 = rng.standard_normal(19) + 1j * rng.standard_normal(19)
+    v2 = rng.standard_normal(19) + 1j * rng.standard_normal(19)
+    p = str(tmp_path / "vec_q00002me00000xx")
+    P.api.write_dsf_vectors(p, 41, v1, v2)
+    assert open(p, "rb").read() == (rec(struct.pack("<i", 41)) + rec(v1.astype("<c16").tobytes()) +
+                                    rec(v2.astype("<c16").tobytes()))
+    i, a, b = P.api.read_dsf_vectors(p, 19)
+    assert i == 41 and np.array_equal(a, v1) and np.array_equal(b, v2)
+    with pytest.raises(P.PnedError):
+        P.api.read_dsf_vectors(p, 18)
+    s = str(tmp_path / "sq.txt")
+    P.api.append_sq(s, 3, [0.5, -2.25], 0.0625)
+    P.api.append_sq(s, 12, [-1.0, 3.0], 1.5)
+    # '(A,I3,2F12.6,F25.18)' as the DSF driver writes it
+    assert open(s).read().split("\n")[:2] == [" q =   3    0.500000   -2.250000     0.062500000000000000",
+                                               " q =  12   -1.000000    3.000000     1.500000000000000000"]
+
+
 def test_dsf_res_text_block(tmp_path):
     p = str(tmp_path / "dsf_res_zz")
     P.api.append_dsf_res(p, 0.75, [0.5, -1.25], [0.0, 1.5], [2.0, 0.125], [3, 4])
