@@ -271,6 +271,17 @@ int pned_tps_run(pned_ctx *c, double L, const pned_c128 *v_init, int n_steps, in
  */
 int pned_dsf_run(pned_ctx *c, const pned_c128 *x, const double *qr, int n_steps, double *cnorm, double *salpha,
                  double *sbeta, int ptr_flags);
+/*
+ * The same chains started from S^{ipm}_q x (intalv_xy: the 'xx' component of
+ * S1/2 DSF.f90:91-193, ipm = +1, bit j 0 -> 1; the 'uu'/'dd' components of Sa
+ * DSF.f90:91-286, ipm = +1 / -1, digit d -> d + ipm with the spin-ladder factor
+ * sqrt((S -+ m)(S +- m + 1))).  x lives on `source`'s basis (for a sector model
+ * its states in mk_list12 order, the reference's listt), the chains on the
+ * context's model (the target sector, Lin tables list3(:,:,0)); n and q must
+ * match.  cnorm, salpha, sbeta as pned_dsf_run.
+ */
+int pned_dsf_xy_run(pned_ctx *c, const pned_model *source, int ipm, const pned_c128 *x, const double *qr, int n_steps,
+                    double *cnorm, double *salpha, double *sbeta, int ptr_flags);
 
 /*
  * parallelized_lncv1z (S1/2 Lanczos.f90:183-329), R = 1: replays the Lanczos
@@ -316,6 +327,9 @@ int pned_session_begin(pned_ctx *c, int kind, const pned_c128 *v_init, int max_s
 /* DSF chains: start vectors S^z_q x (intalv_zz, S1/2 DSF.f90:18-87); cnorm[r] = sbeta(1). */
 int pned_session_begin_dsf(pned_ctx *c, const pned_c128 *x, const double *qr, int max_steps, double *cnorm,
                            int ptr_flags);
+/* DSF chains started from S^{ipm}_q x with x on the source model's basis (see pned_dsf_xy_run). */
+int pned_session_begin_dsf_xy(pned_ctx *c, const pned_model *source, int ipm, const pned_c128 *x, const double *qr,
+                              int max_steps, double *cnorm, int ptr_flags);
 /* Enqueues n_steps steps on the context's stream and returns without waiting. */
 int pned_session_step(pned_ctx *c, int n_steps);
 /*

@@ -76,6 +76,7 @@ def lib():
         L.oracle_tps.argtypes = [vp, C.c_double, vp, C.c_int, C.c_int, c_int_p, c_int_p, c_int_p, vp, vp,
                                  c_dbl_p, c_dbl_p, c_dbl_p, C.c_int]
         L.oracle_intalv_zz.argtypes = [vp, c_dbl_p, vp, vp, vp]
+        L.oracle_intalv_xy.argtypes = [vp, vp, C.c_int, c_dbl_p, vp, vp, vp]
         L.oracle_dsf_chain.argtypes = [vp, vp, c_cplx, C.c_int, c_dbl_p, c_dbl_p]
         L.oracle_exec_renbun.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, c_dbl_p, c_dbl_p,
                                          c_dbl_p, c_int_p, c_dbl_p]
@@ -305,6 +306,17 @@ class Model:
         cn = np.zeros(1, dtype=np.complex128)
         xs = _c128(x)   # keep the array alive across the call
         lib().oracle_intalv_zz(self._h, _p(qr, C.c_double), _p(xs), _p(v), _p(cn))
+        return v, complex(cn[0])
+
+    def intalv_xy(self, source, ipm, qr, x):
+        """S^{ipm}_q start vector on this model's basis from x on `source`'s basis."""
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        v = np.zeros(self.ldim, dtype=np.complex128)
+        cn = np.zeros(1, dtype=np.complex128)
+        xs = _c128(x)   # keep the array alive across the call
+        rc = lib().oracle_intalv_xy(self._h, source._h, int(ipm), _p(qr, C.c_double), _p(xs), _p(v), _p(cn))
+        if rc:
+            raise ValueError(f"oracle_intalv_xy rc={rc}")
         return v, complex(cn[0])
 
     def dsf_chain(self, v1, cnorm, nsteps):

@@ -1029,6 +1029,56 @@ int oracle_intalv_zz(const omodel *m, const double *qr, const cplx *x, cplx *v, 
 }
 
 /*
+ * intalv_xy, one rank (b_bit = n): v = sum_j fac e^{i q.r_j} S^{ipm}_j x,
+ * normalised; returns cnorm = ||v_raw||^2 / n.  x lives on the source model's
+ * basis (its sector states in list1 order, the reference's listt of
+ * get_listt); v on the target model's (its Lin tables, list3(:,:,0)).
+ * S_one_half/Hybrid_TPS_DSF.f90:91-193: ipm = +1 only, bit j 0 -> 1, no
+ * factor.  S_arbitrary/Hybrid_TPS9_DSF.f90:91-286 (local_operation
+ * :196-243): digit is -> is + ipm with fac = sqrt((s - sm)(s + sm + 1))
+ * (ipm = +1) or sqrt((s + sm)(s - sm + 1)) (ipm = -1), sm = is - s; sites in
+ * ascending order, each added over all source states.
+ */
+int oracle_intalv_xy(const omodel *mt, const omodel *ms, int ipm, const double *qr, const cplx *x, cplx *v,
+                     cplx *cnorm_out)
+{
+    if (mt->n != ms->n || mt->q != ms->q || mt->tree_sa != ms->tree_sa) return OR_EINVAL;
+    if (ipm != 1 && ipm != -1) return OR_EINVAL;
+    if (!mt->tree_sa && ipm != 1) return OR_EINVAL;
+    const int q = mt->q;
+    const double ss = 0.5 * (double)(q - 1);
+    for (int64_t i = 0; i < mt->ldim; ++i) v[i] = 0;
+    for (int j = 0; j < mt->n; ++j) {
+        const double qnorm = qr[j];
+        const double cq = cos(qnorm), sq = sin(qnorm);
+        const int64_t basis = ipow(q, j);
+        /* one site: distinct source states reach distinct targets */
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < ms->ldim; ++i) {
+            const int64_t st = ms->list1 ? ms->list1[i] : i;
+            const cplx rot = (cq * creal(x[i]) - sq * cimag(x[i])) + I * (sq * creal(x[i]) + cq * cimag(x[i]));
+            if (!mt->tree_sa) {
+                if (((st >> j) & 1) != 0) continue;
+                v[lin_index(mt, st + basis)] += rot;
+            } else {
+                const int64_t is = (st / basis) % q;
+                if (is + ipm < 0 || is + ipm >= q) continue;
+                const double sm = (double)is - ss;
+                const double fac = ipm == 1 ? sqrt((ss - sm) * (ss + sm + 1.0)) : sqrt((ss + sm) * (ss - sm + 1.0));
+                v[lin_index(mt, st + ipm * basis)] += fac * rot;
+            }
+        }
+    }
+    cplx cnorm = oracle_inprdct(mt->ldim, v, v);
+    if (cabs(cnorm) < 1e-25) cnorm = 1e-25;
+    const double norm2 = 1.0 / sqrt(creal(cnorm));
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < mt->ldim; ++i) v[i] = v[i] * norm2;
+    *cnorm_out = cnorm / (double)mt->n;
+    return OR_OK;
+}
+
+/*
  * parallelized_dsflnc1z (S_one_half/Hybrid_TPS_DSF.f90:195-261): with
  * s_maxitr = nsteps+1, salpha[0..nsteps-1], sbeta[0..nsteps] (sbeta[0] = cnorm).
  */

@@ -55,7 +55,7 @@ EXPORTS = [
     "pned_mk_list12", "pned_model_create", "pned_model_destroy", "pned_model_info", "pned_model_plan", "pned_model_set_plan", "pned_model_tile_staging", "pned_ctx_create",
     "pned_ctx_destroy", "pned_ctx_set_stream", "pned_ctx_synchronize", "pned_ctx_buffer", "pned_ctx_bytes",
     "pned_hv", "pned_inprdct", "pned_calc_beta", "pned_fill_gaussian", "pned_lanczos_run", "pned_tps_run",
-    "pned_dsf_run", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
+    "pned_dsf_run", "pned_dsf_xy_run", "pned_session_begin_dsf_xy", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
     "pned_session_begin", "pned_session_begin_dsf", "pned_session_step", "pned_session_read", "pned_session_vector",
     "pned_session_end", "pned_session_profile", "pned_hv_noalloc",
     "pned_slots_create", "pned_slots_destroy", "pned_slots_info", "pned_slots_set_stream", "pned_slots_load",
@@ -105,6 +105,8 @@ def lib() -> C.CDLL:
     L.pned_lanczos_run.argtypes = [vp, vp, i32, i32, dp, dp, dp, ip, i32]
     L.pned_tps_run.argtypes = [vp, dbl, vp, i32, i32, C.POINTER(Observable), dp, dp, dp, i32]
     L.pned_dsf_run.argtypes = [vp, vp, dp, i32, dp, dp, dp, i32]
+    L.pned_dsf_xy_run.argtypes = [vp, vp, i32, vp, dp, i32, dp, dp, dp, i32]
+    L.pned_session_begin_dsf_xy.argtypes = [vp, vp, i32, vp, dp, i32, dp, i32]
     L.pned_cg_run.argtypes = [vp, dbl, vp, i32, i32, vp, ip, ip, i32]
     L.pned_bisec.argtypes = [dp, dp, i32, dp, i32, dbl]
     L.pned_vec12.argtypes = [dp, dp, dp, i32, i32, dp]

@@ -495,6 +495,22 @@ class Context:
         check(rc)
         return dict(cnorm=cn, salpha=sa.reshape(n_steps, self.R), sbeta=sb.reshape(n_steps + 1, self.R))
 
+    def dsf_xy(self, source: "Model", x, qr, n_steps: int, ipm: int = 1):
+        """intalv_xy + parallelized_dsflnc1z: chains of this context's model (the
+        target sector) from S^{ipm}_q x, x on `source`'s basis; qr [R][n]."""
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        if qr.shape != (self.R, self.model.n):
+            raise ValueError("qr must have shape (R, n)")
+        n_x = x.numel() if _is_dev(x) else x.size
+        if n_x != source.dim:
+            raise ValueError("x must have the source model's dim elements")
+        p, f = _ptr(x)
+        cn = np.zeros(self.R)
+        sa = np.zeros(n_steps * self.R)
+        sb = np.zeros((n_steps + 1) * self.R)
+        check(lib().pned_dsf_xy_run(self._h, source._h, int(ipm), p, _dp(qr), n_steps, _dp(cn), _dp(sa), _dp(sb), f))
+        return dict(cnorm=cn, salpha=sa.reshape(n_steps, self.R), sbeta=sb.reshape(n_steps + 1, self.R))
+
     def lanczos_vector(self, v_init, alpha, beta, coef, x_out=None):
         """parallelized_lncv1z (R = 1): x = sum_k coef[k] v_k over the replayed chain, normalised."""
         self._check_len(v_init)

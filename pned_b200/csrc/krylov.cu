@@ -149,6 +149,59 @@ __global__ void __launch_bounds__(kThreads) szq_kernel(const double2 *__restrict
     block_reduce_store<1, kMaxVPT>(red, Gs, vpt, R, partials);
 }
 
+// S^{ipm}_q start vectors (intalv_xy) as a gather over the target basis:
+// C[st, r] = sum over sites j (ascending) with a valid source digit of
+// fac * e^{i qr[r, j]} x[source index of state - ipm q^j].  Target states come
+// from t_list1 (null: full basis), source indices from the source Lin tables
+// (null: full basis).
+__global__ void __launch_bounds__(kThreads) sxy_kernel(const double2 *__restrict__ x, const double2 *__restrict__ ph,
+                                                       int64_t dim, int R, int vpt, int n, int q, int ipm,
+                                                       const int64_t *__restrict__ t_list1,
+                                                       const int64_t *__restrict__ s_lo,
+                                                       const int64_t *__restrict__ s_hi, int64_t s_mod, double2 *C,
+                                                       double2 *partials)
+{
+    double2 red[1][kMaxVPT];
+    for (int j = 0; j < kMaxVPT; ++j) red[0][j] = make_double2(0.0, 0.0);
+    const int Gs = R / vpt, r0 = (threadIdx.x % Gs) * vpt;
+    const double ss = 0.5 * (q - 1);
+    for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < dim * Gs;
+         it += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t st = it / Gs;
+        const int64_t state = t_list1 ? t_list1[st] : st;
+        double2 w[kMaxVPT];
+        for (int j = 0; j < kMaxVPT; ++j) w[j] = make_double2(0.0, 0.0);
+        int64_t y = state, pw = 1;
+        for (int site = 0; site < n; ++site, pw *= q) {
+            const int64_t z = y / q;
+            const int d = int(y - z * q);
+            y = z;
+            const int ds = d - ipm;   // the source digit
+            if (ds < 0 || ds >= q) continue;
+            const double sm = double(ds) - ss;
+            const double fac = ipm == 1 ? sqrt((ss - sm) * (ss + sm + 1.0)) : sqrt((ss + sm) * (ss - sm + 1.0));
+            const int64_t src = state - int64_t(ipm) * pw;
+            const int64_t si = s_lo ? s_lo[src % s_mod] + s_hi[src / s_mod] - 1 : src;
+            const double2 xs = x[si];
+#pragma unroll
+            for (int j = 0; j < kMaxVPT; ++j) {
+                if (j >= vpt) break;
+                const double2 p = ph[(r0 + j) * n + site];
+                const double2 rot = make_double2(p.x * xs.x - p.y * xs.y, p.y * xs.x + p.x * xs.y);
+                w[j].x += fac * rot.x;
+                w[j].y += fac * rot.y;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxVPT; ++j) {
+            if (j >= vpt) break;
+            C[st * R + r0 + j] = w[j];
+            red[0][j].x += w[j].x * w[j].x + w[j].y * w[j].y;
+        }
+    }
+    block_reduce_store<1, kMaxVPT>(red, Gs, vpt, R, partials);
+}
+
 __global__ void dsf_start_epilogue(const double2 *__restrict__ s, int R, int n, double *sc, double *cnorm)
 {
     const int r = threadIdx.x;
@@ -440,6 +493,55 @@ extern "C" int pned_session_begin_dsf(pned_ctx *c, const pned_c128 *x, const dou
     return PNED_OK;
 }
 
+extern "C" int pned_session_begin_dsf_xy(pned_ctx *c, const pned_model *source, int ipm, const pned_c128 *x,
+                                         const double *qr, int max_steps, double *cnorm, int flags)
+{
+    if (!c || !source || !x || !qr || max_steps < 1 || (ipm != 1 && ipm != -1))
+        return fail(PNED_EINVAL, "pned_session_begin_dsf_xy: bad arguments");
+    if (source->n != c->m->n || source->q != c->m->q || source->device != c->m->device)
+        return fail(PNED_EINVAL, "pned_session_begin_dsf_xy: source and target models differ in n, q or device");
+    cudaSetDevice(c->m->device);
+    int rc = session_common_begin(c, PNED_SESSION_DSF, max_steps);
+    if (rc) return rc;
+    Session &S = c->sess;
+    const int R = c->R, n = c->m->n;
+    const size_t sdim = size_t(source->dim);
+    const double2 *dx = reinterpret_cast<const double2 *>(x);
+    cudaError_t e = cudaSuccess;
+    if (!(flags & PNED_PTR_DEVICE)) {
+        double2 *tmp = sess_alloc<double2>(S, sdim);
+        if (!tmp) { session_release(c); return fail(PNED_ENOMEM, "pned_session_begin_dsf_xy: staging x"); }
+        e = cudaMemcpyAsync(tmp, x, sizeof(double2) * sdim, cudaMemcpyHostToDevice, c->stream);
+        dx = tmp;
+    }
+    std::vector<double2> ph(size_t(R) * n);
+    for (int r = 0; r < R; ++r)
+        for (int j = 0; j < n; ++j) ph[size_t(r) * n + j] = make_double2(std::cos(qr[r * n + j]), std::sin(qr[r * n + j]));
+    double2 *dph = sess_alloc<double2>(S, ph.size());
+    double *dcn = sess_alloc<double>(S, R);
+    if (!dph || !dcn) { session_release(c); return fail(PNED_ENOMEM, "pned_session_begin_dsf_xy: scratch"); }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dph, ph.data(), sizeof(double2) * ph.size(), cudaMemcpyHostToDevice, c->stream);
+    const bool ssec = source->hp.sector;
+    if (e == cudaSuccess) {
+        sxy_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(dx, dph, c->m->dim, R, pick_vpt(R), n, c->m->q, ipm,
+                                                          c->m->d_list1, ssec ? source->d_lin_lo : nullptr,
+                                                          ssec ? source->d_lin_hi : nullptr,
+                                                          ssec ? source->lin_mod : 1, c->buf[S.b0], c->partials);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, c->sums, c->stream);
+    if (e == cudaSuccess) {
+        dsf_start_epilogue<<<1, 32 * ((R + 31) / 32), 0, c->stream>>>(c->sums, R, n, slot(c, kSlotSc), dcn);
+        e = cudaGetLastError();
+    }
+    std::vector<double> hc(R);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hc.data(), dcn, sizeof(double) * R, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "pned_session_begin_dsf_xy: S^pm_q"); }
+    if (cnorm) std::copy(hc.begin(), hc.end(), cnorm);
+    return PNED_OK;
+}
+
 extern "C" int pned_session_step(pned_ctx *c, int n_steps)
 {
     if (!c || n_steps < 0) return fail(PNED_EINVAL, "pned_session_step: bad arguments");
@@ -642,6 +744,24 @@ extern "C" int pned_dsf_run(pned_ctx *c, const pned_c128 *x, const double *qr, i
     if (!c || !x || !qr || !cnorm || !salpha || !sbeta || n_steps < 1)
         return fail(PNED_EINVAL, "pned_dsf_run: bad arguments");
     int rc = pned_session_begin_dsf(c, x, qr, n_steps, cnorm, flags);
+    if (rc) return rc;
+    const int R = c->R;
+    std::vector<double> b(size_t(n_steps) * R);
+    rc = pned_session_step(c, n_steps);
+    int status = 0;
+    if (!rc) rc = pned_session_read(c, salpha, b.data(), nullptr, nullptr, &status);
+    pned_session_end(c);
+    if (rc) return rc;
+    for (int r = 0; r < R; ++r) sbeta[r] = cnorm[r];
+    for (size_t i = 0; i < b.size(); ++i) sbeta[R + i] = b[i];
+    return PNED_OK;
+}
+
+extern "C" int pned_dsf_xy_run(pned_ctx *c, const pned_model *source, int ipm, const pned_c128 *x, const double *qr,
+                               int n_steps, double *cnorm, double *salpha, double *sbeta, int flags)
+{
+    if (!c || !cnorm || !salpha || !sbeta || n_steps < 1) return fail(PNED_EINVAL, "pned_dsf_xy_run: bad arguments");
+    int rc = pned_session_begin_dsf_xy(c, source, ipm, x, qr, n_steps, cnorm, flags);
     if (rc) return rc;
     const int R = c->R;
     std::vector<double> b(size_t(n_steps) * R);

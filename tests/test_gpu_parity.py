@@ -467,6 +467,46 @@ def test_torch_tensors_written_just_before_the_call_are_ready():
     ctx.close()
 
 
+XY_CASES = [
+    # (L1, L2, q, tree, ipm, R, sector): S^{ipm}_q start vectors and DSF chains
+    (3, 2, 2, 0, 1, 2, True),
+    (3, 1, 3, 1, 1, 1, True),
+    (3, 1, 3, 1, -1, 2, True),
+    (2, 2, 2, 0, 1, 1, False),
+]
+
+
+@pytest.mark.parametrize("case", XY_CASES, ids=[f"{c[0]}x{c[1]}q{c[2]}ipm{c[4]}R{c[5]}{'s' if c[6] else 'f'}"
+                                                 for c in XY_CASES])
+def test_dsf_xy_chains(case):
+    """DSF chains from S^{ipm}_q x (intalv_xy): x on the source sector, chains on the
+    target sector (or both on the full basis); cnorm, salpha, sbeta follow the
+    oracle's intalv_xy + parallelized_dsflnc1z."""
+    L1, L2, q, tree, ipm, R, sector = case
+    cl = honeycomb(L1, L2)
+    n = cl.n
+    cpl = CP.kitaev_heisenberg(1.0, 0.0) if sector else KH
+    X, skip, pt = P.build_xlocal(q, tree, cpl)
+    assert (pt == 0) == sector
+    s0 = n // 2 * (q - 1)
+    st = s0 + ipm if sector else s0
+    gs = P.Model(n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt, s0)
+    gt = P.Model(n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt, st)
+    os_ = O.Model(n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt, s0)
+    ot = O.Model(n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt, st)
+    x = O.gaussian(13, gs.dim)
+    x /= np.linalg.norm(x)
+    qr = np.stack([cl.qr(r + 1) for r in range(R)])
+    steps = 25
+    out = P.Context(gt, R=R).dsf_xy(gs, x, qr, steps, ipm=ipm)
+    for r in range(R):
+        v, cn = ot.intalv_xy(os_, ipm, qr[r], x)
+        sa, sb = ot.dsf_chain(v, cn, steps)
+        assert abs(out["cnorm"][r] - cn.real) <= 1e-12 * cn.real
+        assert rel(out["salpha"][:12, r], sa[:12]) <= 1e-10
+        assert rel(out["sbeta"][:12, r], sb[:12]) <= 1e-10
+
+
 def test_lanczos_breakdown_is_reported():
     """A start vector that is an eigenvector makes beta vanish after one step: the
     run returns PNED_EBREAKDOWN (the reference stops with #(E07), Lanczos.f90:126-130)."""

@@ -142,6 +142,42 @@ def test_sz_sector_hv():
     assert np.linalg.norm(w - Hs.T @ v) < 1e-13 * np.linalg.norm(w)
 
 
+@pytest.mark.parametrize("q,tree,ipm", [(2, 0, 1), (3, 1, 1), (3, 1, -1), (4, 1, 1)])
+def test_intalv_xy_vs_explicit_ladder(q, tree, ipm):
+    """S^{ipm}_q x between Sz sectors (the DSF 'xx'/'uu'/'dd' start vector): the
+    oracle equals the ladder operator applied state by state, with the
+    spin-ladder factor sqrt((S -+ m)(S +- m + 1)) (1 for S = 1/2), summed over
+    sites, then normalised; cnorm = ||v||^2 / n."""
+    cl = honeycomb(2, 2) if q == 2 else honeycomb(3, 1)
+    n = cl.n
+    X = O.xlocal(q, tree, CP.kitaev_heisenberg(1.0, 0.0))
+    skip, _, pt = O.parity_skip(q, tree, X)
+    assert pt == 0
+    s0 = n // 2 * (q - 1)
+    ms = O.Model(n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt, s0)
+    mt = O.Model(n, q, tree, cl.ipair, cl.ibond_type, X, skip, pt, s0 + ipm)
+    src, _, _ = O.mk_list12(n, q, 0, s0)
+    tgt, _, _ = O.mk_list12(n, q, 0, s0 + ipm)
+    where = {int(t): i for i, t in enumerate(tgt)}
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(ms.ldim) + 1j * rng.standard_normal(ms.ldim)
+    qr = rng.uniform(-math.pi, math.pi, n)
+    S = 0.5 * (q - 1)
+    ref = np.zeros(mt.ldim, dtype=complex)
+    for j in range(n):
+        for i, st in enumerate(src):
+            d = (int(st) // q ** j) % q
+            if not 0 <= d + ipm < q:
+                continue
+            m_ = d - S
+            fac = math.sqrt((S - m_) * (S + m_ + 1)) if ipm == 1 else math.sqrt((S + m_) * (S - m_ + 1))
+            ref[where[int(st) + ipm * q ** j]] += fac * np.exp(1j * qr[j]) * x[i]
+    raw = np.vdot(ref, ref).real
+    v, cn = mt.intalv_xy(ms, ipm, qr, x)
+    assert np.linalg.norm(v - ref / math.sqrt(raw)) <= 1e-13
+    assert abs(cn - raw / n) <= 1e-12 * raw / n
+
+
 def test_bisec_vec12_vs_numpy():
     rng = np.random.default_rng(3)
     for nd in [5, 40, 300]:
