@@ -681,35 +681,47 @@ int plan_qtiles(const HostProgram &P, int k, int low, std::vector<QTilePass> &pa
     };
     while (left > 0) {
         if (int(passes.size()) >= kQTileMaxPasses) return PNED_ENOTSUP;
-        // seed: the uncovered bond whose sites touch the most uncovered bonds
-        size_t seed = 0;
-        int best = -1;
+        // the site set grown from one seed bond: the `low` lowest sites (kept in
+        // every tile for runs of q^low consecutive states), the seed's sites, then
+        // the site that brings the most uncovered bonds inside (ties: the one
+        // touching most uncovered bonds)
+        auto grow = [&](size_t seed) {
+            std::vector<int> T;
+            for (int x = 0; x < low && x < k; ++x) T.push_back(x);
+            for (int x : {bonds[seed].first, bonds[seed].second})
+                if (int(T.size()) < k && std::find(T.begin(), T.end(), x) == T.end()) T.push_back(x);
+            auto has = [&](int x) { return std::find(T.begin(), T.end(), x) != T.end(); };
+            while (int(T.size()) < k) {
+                int bx = -1, bg = -1, bt = -1;
+                for (int x = 0; x < n; ++x) {
+                    if (has(x)) continue;
+                    int g = 0;
+                    for (size_t i = 0; i < bonds.size(); ++i) {
+                        if (covered[i]) continue;
+                        const int a = bonds[i].first, b = bonds[i].second;
+                        if ((a == x && (b == x || has(b))) || (b == x && has(a))) ++g;
+                    }
+                    const int t = touching(x);
+                    if (g > bg || (g == bg && t > bt)) { bx = x; bg = g; bt = t; }
+                }
+                T.push_back(bx);
+            }
+            return T;
+        };
+        // every uncovered bond is tried as the seed; the set covering most wins
+        std::vector<int> S;
+        int best_gain = -1;
         for (size_t i = 0; i < bonds.size(); ++i) {
             if (covered[i]) continue;
-            const int c = touching(bonds[i].first) + touching(bonds[i].second);
-            if (c > best) { best = c; seed = i; }
+            std::vector<int> T = grow(i);
+            int gain = 0;
+            for (size_t b = 0; b < bonds.size(); ++b)
+                if (!covered[b] && std::find(T.begin(), T.end(), bonds[b].first) != T.end() &&
+                    std::find(T.begin(), T.end(), bonds[b].second) != T.end())
+                    ++gain;
+            if (gain > best_gain) { best_gain = gain; S = T; }
         }
-        // the `low` lowest sites are in every tile: runs of q^low consecutive states
-        std::vector<int> S;
-        for (int x = 0; x < low && x < k; ++x) S.push_back(x);
-        for (int x : {bonds[seed].first, bonds[seed].second})
-            if (int(S.size()) < k && std::find(S.begin(), S.end(), x) == S.end()) S.push_back(x);
         auto in = [&](int x) { return std::find(S.begin(), S.end(), x) != S.end(); };
-        while (int(S.size()) < k) {
-            int bx = -1, bg = -1, bt = -1;
-            for (int x = 0; x < n; ++x) {
-                if (in(x)) continue;
-                int g = 0;
-                for (size_t i = 0; i < bonds.size(); ++i) {
-                    if (covered[i]) continue;
-                    const int a = bonds[i].first, b = bonds[i].second;
-                    if ((a == x && (b == x || in(b))) || (b == x && in(a))) ++g;
-                }
-                const int t = touching(x);
-                if (g > bg || (g == bg && t > bt)) { bx = x; bg = g; bt = t; }
-            }
-            S.push_back(bx);
-        }
         std::sort(S.begin(), S.end());
         QTilePass pass;
         pass.sites = S;
