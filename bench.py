@@ -303,7 +303,9 @@ def run_ours(args, rank, world, local_rank):
     if tuning is not None:
         pl = list(tuning["plan"]) + [-1] * (4 - len(tuning["plan"]))
         line["roofline"]["tuned_plan"] = {"row_fixed_bits": pl[0], "window_bits": pl[1], "max_passes": pl[2],
-                                          "j_bits": pl[3], "candidates": len(tuning.get("tried", []))}
+                                          "j_bits": pl[3] if len(pl) > 3 else -1,
+                                          "blocks_per_sm": pl[6] if len(pl) > 6 else -1,
+                                          "candidates": len(tuning.get("tried", []))}
     if rank == 0 and args.cpu_baseline:
         try:
             cs = CpuSample(args.n_sites, os.cpu_count() or 1, slice_log2=args.ref_slice_log2)

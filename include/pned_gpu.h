@@ -152,6 +152,8 @@ typedef struct {
                                     (cp.async); 2 streams own and partner tiles with bulk copies (TMA engine)
                                     through a ring of 32 KB shared-memory stages, one block per SM; 2 needs
                                     tile rows that keep >= 3 low global bits, else the plan uses 0 */
+    int32_t blocks_per_sm; /* R = 1, j_bits 3: 3 builds the gather kernel for three resident blocks per SM
+                              (85 registers, faster up to about 2^26 states); else two (the default) */
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 /*

@@ -314,10 +314,10 @@ class Model:
         return out
 
     def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
-                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0):
+                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1):
         """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""
         tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles))
+                            int(stage_partner_tiles), int(blocks_per_sm))
         check(lib().pned_model_set_plan(self._h, int(R), C.byref(tp)))
         return self.plan(R)
 
@@ -698,9 +698,9 @@ class SlotBatch:
         return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
 
     def set_plan(self, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
-                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0) -> dict:
+                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1) -> dict:
         tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles))
+                            int(stage_partner_tiles), int(blocks_per_sm))
         check(lib().pned_slots_set_plan(self._h, C.byref(tp)))
         return self.plan()
 

@@ -135,8 +135,8 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
 // rows per thread, fewer registers, more warps to hide the gather latency.
 __host__ __device__ constexpr int tile_blocks_per_sm(int jb) { return jb >= 3 ? 2 : (jb == 2 ? 3 : 4); }
 
-template <int JB, bool RC, bool RD, int K>
-__global__ void __launch_bounds__(kThreads, tile_blocks_per_sm(JB))
+template <int JB, bool RC, bool RD, int K, int BPS = tile_blocks_per_sm(JB)>
+__global__ void __launch_bounds__(kThreads, BPS)
     hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
 {
     constexpr int SPT = 1 << JB;
@@ -1313,17 +1313,17 @@ static cudaError_t set_carveout(const void *kern, int device, size_t smem, int b
 // consecutive tiles, so partner tiles on the fast outer bits are found in L2.
 static int tile_grid(const pned_model *m, int nblocks)
 {
-    const int per_sm = m->tile_stage == 2 ? 1 : tile_blocks_per_sm(m->tile_jb);
+    const int per_sm = m->tile_stage == 2 ? 1 : m->tile_bps;
     return std::max(1, std::min(nblocks, per_sm * m->nsm));
 }
 
-template <int JB, bool RC, bool RD, int K>
+template <int JB, bool RC, bool RD, int K, int BPS = tile_blocks_per_sm(JB)>
 static cudaError_t launch_tile_j(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
-    auto kern = hv_tile_kernel<JB, RC, RD, K>;
+    auto kern = hv_tile_kernel<JB, RC, RD, K, BPS>;
     cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
     if (e == cudaSuccess && m->carveout)
-        e = set_carveout(reinterpret_cast<const void *>(kern), m->device, m->tile_smem, tile_blocks_per_sm(JB));
+        e = set_carveout(reinterpret_cast<const void *>(kern), m->device, m->tile_smem, BPS);
     if (e != cudaSuccess) return e;
     const int grid = tile_grid(m, nblocks);
     HvArgs b = a;
@@ -1401,7 +1401,9 @@ static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nbloc
     switch (m->tile_jb) {
     case 1: return launch_tile_j<1, RC, RD, K>(m, a, nblocks, st);
     case 2: return launch_tile_j<2, RC, RD, K>(m, a, nblocks, st);
-    case 3: return launch_tile_j<3, RC, RD, K>(m, a, nblocks, st);
+    case 3:   // 8 rows per thread: two resident blocks (121 registers) or three (85, some spills)
+        if (m->tile_bps == 3) return launch_tile_j<3, RC, RD, K, 3>(m, a, nblocks, st);
+        return launch_tile_j<3, RC, RD, K>(m, a, nblocks, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1716,6 +1718,7 @@ void build_tile_programs(pned_model *m)
     if (hp.q == 2 && !hp.sector && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes) == PNED_OK) {
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
+        m->tile_bps = (jb == 3 && m->plan1.blocks_per_sm == 3) ? 3 : tile_blocks_per_sm(jb);
         m->tile_stage = std::max(0, std::min(2, m->plan1.stage_partner_tiles));
         m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
         m->use_tile = true;
@@ -2012,12 +2015,12 @@ extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *p
                  plan->j_bits > kTileMaxJB || plan->j_bits == 0))
         return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
     if (R == 1) {
-        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1};
+        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1, -1};
         m->carveout = m->plan1.l1_carveout != 0;
         build_tile_programs(m);
         return PNED_OK;
     }
-    const pned_tile_plan def{-1, -1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1};
     if (plan) m->carveout = plan->l1_carveout != 0;
     ensure_rtiles(m, R, false, plan ? plan : &def);
     return PNED_OK;

@@ -36,8 +36,9 @@ struct pned_model {
         size_t smem = 0;
     };
     std::map<int, QTileSet> qtiles;
-    pned_tile_plan plan1{-1, -1, -1, -1, -1, -1};   // single-vector plan parameters (-1: defaults)
+    pned_tile_plan plan1{-1, -1, -1, -1, -1, -1, -1};   // single-vector plan parameters (-1: defaults)
     int tile_jb = 3;                        // j bits (rows per thread 2^jb) of the single-vector tiles
+    int tile_bps = 2;                       // resident blocks per SM the single-vector tile kernel is built for
     bool carveout = true;                   // size the shared-memory carveout to the tiles (rest L1)
     int tile_stage = 0;                     // single-vector partner tiles: 0 gathered through L1/L2,
                                             // 1 staged in shared memory (cp.async), 2 streamed by bulk copies

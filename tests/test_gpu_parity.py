@@ -390,7 +390,7 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
 
 @pytest.mark.parametrize("plan", [(8, 10, 4, 3, 1, 1), (5, 10, 2, 3, 1, 1), (3, 8, 1, 3, 1, 1), (5, 12, 2, 2, 1, 0),
                                   (5, 12, 2, 1, 0, 0), (8, 10, 4, 3, 1, 2), (5, 10, 2, 3, 1, 2), (3, 8, 1, 3, 1, 2),
-                                  (5, 6, 3, 3, 1, 2)])
+                                  (5, 6, 3, 3, 1, 2), (8, 8, 2, 3, 1, 0, 3), (5, 10, 2, 3, 1, 0, 3)])
 def test_tile_plans_agree_with_oracle(plan):
     """Every tile plan the autotuner may pick (rows kept, window, passes, rows per
     thread, carveout, staged or bulk-streamed partner tiles) gives the oracle's
