@@ -548,3 +548,23 @@ def test_larger_hv_parity_n24():
     # prdct sums 2^24 terms with cancellation: bound the error by the absolute sum
     scale = np.sum(np.abs(v1) * np.abs(v0))
     assert abs(pr[0] - prr) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("name", ["s12_kh_n8", "s12_khg_h111_n12", "s1_kh_n6", "s1_khg_h111_n8"])
+def test_cuda_path_against_golden_fixtures(name):
+    """The CUDA path, through the C ABI, reproduces the committed fixtures of
+    tests/golden (H^T v and the ground-state energy from the independent dense
+    construction)."""
+    from tests.test_oracle import golden_case
+    c = golden_case(name)
+    X, skip, pt = P.build_xlocal(c["q"], c["tree"], c["cpl"], field=c["field"])
+    m = P.Model(c["n"], c["q"], c["tree"], c["ipair"], c["btype"], X, skip, pt)
+    ctx = P.Context(m, R=1)
+    if "v" in c:
+        w = np.zeros_like(c["v"])
+        ctx.p_mltply_v3(np.ascontiguousarray(c["v"]), w)
+        assert np.linalg.norm(w - c["w"]) <= 1e-12 * np.linalg.norm(c["w"])
+    v = O.gaussian(3, m.dim)
+    v /= np.linalg.norm(v)
+    run = ctx.lanczos(v, 250, check_conv=True)
+    assert abs(run["ene"][0] - c["e"][0]) <= 1e-10 * abs(c["e"][0])

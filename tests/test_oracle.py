@@ -6,6 +6,7 @@ construction of H, known analytic answers, and numpy/scipy for the
 tridiagonal and continued-fraction routines.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -289,3 +290,36 @@ def test_inverse_iteration_ground_state():
     # the reference shifts by the Lanczos E0; a tiny offset keeps (H - E) regular
     x, ni, nc = m.inverse_iteration(ev[0] - 1e-9, b, inv_max=50, cg_max=500)
     assert abs(abs(np.vdot(evec[:, 0], x)) - 1) < 1e-8
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.npz")
+GOLDEN_CASES = ["s12_kh_n8", "s12_khg_h111_n12", "s1_kh_n6", "s1_khg_h111_n8"]
+
+
+def golden_case(name):
+    g = np.load(GOLDEN)
+    q, tree, n = (int(x) for x in g[f"{name}/q"])
+    fld = g[f"{name}/field"] if bool(g[f"{name}/has_field"][0]) else None
+    case = dict(q=q, tree=tree, n=n, ipair=g[f"{name}/ipair"], btype=g[f"{name}/btype"],
+                cpl=g[f"{name}/couplings"], field=fld, e=g[f"{name}/e"])
+    if f"{name}/v" in g:
+        case["v"], case["w"] = g[f"{name}/v"], g[f"{name}/w"]
+    return case
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_against_golden_fixtures(name):
+    """The oracle reproduces the committed fixtures of tests/golden (H^T v and the
+    ground-state energy from the independent dense construction)."""
+    c = golden_case(name)
+    X = O.xlocal(c["q"], c["tree"], c["cpl"], field=c["field"])
+    skip, _, pt = O.parity_skip(c["q"], c["tree"], X)
+    m = O.Model(c["n"], c["q"], c["tree"], c["ipair"], c["btype"], X, skip, pt)
+    if "v" in c:
+        w = np.zeros_like(c["v"])
+        m.p_mltply_v3(np.ascontiguousarray(c["v"]), w)
+        assert np.linalg.norm(w - c["w"]) <= 1e-12 * np.linalg.norm(c["w"])
+    v = O.gaussian(3, m.ldim)
+    v /= np.linalg.norm(v)
+    run = m.lanczos(v, 250, check_conv=True)
+    assert abs(run["ene"][0] - c["e"][0]) <= 1e-10 * abs(c["e"][0])
