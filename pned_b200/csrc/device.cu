@@ -742,12 +742,13 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1)
 // Tiled multi-vector H.V (R > 1 interleaved vectors, S = 1/2 full basis), one
 // pass of a multi-pass program.  G = R / VPT threads share a state; a block
 // owns a tile of NS * SPT states (NS = 256 / G state rows): thread t serves
-// vectors r0 .. r0 + VPT - 1 (r0 = (t mod G) VPT) of row l = t / G, whose j-th
-// state is base | jexp[j] with the bits of l on the global bits rowpos[].  The
-// tile's rows of R values are staged in shared memory ([SPT][NS][R]): in-tile
-// flips gather there, the others through L1/L2 from the partner tile, VPT
-// contiguous values per load.  SLOT: per-vector coefficient tables
-// ([ntab][R]) and real diagonals ([dim][R]).
+// vectors g, g + G, ..., g + (VPT-1) G (g = t mod G) of row l = t / G, whose
+// j-th state is base | jexp[j] with the bits of l on the global bits rowpos[]:
+// the G threads of a row read its R values as VPT contiguous runs of G
+// values, so every load instruction uses whole sectors.  The tile's rows of R
+// values are staged in shared memory ([SPT][NS][R]): in-tile flips gather
+// there, the others through L1/L2 from the partner tile.  SLOT: per-vector
+// coefficient tables ([ntab][R]) and real diagonals ([dim][R]).
 template <int VPT, int SPT, bool SLOT, bool RC, bool RD, int K>
 __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
 {
@@ -759,7 +760,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
     double2 *s_tab = smem + size_t(SPT) * NS * R;
     const int tabw = SLOT ? R : 1;
     for (int i = threadIdx.x; i < prog.ntab * tabw; i += blockDim.x) s_tab[i] = a.table[i];
-    const int g = threadIdx.x % G, l = threadIdx.x / G, r0 = g * VPT;
+    const int g = threadIdx.x % G, l = threadIdx.x / G;   // vectors g, g + G, ..., g + (VPT-1) G
     const int64_t ntiles = int64_t(1) << prog.nouter;
     double2 red[K][VPT];
 #pragma unroll
@@ -777,18 +778,18 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
 #pragma unroll
             for (int j = 0; j < SPT; ++j)
 #pragma unroll
-                for (int q = 0; q < VPT; ++q) v[j][q] = __ldg(a.C + int64_t(base | prog.jexp[j]) * R + r0 + q);
+                for (int q = 0; q < VPT; ++q) v[j][q] = __ldg(a.C + int64_t(base | prog.jexp[j]) * R + g + q * G);
             __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
 #pragma unroll
             for (int j = 0; j < SPT; ++j)
 #pragma unroll
-                for (int q = 0; q < VPT; ++q) s_v[(j * NS + l) * R + r0 + q] = v[j][q];
+                for (int q = 0; q < VPT; ++q) s_v[(j * NS + l) * R + g + q * G] = v[j][q];
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const int64_t sj = base | prog.jexp[j];
 #pragma unroll
                 for (int q = 0; q < VPT; ++q) {
-                    const int r = r0 + q;
+                    const int r = g + q * G;
                     if (!prog.first) {
                         acc[j][q] = make_double2(0.0, 0.0);
                         continue;
@@ -819,12 +820,12 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const uint32_t idx = T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib;
-                const double2 *ct = s_tab + (T.tab + idx) * tabw + (SLOT ? r0 : 0);
-                const double2 *sv = s_v + ((int(j ^ mhi)) * NS + lp) * R + r0;
+                const double2 *ct = s_tab + (T.tab + idx) * tabw + (SLOT ? g : 0);
+                const double2 *sv = s_v + ((int(j ^ mhi)) * NS + lp) * R + g;
 #pragma unroll
                 for (int q = 0; q < VPT; ++q) {
-                    const double2 c = ct[SLOT ? q : 0];
-                    const double2 w = sv[q];
+                    const double2 c = ct[SLOT ? q * G : 0];
+                    const double2 w = sv[q * G];
                     if (RC && !SLOT) { acc[j][q].x = fma(c.x, w.x, acc[j][q].x); acc[j][q].y = fma(c.x, w.y, acc[j][q].y); }
                     else acc[j][q] = cfma(c, w, acc[j][q]);
                 }
@@ -838,7 +839,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
             for (int j = 0; j < SPT; ++j)
 #pragma unroll
                 for (int q = 0; q < VPT; ++q)
-                    w0[j][q] = __ldg(a.C + int64_t((base | prog.jexp[j]) ^ T.mask) * R + r0 + q);
+                    w0[j][q] = __ldg(a.C + int64_t((base | prog.jexp[j]) ^ T.mask) * R + g + q * G);
             uint32_t ib = 0;
 #pragma unroll
             for (int d = 0; d < kMaxDeps; ++d)
@@ -846,10 +847,10 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const uint32_t idx = T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib;
-                const double2 *ct = s_tab + (T.tab + idx) * tabw + (SLOT ? r0 : 0);
+                const double2 *ct = s_tab + (T.tab + idx) * tabw + (SLOT ? g : 0);
 #pragma unroll
                 for (int q = 0; q < VPT; ++q) {
-                    const double2 c = ct[SLOT ? q : 0];
+                    const double2 c = ct[SLOT ? q * G : 0];
                     if (RC && !SLOT) {
                         acc[j][q].x = fma(c.x, w0[j][q].x, acc[j][q].x);
                         acc[j][q].y = fma(c.x, w0[j][q].y, acc[j][q].y);
@@ -863,7 +864,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
         for (int j = 0; j < SPT; ++j) {
 #pragma unroll
             for (int q = 0; q < VPT; ++q) {
-                const int r = r0 + q;
+                const int r = g + q * G;
                 const int64_t e = int64_t(base | prog.jexp[j]) * R + r;
                 const double sc = a.sc[r];
                 const double2 hv = cscale(a.hsc ? a.hsc[r] : sc, acc[j][q]);
@@ -891,7 +892,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
             }
         }
     }
-    block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
+    block_reduce_store<K, VPT, true>(red, G, VPT, R, a.partials);
 }
 
 // Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by

@@ -169,9 +169,10 @@ __device__ __forceinline__ uint64_t pack_digits(int64_t s, int n, int q)
 }
 __device__ __forceinline__ int digit_at(uint64_t digits, int j) { return int((digits >> (2 * j)) & 3u); }
 
-// Block-level reduction of red[K][VPT] (vector r = g*vpt + j, g = lane % G,
-// G a power of two dividing 32) into partials[blockIdx.x][K][R].
-template <int K, int VPT>
+// Block-level reduction of red[K][VPT] (vector r = g*vpt + j, or g + j*G when
+// STRIDED; g = lane % G, G a power of two dividing 32) into
+// partials[blockIdx.x][K][R].
+template <int K, int VPT, bool STRIDED = false>
 __device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G, int vpt, int R, double2 *partials)
 {
     __shared__ double2 sm[kThreads / 32][kMaxK][kMaxR];
@@ -189,7 +190,7 @@ __device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G
         for (int k = 0; k < K; ++k)
 #pragma unroll
             for (int j = 0; j < VPT; ++j)
-                if (j < vpt) sm[warp][k][lane * vpt + j] = red[k][j];
+                if (j < vpt) sm[warp][k][STRIDED ? lane + j * G : lane * vpt + j] = red[k][j];
     __syncthreads();
     const int nw = blockDim.x >> 5;
     for (int idx = threadIdx.x; idx < K * R; idx += blockDim.x) {
