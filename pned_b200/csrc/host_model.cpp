@@ -357,6 +357,7 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
         rc = pned_mk_list12(n, q, 0, d->total_sz, &ldim, P.list1.data(), P.lin_lo.data(), P.lin_hi.data());
         if (rc) return rc;
         P.sector = true;
+        P.total = d->total_sz;
         P.ihf = ihf;
         P.dim = ldim;
     }

@@ -500,6 +500,11 @@ extern "C" int pned_session_begin_dsf_xy(pned_ctx *c, const pned_model *source, 
         return fail(PNED_EINVAL, "pned_session_begin_dsf_xy: bad arguments");
     if (source->n != c->m->n || source->q != c->m->q || source->device != c->m->device)
         return fail(PNED_EINVAL, "pned_session_begin_dsf_xy: source and target models differ in n, q or device");
+    // a sector source needs the neighbouring sector as target: every target state
+    // minus one ladder step must be a source-sector state for its Lin lookup
+    if (source->hp.sector && (!c->m->hp.sector || c->m->hp.total != source->hp.total + ipm))
+        return fail(PNED_EINVAL, "pned_session_begin_dsf_xy: for a sector source the context's model must be the "
+                                 "sector of digit sum source + ipm");
     cudaSetDevice(c->m->device);
     int rc = session_common_begin(c, PNED_SESSION_DSF, max_steps);
     if (rc) return rc;

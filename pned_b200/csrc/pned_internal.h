@@ -85,6 +85,7 @@ struct HostProgram {
     // Sz sector (parity_type == 0): sector index -> state, and the Lin tables
     // (index = lin_lo[state mod q^ihf] + lin_hi[state / q^ihf] - 1)
     bool sector = false;
+    int total = 0;                       // digit sum of the sector states (sector only)
     int ihf = 0;
     std::vector<int64_t> list1, lin_lo, lin_hi;
     int nbond = 0;

@@ -499,6 +499,9 @@ def test_dsf_xy_chains(case):
     qr = np.stack([cl.qr(r + 1) for r in range(R)])
     steps = 25
     out = P.Context(gt, R=R).dsf_xy(gs, x, qr, steps, ipm=ipm)
+    if sector:   # a target that is not the neighbouring sector is refused before any kernel runs
+        with pytest.raises(P.PnedError):
+            P.Context(gs, R=R).dsf_xy(gs, x, qr, steps, ipm=ipm)
     for r in range(R):
         v, cn = ot.intalv_xy(os_, ipm, qr[r], x)
         sa, sb = ot.dsf_chain(v, cn, steps)
