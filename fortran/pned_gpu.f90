@@ -10,6 +10,7 @@ module pned_gpu
   public :: pned_gpu_init, pned_gpu_finalize, p_mltply_v3_gpu, calc_vec_inprdct_gpu, pned_lanczos_run_f
   public :: pned_lncv1_f, pned_inv1_f, pned_tps_run_f, pned_dump_alpha_beta_coef_f
   public :: pned_lanczos_begin_f, pned_steps_f, pned_lanczos_read_f, pned_interval_dump_f, pned_interval_dump_read_f
+  public :: pned_gpu_init_target, pned_dsf_zz_f, pned_dsf_xy_f, pned_append_sq_f, pned_dump_alpha_beta_f
 
   type, bind(C) :: pned_model_desc
     integer(c_int32_t) :: n_sites, q_spin, tree, n_bonds
@@ -119,6 +120,44 @@ module pned_gpu
       character(kind=c_char), intent(in) :: path(*)
       integer(c_int), value :: max_steps
     end function
+    integer(c_int) function pned_dsf_run(c, x, qr, nsteps, cnorm, salpha, sbeta, flags) bind(C, name="pned_dsf_run")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c
+      complex(c_double_complex), intent(in) :: x(*)
+      real(c_double), intent(in) :: qr(*)
+      integer(c_int), value :: nsteps, flags
+      real(c_double), intent(out) :: cnorm(*), salpha(*), sbeta(*)
+    end function
+    integer(c_int) function pned_dsf_xy_run(c, source, ipm, x, qr, nsteps, cnorm, salpha, sbeta, flags) &
+        bind(C, name="pned_dsf_xy_run")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c, source
+      integer(c_int), value :: ipm, nsteps, flags
+      complex(c_double_complex), intent(in) :: x(*)
+      real(c_double), intent(in) :: qr(*)
+      real(c_double), intent(out) :: cnorm(*), salpha(*), sbeta(*)
+    end function
+    integer(c_int) function pned_append_sq(path, iq, q1, q2, norm_re) bind(C, name="pned_append_sq")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), value :: iq
+      real(c_double), value :: q1, q2, norm_re
+    end function
+    integer(c_int) function pned_write_dsf_alpha_beta(path, sq, salpha, sbeta, s_maxitr) &
+        bind(C, name="pned_write_dsf_alpha_beta")
+      import :: c_int, c_char, c_double, c_double_complex
+      character(kind=c_char), intent(in) :: path(*)
+      complex(c_double_complex), value :: sq
+      real(c_double), intent(in) :: salpha(*), sbeta(*)
+      integer(c_int), value :: s_maxitr
+    end function
+    integer(c_int) function pned_write_dsf_vectors(path, indx, v1, v2, ll) bind(C, name="pned_write_dsf_vectors")
+      import :: c_int, c_char, c_double_complex, c_int64_t
+      character(kind=c_char), intent(in) :: path(*)
+      integer(c_int), value :: indx
+      complex(c_double_complex), intent(in) :: v1(*), v2(*)
+      integer(c_int64_t), value :: ll
+    end function
     integer(c_int) function pned_ctx_destroy(c) bind(C, name="pned_ctx_destroy")
       import :: c_int, c_ptr
       type(c_ptr), value :: c
@@ -130,6 +169,8 @@ module pned_gpu
   end interface
 
   type(c_ptr), save :: g_model = c_null_ptr, g_ctx = c_null_ptr
+  !! second model and context: the neighbouring Sz sector of the S^+-_q DSF chains
+  type(c_ptr), save :: g_model2 = c_null_ptr, g_ctx2 = c_null_ptr
   integer(c_int32_t), allocatable, target, save :: g_ipair(:), g_btype(:)
   integer(c_int8_t), allocatable, target, save :: g_skip(:,:,:)
   complex(c_double_complex), allocatable, target, save :: g_x(:,:,:)
@@ -242,6 +283,69 @@ contains
                                alpha, beta, coef) /= 0) stop 'pned_write_salphasbeta failed'
   end subroutine pned_dump_alpha_beta_coef_f
 
+  !! The model of the same lattice and couplings in the sector of digit sum
+  !! total_sz_target (for intalv_xy: total_sz + ipm), after pned_gpu_init.
+  subroutine pned_gpu_init_target(n, q_spin, tree, ibond, parity_type, total_sz_target)
+    integer, intent(in) :: n, q_spin, tree, ibond, parity_type, total_sz_target
+    type(pned_model_desc) :: d
+    integer(c_int) :: rc
+    d%n_sites = n; d%q_spin = q_spin; d%tree = tree; d%n_bonds = ibond
+    d%ipair = c_loc(g_ipair); d%bond_type = c_loc(g_btype)
+    d%xlocal = c_loc(g_x); d%skip = c_loc(g_skip)
+    d%parity_type = parity_type; d%total_sz = total_sz_target
+    rc = pned_model_create(d, g_model2)
+    if (rc /= 0) stop 'pned_model_create (target sector) failed'
+    rc = pned_ctx_create(g_model2, 1_c_int, 0_c_size_t, g_ctx2)
+    if (rc /= 0) stop 'pned_ctx_create (target sector) failed'
+  end subroutine pned_gpu_init_target
+
+  !! intalv_zz + parallelized_dsflnc1z for one momentum: qr(j) = q.r_j; salpha(1:nsteps),
+  !! sbeta(1:nsteps+1) with sbeta(1) = cnorm, as the reference's DSF arrays.
+  subroutine pned_dsf_zz_f(x, qr, nsteps, cnorm, salpha, sbeta)
+    complex(kind(0d0)), intent(in) :: x(:)
+    double precision, intent(in) :: qr(:)
+    integer, intent(in) :: nsteps
+    double precision, intent(out) :: cnorm, salpha(:), sbeta(:)
+    double precision :: cn(1)
+    if (pned_dsf_run(g_ctx, x, qr, int(nsteps, c_int), cn, salpha, sbeta, 0_c_int) /= 0) stop 'pned_dsf_run failed'
+    cnorm = cn(1)
+  end subroutine pned_dsf_zz_f
+
+  !! intalv_xy ('xx'; Sa 'uu' ipm = 1, 'dd' ipm = -1) + parallelized_dsflnc1z: x on the
+  !! pned_gpu_init model's basis, the chain on pned_gpu_init_target's.
+  subroutine pned_dsf_xy_f(x, qr, nsteps, ipm, cnorm, salpha, sbeta)
+    complex(kind(0d0)), intent(in) :: x(:)
+    double precision, intent(in) :: qr(:)
+    integer, intent(in) :: nsteps, ipm
+    double precision, intent(out) :: cnorm, salpha(:), sbeta(:)
+    double precision :: cn(1)
+    if (pned_dsf_xy_run(g_ctx2, g_model, int(ipm, c_int), x, qr, int(nsteps, c_int), cn, salpha, sbeta, &
+                        0_c_int) /= 0) stop 'pned_dsf_xy_run failed'
+    cnorm = cn(1)
+  end subroutine pned_dsf_xy_f
+
+  !! The DSF driver's sq.txt line.
+  subroutine pned_append_sq_f(filename, iq, q, norm)
+    character(len=*), intent(in) :: filename
+    integer, intent(in) :: iq
+    double precision, intent(in) :: q(2), norm
+    if (pned_append_sq(trim(filename) // c_null_char, int(iq, c_int), real(q(1), c_double), real(q(2), c_double), &
+                       real(norm, c_double)) /= 0) stop 'pned_append_sq failed'
+  end subroutine pned_append_sq_f
+
+  !! dump_alpha_beta: SalphaSbeta_q... and vec_q... files in the reference's layout.
+  subroutine pned_dump_alpha_beta_f(ab_file, vec_file, indx, sq, salpha, sbeta, v1, v2)
+    character(len=*), intent(in) :: ab_file, vec_file
+    integer, intent(in) :: indx
+    complex(kind(0d0)), intent(in) :: sq
+    double precision, intent(in) :: salpha(:), sbeta(:)
+    complex(kind(0d0)), intent(in) :: v1(:), v2(:)
+    if (pned_write_dsf_alpha_beta(trim(ab_file) // c_null_char, sq, salpha, sbeta, &
+                                  int(size(salpha), c_int)) /= 0) stop 'pned_write_dsf_alpha_beta failed'
+    if (pned_write_dsf_vectors(trim(vec_file) // c_null_char, int(indx, c_int), v1, v2, &
+                               int(size(v1), c_int64_t)) /= 0) stop 'pned_write_dsf_vectors failed'
+  end subroutine pned_dump_alpha_beta_f
+
   !! Lanczos run in steps that can stop and resume (interval_dump / interval_dump_read).
   subroutine pned_lanczos_begin_f(v, max_steps)
     complex(kind(0d0)), intent(in) :: v(:)
@@ -277,8 +381,10 @@ contains
 
   subroutine pned_gpu_finalize()
     integer(c_int) :: rc
+    if (c_associated(g_ctx2)) rc = pned_ctx_destroy(g_ctx2)
+    if (c_associated(g_model2)) rc = pned_model_destroy(g_model2)
     if (c_associated(g_ctx)) rc = pned_ctx_destroy(g_ctx)
     if (c_associated(g_model)) rc = pned_model_destroy(g_model)
-    g_ctx = c_null_ptr; g_model = c_null_ptr
+    g_ctx = c_null_ptr; g_model = c_null_ptr; g_ctx2 = c_null_ptr; g_model2 = c_null_ptr
   end subroutine pned_gpu_finalize
 end module pned_gpu
