@@ -35,11 +35,16 @@ SEED = 20261203
 
 
 def workload_config(n_sites=30):
+    from pned_b200.lattice import cluster_for_sites
+    cl = cluster_for_sites(n_sites)
+    gb = 16 * 2 ** n_sites / 1e9
+    l2 = (f"inputs larger than L2 ({gb:.1f} GB per vector), no flush" if gb > 0.126 else
+          f"vectors of {gb * 1e3:.0f} MB, below L2 (no flush)")
     return {
-        "workload": f"S=1/2 Kitaev-Heisenberg honeycomb N={n_sites} (3x5 periodic, 45 bonds), full basis "
-                    f"D=2^{n_sites}, complex128, 1 Lanczos chain, J=cos(0.3pi), K=2sin(0.3pi)",
+        "workload": f"S=1/2 Kitaev-Heisenberg honeycomb N={n_sites} ({cl.L1}x{cl.L2} periodic, {cl.nbond} bonds), "
+                    f"full basis D=2^{n_sites}, complex128, 1 Lanczos chain, J=cos(0.3pi), K=2sin(0.3pi)",
         "n_sites": n_sites, "dim": 2 ** n_sites, "R": 1, "parallelism": "replicas",
-        "l2": "inputs larger than L2 (17.2 GB per vector), no flush",
+        "l2": l2,
         "seed": SEED,
     }
 
@@ -196,6 +201,41 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def dense_check(n_sites: int = 12):
+    """E0 of the headline couplings on a small cluster: the library's Lanczos
+    against full FP64 diagonalisation (numpy eigvalsh, LAPACK zheevd) of the
+    dense matrix assembled column by column from the library's own H.v.
+    Reports the Lanczos error only; the H.v itself is held to the oracle by the
+    parity tests."""
+    import numpy as np
+    import torch
+    import pned_b200 as P
+    model, cl = build_model(n_sites)
+    D, R = model.dim, 16
+    ctx = P.Context(model, R=R)
+    Ht = np.zeros((D, D), dtype=np.complex128)   # rows: H^T e_k (p_mltply_v3 applies H^T)
+    eye = torch.zeros(D * R, dtype=torch.complex128, device="cuda")
+    out = torch.zeros_like(eye)
+    for k0 in range(0, D, R):
+        eye.zero_()
+        out.zero_()
+        idx = torch.arange(R, device="cuda")
+        eye[(k0 + idx) * R + idx] = 1.0
+        ctx.p_mltply_v3(eye, out)
+        Ht[k0:k0 + R] = out.view(D, R).t().cpu().numpy()
+    ctx.close()
+    e_dense = float(np.linalg.eigvalsh(Ht.T)[0])
+    ctx1 = P.Context(model, R=1)
+    v = torch.empty(D, dtype=torch.complex128, device="cuda")
+    ctx1.fill_gaussian(SEED, v, normalise=True)
+    run = ctx1.lanczos(v, 300, check_conv=True)
+    ctx1.close()
+    model.close()
+    e_lz = float(run["ene"][0])
+    return {"n_sites": n_sites, "dim": D, "e0_lanczos": e_lz, "e0_dense_zheevd": e_dense,
+            "rel_err": abs(e_lz - e_dense) / abs(e_dense), "lanczos_steps": int(run["itr"])}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -306,6 +346,11 @@ def run_ours(args, rank, world, local_rank):
                                           "j_bits": pl[3] if len(pl) > 3 else -1,
                                           "blocks_per_sm": pl[6] if len(pl) > 6 else -1,
                                           "candidates": len(tuning.get("tried", []))}
+    if rank == 0 and args.dense_check:
+        try:
+            line["dense_check"] = dense_check(12)
+        except Exception as exc:  # reported, not fatal: the headline line stands without it
+            line["dense_check"] = {"error": str(exc)}
     if rank == 0 and args.cpu_baseline:
         try:
             cs = CpuSample(args.n_sites, os.cpu_count() or 1, slice_log2=args.ref_slice_log2)
@@ -591,6 +636,7 @@ def main():
     ap.add_argument("--p30", type=float, default=0.02)
     ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--no-served", dest="served", action="store_false")
+    ap.add_argument("--no-dense-check", dest="dense_check", action="store_false")
     ap.add_argument("--s1-sites", type=int, default=18)
     ap.add_argument("--s1-vectors", type=int, default=4)
     ap.add_argument("--served-requests", type=int, default=40)
