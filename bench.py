@@ -541,9 +541,10 @@ def run_s1(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def served_section(args, local_rank, n_requests, rate):
+def served_section(args, local_rank, n_requests, rate, sweep=()):
     """Serving stream (continuous batching) against the plain one-at-a-time path:
-    capacity (all requests queued at once), p50/p99 latency at `rate`, and the
+    capacity (all requests queued at once), p50/p99 latency at `rate` (and at
+    each rate of `sweep`: the same requests with arrival times rescaled), and the
     same requests run alone through the plain path."""
     import torch
     from pned_b200 import serve
@@ -552,9 +553,15 @@ def served_section(args, local_rank, n_requests, rate):
     budget = int(0.85 * free)
     cap_reqs = [serve.Request(**{**q.__dict__, "arrival": 0.0}) for q in reqs]
     srv = serve.Server(budget=budget, max_steps=512)
+    swept = []
     with ClockSampler(local_rank) as clk:
         cap = srv.run(cap_reqs, realtime=True)
         st = srv.run(reqs, realtime=True)
+        for r in sweep:
+            reqs_r = [serve.Request(**{**q.__dict__, "arrival": q.arrival * rate / r}) for q in reqs]
+            sr = serve.summarize(srv.run(reqs_r, realtime=True), reqs_r)
+            swept.append({"rate_per_s": r, "solves_per_s": sr["solves_per_s"], "p50_s": sr["p50_latency_s"],
+                          "p99_s": sr["p99_latency_s"], "makespan_s": sr["makespan_s"]})
     srv.close()
     torch.cuda.empty_cache()
     capacity = len(cap.results) / cap.makespan_s
@@ -582,6 +589,7 @@ def served_section(args, local_rank, n_requests, rate):
                      "note": "all requests queued at t=0"},
         "latency": {"rate_per_s": rate, "solves_per_s": s["solves_per_s"], "p50_s": s["p50_latency_s"],
                     "p99_s": s["p99_latency_s"], "makespan_s": s["makespan_s"]},
+        **({"latency_sweep": swept} if swept else {}),
         "plain": {"solves_per_s": plain, "sample": k, "mean_s": tp / k,
                   "max_rel_e0_diff_served_vs_plain": max(diffs) if diffs else None},
         "vs_plain": capacity / plain,
@@ -597,7 +605,8 @@ def run_serve(args, rank, world, local_rank):
         return
     torch.cuda.set_device(local_rank)
     P.lib().pned_set_device(local_rank)
-    sv = served_section(args, local_rank, args.requests, args.rate)
+    sweep = [float(x) for x in args.rates.split(",")] if args.rates else []
+    sv = served_section(args, local_rank, args.requests, args.rate, sweep)
     line = {
         "metric": "served_solves_per_s", "value": sv["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
@@ -633,6 +642,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=40)
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--rates", default=None, help="serve workload: further arrival rates, comma-separated "
+                                                  "(the same requests, arrival times rescaled)")
     ap.add_argument("--p30", type=float, default=0.02)
     ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--no-served", dest="served", action="store_false")
