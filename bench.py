@@ -482,6 +482,63 @@ def batched_dsf(dev, args):
     return out
 
 
+def run_sector(args, rank, world, local_rank):
+    """--workload sector: pure Heisenberg (J = 1) on the N-site honeycomb in the
+    Sz = 0 sector (parity_type 0: mk_list12 order, Lin-table partner lookup),
+    one Lanczos chain: K timed steps after W warm-up steps."""
+    import math
+    import torch
+    import pned_b200 as P
+    from pned_b200 import couplings as CP
+    from pned_b200.lattice import cluster_for_sites
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    P.lib().pned_set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.sector_sites
+    cl = cluster_for_sites(n)
+    with ClockSampler(local_rank) as clk:
+        m = P.Model.from_couplings(cl, CP.kitaev_heisenberg(1.0, 0.0))
+        D = m.dim
+        st = torch.cuda.Stream(device=dev)
+        ctx = P.Context(m, R=1, stream=st)
+        v = torch.empty(D, dtype=torch.complex128, device=dev)
+        ctx.fill_gaussian(SEED, v)
+        ctx.session_begin("lanczos", v, args.warmup + args.steps + args.profile_steps + 1)
+        ctx.session_step(args.warmup)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ctx.session_step(args.steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        hv_ms, step_ms = ctx.session_profile(args.profile_steps)
+        res = ctx.session_read()
+        ctx.session_end()
+        ctx.close()
+        m.close()
+    peak, peak_kind = load_peaks()
+    # per sector state: C 16 + P 16 + W 16 + real diagonal 8 = 56 B (as the full basis), plus the
+    # state list entry (8 B); the Lin tables (2 x 2^ceil(n/2) entries) stay in L2
+    bytes_hv = 64 * D
+    line = {
+        "metric": f"sector_lanczos_steps_per_s_N{n}", "value": 1000.0 / ms, "unit": "steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded complex Gaussian start vector)",
+        "config": {"workload": f"S=1/2 Heisenberg (J=1) honeycomb N={n} ({cl.L1}x{cl.L2}), Sz=0 sector "
+                               f"D={D} (mk_list12 order), complex128, 1 Lanczos chain", "dim": D, "R": 1},
+        "e0_per_site": float(P.bisec(res["alpha"][:, 0], res["beta"][:, 0], res["alpha"].shape[0], 1)[0]) / n,
+        "roofline": {"bound": "hbm", "kernel": "hv_xor_kernel (sector, K=1)", "achieved": bytes_hv / (hv_ms * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": bytes_hv / (hv_ms * 1e-3) / 1e9 / peak,
+                     "peak_kind": peak_kind, "hv_ms": hv_ms, "algorithmic_bytes_per_hv": bytes_hv},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_s1(args, rank, world, local_rank):
     """--workload s1: S=1 Kitaev-Heisenberg (mixed radix, base 3) on the 18-site honeycomb
     (3x3), K=-1, J=0.2, D=3^18: batched mTPQ with R=4 vectors (l=3.0, L=54) and a
@@ -634,7 +691,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
-    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1"])
+    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1", "sector"])
+    ap.add_argument("--sector-sites", type=int, default=30)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits[,l1_carveout[,stage]]' "
                                                  "instead of autotuning (profiling runs)")
@@ -672,6 +730,8 @@ def main():
             run_serve(args, rank, world, local_rank)
         elif args.workload == "s1":
             run_s1(args, rank, world, local_rank)
+        elif args.workload == "sector":
+            run_sector(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
