@@ -1451,6 +1451,12 @@ static cudaError_t launch_hv_v(const pned_model *m, const HvArgs &a, int nblocks
         b.lin_lo = m->d_lin_lo;
         b.lin_hi = m->d_lin_hi;
         b.lin_mod = m->lin_mod;
+        b.lin_pow2 = 0;
+        if ((m->lin_mod & (m->lin_mod - 1)) == 0) {
+            int sh = 0;
+            while ((int64_t(1) << sh) < m->lin_mod) ++sh;
+            b.lin_pow2 = sh + 1;
+        }
         return launch_hv_t<VPT, false, true, K, true>(m, b, nblocks, st);
     }
     if (m->real_coef && m->real_diag) return launch_hv_t<VPT, true, true, K>(m, a, nblocks, st);

@@ -106,11 +106,20 @@ struct HvArgs {
     const int64_t *lin_lo;
     const int64_t *lin_hi;
     int64_t lin_mod;
+    int lin_pow2;           // log2(lin_mod) + 1 when lin_mod is a power of two (q = 2, 4), else 0
 };
 
 // Sector index of a state (the reference's list_lib lookup).
 __device__ __forceinline__ int64_t lin_index(const HvArgs &a, uint64_t st)
 {
+    if (a.lin_pow2 > 0) {   // shift and mask
+        const int sh = a.lin_pow2 - 1;
+        return a.lin_lo[st & ((uint64_t(1) << sh) - 1)] + a.lin_hi[st >> sh] - 1;
+    }
+    if ((st >> 32) == 0) {   // 32-bit division (q^n < 2^32)
+        const uint32_t s32 = uint32_t(st), m = uint32_t(a.lin_mod), hi = s32 / m;
+        return a.lin_lo[s32 - hi * m] + a.lin_hi[hi] - 1;
+    }
     return a.lin_lo[st % uint64_t(a.lin_mod)] + a.lin_hi[st / uint64_t(a.lin_mod)] - 1;
 }
 
