@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
     }
     for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < nitems;
          it += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = it / G;
+        const int64_t s = G == 1 ? it : it / G;
         const uint32_t su = SECTOR ? uint32_t(a.list1[s]) : uint32_t(s);
         double2 v[VPT], acc[VPT];
         const double2 *cs = a.C + s * R + r0;
