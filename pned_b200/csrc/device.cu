@@ -103,9 +103,12 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
             for (int k = 0; k < kMaxDeps; ++k)
                 if (k < T.nb) idx |= ((su >> ((T.pos4 >> (8 * k)) & 0xffu)) & 1u) << k;
             const double2 c = s_tab[T.tab + idx];
-            // in the sector, zero elements (the reference's skip mask) leave it: no partner
-            if (SECTOR && c.x == 0.0 && c.y == 0.0) continue;
-            const double2 *ps = a.C + (SECTOR ? lin_index(a, su ^ T.xmask) : int64_t(su ^ T.xmask)) * R + r0;
+            // in the sector, zero elements (the reference's skip mask) lead out of it: their
+            // partner index is meaningless, so they read the own row and add zero (branch-free;
+            // the Lin tables cover every half-state, so the lookup itself stays in bounds)
+            int64_t pi = SECTOR ? lin_index(a, su ^ T.xmask) : int64_t(su ^ T.xmask);
+            if (SECTOR && c.x == 0.0 && c.y == 0.0) pi = s;
+            const double2 *ps = a.C + pi * R + r0;
 #pragma unroll
             for (int j = 0; j < VPT; ++j) {
                 const double2 w = __ldg(ps + j);
