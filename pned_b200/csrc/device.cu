@@ -270,478 +270,6 @@ __global__ void __launch_bounds__(kThreads, BPS)
     block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
 }
 
-// cp.async (Ampere-style asynchronous global -> shared copies, 16 bytes a thread).
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
-{
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// Single-vector tiled H.v with staged partner tiles: the same tiles and
-// passes as hv_tile_kernel, but each partner tile (the terms of one group) is
-// copied into shared memory once with cp.async, two buffers deep (group g + 1
-// loads while group g is computed), and all terms of the group gather from
-// there.  L2 sends each partner tile once instead of once per term, and the
-// copies in flight hold no registers.
-template <bool RC, bool RD, int K>
-__global__ void __launch_bounds__(kThreads, 2)
-    hv_tile_stage_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
-{
-    constexpr int SPT = 8;
-    constexpr int TILE = kThreads * SPT;
-    extern __shared__ double2 smem[];
-    double2 *s_v = smem;              // own tile
-    double2 *s_p = smem + TILE;       // two partner-tile buffers
-    double2 *s_tab = smem + 3 * TILE;
-    for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
-    const uint32_t tid = threadIdx.x;
-    const int64_t ntiles = int64_t(1) << prog.nouter;
-    double2 red[K][1];
-#pragma unroll
-    for (int k = 0; k < K; ++k) red[k][0] = make_double2(0.0, 0.0);
-    const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
-    const double hs = a.hsc ? a.hsc[0] : sc;
-    const double shift = a.shift + (a.shiftv ? a.shiftv[0] : 0.0);
-    uint32_t rowbase = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) rowbase |= ((tid >> k) & 1u) << prog.rowpos[k];
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        uint32_t base = rowbase;
-        for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
-        double2 acc[SPT];
-        {
-            double2 v[SPT];
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) v[j] = __ldg(a.C + (base | prog.jexp[j]));
-            __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) s_v[tid + kThreads * j] = v[j];
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) {
-                const uint32_t sj = base | prog.jexp[j];
-                if (!prog.first) {
-                    acc[j] = make_double2(0.0, 0.0);
-                } else if (RD) {
-                    acc[j] = cscale(__ldcs(static_cast<const double *>(a.diag) + sj) - shift, v[j]);
-                } else {
-                    double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + sj);
-                    dd.x -= shift;
-                    acc[j] = cmul(dd, v[j]);
-                }
-            }
-        }
-        // the first partner tile loads while the in-tile terms run
-        if (prog.ngroups > 0) {
-            const uint32_t pb = base ^ prog.gxor[0];
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) cp_async16(s_p + tid + kThreads * j, a.C + (pb | prog.jexp[j]));
-            cp_async_commit();
-        }
-        __syncthreads();
-        for (int t = 0; t < prog.nin; ++t) {
-            const TileTerm T = prog.t[t];
-            uint32_t ib = 0;
-#pragma unroll
-            for (int d = 0; d < kMaxDeps; ++d)
-                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
-            const double2 *sv = s_v + (tid ^ (T.mask & 0xffu));
-            const uint32_t mhi = T.mask >> 8;
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) {
-                const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
-                const double2 w = sv[kThreads * (j ^ mhi)];
-                if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                else acc[j] = cfma(c, w, acc[j]);
-            }
-        }
-        for (int g = 0; g < prog.ngroups; ++g) {
-            double2 *buf = s_p + (g & 1) * TILE;
-            if (g + 1 < prog.ngroups) {
-                // its buffer was released by the barrier that ended group g - 1
-                const uint32_t pb = base ^ prog.gxor[g + 1];
-                double2 *nb = s_p + ((g + 1) & 1) * TILE;
-#pragma unroll
-                for (int j = 0; j < SPT; ++j) cp_async16(nb + tid + kThreads * j, a.C + (pb | prog.jexp[j]));
-                cp_async_commit();
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
-            }
-            __syncthreads();   // group g's tile has landed for every thread
-            for (int t = prog.gstart[g]; t < prog.gstart[g + 1]; ++t) {
-                const TileTerm T = prog.t[t];
-                uint32_t ib = 0;
-#pragma unroll
-                for (int d = 0; d < kMaxDeps; ++d)
-                    if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
-                const double2 *sv = buf + (tid ^ (T.lmask & 0xffu));
-                const uint32_t mhi = T.lmask >> 8;
-#pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    const double2 c = s_tab[T.tab + (T.hasj ? (ib | ((T.jtab >> (4 * j)) & 15u)) : ib)];
-                    const double2 w = sv[kThreads * (j ^ mhi)];
-                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                    else acc[j] = cfma(c, w, acc[j]);
-                }
-            }
-            __syncthreads();   // every thread is done with buf before it is refilled
-        }
-#pragma unroll
-        for (int j = 0; j < SPT; ++j) {
-            const int64_t e = base | prog.jexp[j];
-            const double2 hv = cscale(hs, acc[j]);
-            double2 out = hv;
-            if (!prog.first) {
-                const double2 w0 = __ldcs(a.W + e);
-                out.x += w0.x;
-                out.y += w0.y;
-            } else if (a.P) {
-                const double2 p = __ldcs(a.P + e);
-                out.x = fma(pc, p.x, out.x);
-                out.y = fma(pc, p.y, out.y);
-            }
-            __stcs(a.W + e, out);
-            const double2 vv = cscale(sc, s_v[tid + kThreads * j]);
-            red[0][0] = cadd(red[0][0], cconjmul(vv, hv));
-            if (!prog.last) continue;
-            if (K >= 2) red[1][0].x += out.x * out.x + out.y * out.y;
-            if (K >= 4 && a.G) {
-                const double2 gv = cscale(gs, a.G[e]);
-                red[2][0] = cadd(red[2][0], cconjmul(gv, out));
-                red[3][0] = cadd(red[3][0], cconjmul(gv, vv));
-            }
-        }
-    }
-    block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
-}
-
-// ---------------------------------------------------------------------------
-// Bulk-copy pipeline (TMA engine, mbarriers) for the single-vector tiles
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-// Bounded wait for the phase of parity `parity` to complete: at most
-// kBulkSpins polls, each suspended for at most ~1 us; false if it gave up.
-constexpr uint32_t kBulkSpins = 1u << 22;
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    for (uint32_t i = 0; i < kBulkSpins; ++i) {
-        uint32_t ok;
-        asm volatile("{\n\t.reg .pred p;\n\t"
-                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}\n"
-                     : "=r"(ok)
-                     : "r"(bar), "r"(parity), "r"(1000u)
-                     : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-// The same wait for a whole warp: true only if every lane saw the phase.
-__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity)
-{
-    return __all_sync(0xffffffffu, mbar_wait(bar, parity));
-}
-// One contiguous global -> shared copy by the bulk-copy (TMA) engine, no
-// multicast; completion is counted in bytes on the mbarrier.
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-constexpr int kBulkJB = 3;
-constexpr int kBulkTile = kThreads << kBulkJB;   // 2048 states, 32 KB
-constexpr int kBulkMaxStages = 8;
-constexpr int kBulkHead = 256;                   // bytes before the ring: mbarriers and bookkeeping
-constexpr int kBulkMinRunBits = 3;               // copies of at least 8 states (128 B)
-constexpr int kBulkConsumerWarps = 16;           // 8: 8 states per thread; 16: 4
-
-// Single-vector tiled H.v with the partner tiles streamed by the bulk-copy
-// engine: the same tiles, passes, term order and arithmetic as
-// hv_tile_kernel (W is bit-identical; the block sums group the tiles
-// differently), with the data movement split off.  Warp CW (producer) walks
-// the block's item sequence -- per tile its own tile, then one partner tile
-// per group -- and streams each item into a ring of `nst` 32 KB
-// shared-memory stages as contiguous runs of 2^f states (the tile's rows keep
-// global bits 0..f-1), accounted on the stage's `full` mbarrier.  Warps
-// 0..CW-1 (consumers) wait on `full`, gather their terms' partners from the
-// stage and release it on `empty` (one arrival per warp); consumer thread c
-// serves row c mod 256 and 2048 / (32 CW) of its states.  Up to nst items are
-// in flight per SM without holding registers, and no block-wide barrier sits
-// in the tile loop.  One block per SM (grid = SM count).  Every wait is
-// bounded: on a timeout the block sets *a.err, stops, waits (bounded) for the
-// copies it issued and exits.
-template <int CW, bool RC, bool RD, int K>
-__global__ void __launch_bounds__(32 * (CW + 1), 1)
-    hv_tile_bulk_kernel(const __grid_constant__ TileProgram prog, const HvArgs a, int nst)
-{
-    constexpr int SPT = (1 << kBulkJB) * 8 / CW;   // states per consumer thread
-    extern __shared__ __align__(128) unsigned char bulk_smem[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(bulk_smem);
-    uint64_t *empty = full + kBulkMaxStages;
-    volatile int *s_abort = reinterpret_cast<volatile int *>(empty + kBulkMaxStages);
-    int *s_count = reinterpret_cast<int *>(bulk_smem) + 2 * 2 * kBulkMaxStages + 1;   // [CW + 1]: consumed, issued
-    double2 *ring = reinterpret_cast<double2 *>(bulk_smem + kBulkHead);
-    double2 *s_tab = ring + size_t(nst) * kBulkTile;
-    __shared__ double2 s_red[CW + 1][kMaxK];
-
-    const uint32_t tid = threadIdx.x;
-    const int warp = int(tid >> 5), lane = int(tid & 31);
-    for (int i = tid; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
-    if (tid == 0) {
-        for (int s = 0; s < nst; ++s) {
-            mbar_init(smem_addr(full + s), 1);
-            mbar_init(smem_addr(empty + s), CW);
-        }
-        *s_abort = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    }
-    __syncthreads();
-
-    const int64_t ntiles = int64_t(1) << prog.nouter;
-    const int items = 1 + prog.ngroups;
-    double2 red[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) red[k] = make_double2(0.0, 0.0);
-
-    if (warp == CW) {
-        // ---------------- producer ----------------
-        int f = 0;
-        while (f < 8 && prog.rowpos[f] == f) ++f;
-        const int ncp = kBulkTile >> f;
-        const uint32_t bytes = uint32_t(sizeof(double2)) << f;
-        uint32_t it = 0;
-        bool ok = true;
-        for (int64_t tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
-            uint32_t ob = 0;
-            for (int k = 0; k < prog.nouter; ++k) ob |= uint32_t((tile >> k) & 1) << prog.outer[k];
-            for (int item = 0; item < items; ++item, ++it) {
-                const uint32_t s = it % uint32_t(nst), round = it / uint32_t(nst);
-                if (round > 0 && !warp_wait(smem_addr(empty + s), (round - 1) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                if (__any_sync(0xffffffffu, *s_abort != 0)) {
-                    ok = false;
-                    break;
-                }
-                const uint32_t src = ob ^ (item == 0 ? 0u : prog.gxor[item - 1]);
-                if (lane == 0) mbar_arrive_expect_tx(smem_addr(full + s), uint32_t(kBulkTile * sizeof(double2)));
-                __syncwarp();
-                const uint32_t dst0 = smem_addr(ring + size_t(s) * kBulkTile);
-                for (int c = lane; c < ncp; c += 32) {
-                    const uint32_t L = uint32_t(c) << f;
-                    uint32_t off = prog.jexp[L >> 8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                        if (k >= f) off |= ((L >> k) & 1u) << prog.rowpos[k];
-                    bulk_g2s(dst0 + L * uint32_t(sizeof(double2)), a.C + (src | off), bytes, smem_addr(full + s));
-                }
-            }
-        }
-        if (!ok) {
-            *s_abort = 1;
-            if (lane == 0 && a.err) atomicExch(a.err, 1);
-        }
-        if (lane == 0) s_count[CW] = int(it);
-    } else {
-        // ---------------- consumers ----------------
-        const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
-        const double hs = a.hsc ? a.hsc[0] : sc;
-        const double shift = a.shift + (a.shiftv ? a.shiftv[0] : 0.0);
-        const uint32_t row = tid & (kThreads - 1);
-        const int j0 = int(tid / kThreads) * SPT;   // first of the thread's states in the row
-        uint32_t rowbase = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) rowbase |= ((row >> k) & 1u) << prog.rowpos[k];
-        uint32_t it = 0;
-        bool ok = true;
-        for (int64_t tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
-            uint32_t base = rowbase;
-            for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
-            // streams of the epilogue and the diagonal, issued before the first wait
-            double2 pw[SPT];
-            double dr[SPT];
-            double2 dc[SPT];
-#pragma unroll
-            for (int jj = 0; jj < SPT; ++jj) {
-                const uint32_t e = base | prog.jexp[j0 + jj];
-                if (!prog.first) pw[jj] = __ldcs(a.W + e);
-                else if (a.P) pw[jj] = __ldcs(a.P + e);
-                if (prog.first) {
-                    if (RD) dr[jj] = __ldcs(static_cast<const double *>(a.diag) + e);
-                    else dc[jj] = __ldcs(static_cast<const double2 *>(a.diag) + e);
-                }
-            }
-            double2 v[SPT], acc[SPT];
-            // own tile: its values, the diagonal and the in-tile terms
-            {
-                const uint32_t s = it % uint32_t(nst);
-                if (!warp_wait(smem_addr(full + s), (it / uint32_t(nst)) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                const double2 *sv0 = ring + size_t(s) * kBulkTile;
-#pragma unroll
-                for (int jj = 0; jj < SPT; ++jj) {
-                    v[jj] = sv0[row + kThreads * (j0 + jj)];
-                    if (!prog.first) {
-                        acc[jj] = make_double2(0.0, 0.0);
-                    } else if (RD) {
-                        acc[jj] = cscale(dr[jj] - shift, v[jj]);
-                    } else {
-                        double2 dd = dc[jj];
-                        dd.x -= shift;
-                        acc[jj] = cmul(dd, v[jj]);
-                    }
-                }
-                for (int t = 0; t < prog.nin; ++t) {
-                    const TileTerm T = prog.t[t];
-                    uint32_t ib = 0;
-#pragma unroll
-                    for (int d = 0; d < kMaxDeps; ++d)
-                        if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
-                    const double2 *sv = sv0 + (row ^ (T.mask & 0xffu));
-                    const uint32_t mhi = T.mask >> 8;
-                    if (!T.hasj) {
-                        const double2 c = s_tab[T.tab + ib];
-#pragma unroll
-                        for (int jj = 0; jj < SPT; ++jj) {
-                            const double2 w = sv[kThreads * ((j0 + jj) ^ mhi)];
-                            if (RC) { acc[jj].x = fma(c.x, w.x, acc[jj].x); acc[jj].y = fma(c.x, w.y, acc[jj].y); }
-                            else acc[jj] = cfma(c, w, acc[jj]);
-                        }
-                        continue;
-                    }
-#pragma unroll
-                    for (int jj = 0; jj < SPT; ++jj) {
-                        const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * (j0 + jj))) & 15u))];
-                        const double2 w = sv[kThreads * ((j0 + jj) ^ mhi)];
-                        if (RC) { acc[jj].x = fma(c.x, w.x, acc[jj].x); acc[jj].y = fma(c.x, w.y, acc[jj].y); }
-                        else acc[jj] = cfma(c, w, acc[jj]);
-                    }
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_addr(empty + s));
-                ++it;
-            }
-            // partner tiles, one per group, in the program's term order
-            for (int g = 0; g < prog.ngroups; ++g, ++it) {
-                const uint32_t s = it % uint32_t(nst);
-                if (!warp_wait(smem_addr(full + s), (it / uint32_t(nst)) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                const double2 *buf = ring + size_t(s) * kBulkTile;
-                for (int t = prog.gstart[g]; t < prog.gstart[g + 1]; ++t) {
-                    const TileTerm T = prog.t[t];
-                    uint32_t ib = 0;
-#pragma unroll
-                    for (int d = 0; d < kMaxDeps; ++d)
-                        if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
-                    const double2 *sv = buf + (row ^ (T.lmask & 0xffu));
-                    const uint32_t mhi = T.lmask >> 8;
-                    if (!T.hasj) {
-                        const double2 c = s_tab[T.tab + ib];
-#pragma unroll
-                        for (int jj = 0; jj < SPT; ++jj) {
-                            const double2 w = sv[kThreads * ((j0 + jj) ^ mhi)];
-                            if (RC) { acc[jj].x = fma(c.x, w.x, acc[jj].x); acc[jj].y = fma(c.x, w.y, acc[jj].y); }
-                            else acc[jj] = cfma(c, w, acc[jj]);
-                        }
-                        continue;
-                    }
-#pragma unroll
-                    for (int jj = 0; jj < SPT; ++jj) {
-                        const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * (j0 + jj))) & 15u))];
-                        const double2 w = sv[kThreads * ((j0 + jj) ^ mhi)];
-                        if (RC) { acc[jj].x = fma(c.x, w.x, acc[jj].x); acc[jj].y = fma(c.x, w.y, acc[jj].y); }
-                        else acc[jj] = cfma(c, w, acc[jj]);
-                    }
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_addr(empty + s));
-            }
-            if (!ok) break;
-#pragma unroll
-            for (int jj = 0; jj < SPT; ++jj) {
-                const int64_t e = base | prog.jexp[j0 + jj];
-                const double2 hv = cscale(hs, acc[jj]);
-                double2 out = hv;
-                if (!prog.first) {
-                    out.x += pw[jj].x;
-                    out.y += pw[jj].y;
-                } else if (a.P) {
-                    out.x = fma(pc, pw[jj].x, out.x);
-                    out.y = fma(pc, pw[jj].y, out.y);
-                }
-                __stcs(a.W + e, out);
-                const double2 vv = cscale(sc, v[jj]);
-                red[0] = cadd(red[0], cconjmul(vv, hv));
-                if (!prog.last) continue;
-                if (K >= 2) red[1].x += out.x * out.x + out.y * out.y;
-                if (K >= 4 && a.G) {
-                    const double2 gv = cscale(gs, a.G[e]);
-                    red[2] = cadd(red[2], cconjmul(gv, out));
-                    red[3] = cadd(red[3], cconjmul(gv, vv));
-                }
-            }
-        }
-        if (!ok) {
-            *s_abort = 1;
-            if (lane == 0 && a.err) atomicExch(a.err, 1);
-        }
-        if (lane == 0) s_count[warp] = int(it);
-    }
-    __syncthreads();
-    // after a timeout: wait (bounded) for every copy still in flight before the
-    // block's shared memory is released
-    if (*s_abort && tid == 0) {
-        int lo = s_count[0];
-        for (int w = 1; w < CW; ++w) lo = min(lo, s_count[w]);
-        for (int i = lo; i < s_count[CW]; ++i)
-            mbar_wait(smem_addr(full + (uint32_t(i) % uint32_t(nst))), (uint32_t(i) / uint32_t(nst)) & 1u);
-    }
-    // deterministic block sum: warps in order (the producer's terms are zero)
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        for (int off = 16; off >= 1; off >>= 1) {
-            red[k].x += __shfl_xor_sync(0xffffffffu, red[k].x, off);
-            red[k].y += __shfl_xor_sync(0xffffffffu, red[k].y, off);
-        }
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < K; ++k) s_red[warp][k] = red[k];
-    __syncthreads();
-    if (int(tid) < K) {
-        double2 sum = make_double2(0.0, 0.0);
-        for (int w = 0; w < CW + 1; ++w) sum = cadd(sum, s_red[w][tid]);
-        a.partials[(size_t)blockIdx.x * K + tid] = sum;
-    }
-}
-
 // Tiled multi-vector H.V (R > 1 interleaved vectors, S = 1/2 full basis), one
 // pass of a multi-pass program.  G = R / VPT threads share a state; a block
 // owns a tile of NS * SPT states (NS = 256 / G state rows): thread t serves
@@ -968,192 +496,6 @@ __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constan
     block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
 }
 
-// Tiled mixed-radix H.V (q > 2, full basis, R interleaved vectors), one pass
-// of a multi-pass program.  A block stages tile t -- the q^k states whose
-// outer digits spell t -- in shared memory with cp.async, vector-major
-// ([R][nt]: a warp's partner reads fall on distinct banks), then applies the
-// pass's terms (bonds with both sites among the k tile sites) there: partner =
-// local index + loff, coefficient = the pass's table[tab + pair state].
-// G = R / VPT threads share a state, each with VPT consecutive vectors.  The
-// epilogue's streams (P or W, the diagonal) of an item are requested before
-// its terms run.  The first pass adds the diagonal and pc P; later passes
-// accumulate into W; the last forms the K >= 2 sums.
-template <int VPT, bool RC, bool RD, int K>
-__global__ void __launch_bounds__(kThreads, 2) hv_qtile_kernel(const __grid_constant__ QTileProgram prog, const HvArgs a)
-{
-    extern __shared__ double2 smem[];
-    const int R = a.R, G = R / VPT, nt = prog.nt, q = prog.q;
-    double2 *s_v = smem;                                           // [R][nt]
-    double2 *s_tab = s_v + size_t(nt) * R;                         // [ntab]
-    uint32_t *s_goff = reinterpret_cast<uint32_t *>(s_tab + prog.ntab);   // [nt]
-    uint32_t *s_dig = s_goff + nt;                                 // [nt]
-    for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = prog.tab[i];
-    for (int l = threadIdx.x; l < nt; l += blockDim.x) {
-        uint32_t dig = 0, off = 0;
-        int x = l;
-        for (int i = 0; i < prog.k; ++i) {
-            const int d = x % q;
-            x /= q;
-            dig |= uint32_t(d) << (2 * i);
-            off += uint32_t(d) * prog.spow[i];
-        }
-        s_dig[l] = dig;
-        s_goff[l] = off;
-    }
-    const int g = int(threadIdx.x) % G;
-    const int r0 = g * VPT;
-    double scr[VPT], pcr[VPT], gsr[VPT];
-#pragma unroll
-    for (int j = 0; j < VPT; ++j) {
-        scr[j] = a.sc[r0 + j];
-        pcr[j] = a.pc ? a.pc[r0 + j] : 0.0;
-        gsr[j] = a.gsc ? a.gsc[r0 + j] : 0.0;
-    }
-    double2 red[K][VPT];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int j = 0; j < VPT; ++j) red[k][j] = make_double2(0.0, 0.0);
-    const int nitems = nt * G;
-    __shared__ uint32_t s_base;
-    for (int64_t tile = blockIdx.x; tile < prog.ntiles; tile += gridDim.x) {
-        __syncthreads();   // the previous tile's shared reads are done (first tile: tables staged)
-        if (threadIdx.x == 0) {   // tile -> outer digits -> first state (q^n < 2^32)
-            uint32_t b = 0, x = uint32_t(tile);
-            for (int i = 0; i < prog.nouter; ++i) {
-                const uint32_t y = x / uint32_t(q);
-                b += (x - y * uint32_t(q)) * prog.opow[i];
-                x = y;
-            }
-            s_base = b;
-        }
-        __syncthreads();
-        const uint32_t base = s_base;
-        for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
-            const int l = it / G;
-            const double2 *src = a.C + size_t(base + s_goff[l]) * R + r0;
-#pragma unroll
-            for (int j = 0; j < VPT; ++j) cp_async16(s_v + ((r0 + j) * nt + l), src + j);
-        }
-        cp_async_commit();
-        // the first item's epilogue streams load while the tile lands
-        double2 pn[VPT];
-        double dn = 0.0;
-        double2 dcn = make_double2(0.0, 0.0);
-        auto prefetch = [&](int it) {
-            if (it >= nitems) return;
-            const size_t st = base + s_goff[it / G];
-#pragma unroll
-            for (int j = 0; j < VPT; ++j) {
-                const size_t e = st * R + r0 + j;
-                if (!prog.first) pn[j] = __ldcs(a.W + e);
-                else if (a.P) pn[j] = __ldcs(a.P + e);
-            }
-            if (prog.first) {
-                if (RD) dn = __ldcs(static_cast<const double *>(a.diag) + st);
-                else dcn = __ldcs(static_cast<const double2 *>(a.diag) + st);
-            }
-        };
-        prefetch(threadIdx.x);
-        cp_async_wait<0>();
-        __syncthreads();
-        for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
-            const int l = it / G;
-            double2 v[VPT], acc[VPT];
-#pragma unroll
-            for (int j = 0; j < VPT; ++j) {
-                v[j] = s_v[(r0 + j) * nt + l];
-                acc[j] = make_double2(0.0, 0.0);
-            }
-            const uint32_t dig = s_dig[l];
-            // branch-free: a zero coefficient (target digit out of range, or a
-            // zero matrix element) adds zero; its partner index, which may leave
-            // the tile, is clamped into it
-#pragma unroll 2
-            for (int t = 0; t < prog.nterms; ++t) {
-                const QTileTerm T = prog.t[t];
-                const int pair = int((dig >> (2 * T.ls1)) & 3u) + q * int((dig >> (2 * T.ls2)) & 3u);
-                const double2 c = s_tab[T.tab + pair];
-                const int pidx = r0 * nt + min(max(l + T.loff, 0), nt - 1);
-#pragma unroll
-                for (int j = 0; j < VPT; ++j) {
-                    const double2 w = s_v[pidx + j * nt];
-                    if (RC) {
-                        acc[j].x = fma(c.x, w.x, acc[j].x);
-                        acc[j].y = fma(c.x, w.y, acc[j].y);
-                    } else {
-                        acc[j] = cfma(c, w, acc[j]);
-                    }
-                }
-            }
-            if (prog.first) {   // the diagonal after the terms: its value arrived meanwhile
-#pragma unroll
-                for (int j = 0; j < VPT; ++j) {
-                    if (RD) {
-                        const double dd = dn - a.shift;
-                        acc[j].x = fma(dd, v[j].x, acc[j].x);
-                        acc[j].y = fma(dd, v[j].y, acc[j].y);
-                    } else {
-                        double2 dd = dcn;
-                        dd.x -= a.shift;
-                        acc[j] = cfma(dd, v[j], acc[j]);
-                    }
-                }
-            }
-            const size_t st = base + s_goff[l];
-#pragma unroll
-            for (int j = 0; j < VPT; ++j) {
-                const size_t e = st * R + r0 + j;
-                const double2 hv = cscale(scr[j], acc[j]);
-                double2 out = hv;
-                if (!prog.first) {
-                    out.x += pn[j].x;
-                    out.y += pn[j].y;
-                } else if (a.P) {
-                    out.x = fma(pcr[j], pn[j].x, out.x);
-                    out.y = fma(pcr[j], pn[j].y, out.y);
-                }
-                __stcs(a.W + e, out);
-                const double2 vv = cscale(scr[j], v[j]);
-                red[0][j] = cadd(red[0][j], cconjmul(vv, hv));
-                if (!prog.last) continue;
-                if (K >= 2) red[1][j].x += out.x * out.x + out.y * out.y;
-                if (K >= 4 && a.G) {
-                    const double2 gv = cscale(gsr[j], a.G[e]);
-                    red[2][j] = cadd(red[2][j], cconjmul(gv, out));
-                    red[3][j] = cadd(red[3][j], cconjmul(gv, vv));
-                }
-            }
-            prefetch(it + int(blockDim.x));
-        }
-    }
-    // block sums (the pattern of block_reduce_store, in the dynamic buffer)
-    for (int off = 16; off >= G; off >>= 1)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-#pragma unroll
-            for (int j = 0; j < VPT; ++j) {
-                red[k][j].x += __shfl_xor_sync(0xffffffffu, red[k][j].x, off);
-                red[k][j].y += __shfl_xor_sync(0xffffffffu, red[k][j].y, off);
-            }
-    __syncthreads();   // the tile buffer is free
-    double2 *sm = s_v;   // [warps][K][R]
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane < G)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-#pragma unroll
-            for (int j = 0; j < VPT; ++j) sm[(size_t(warp) * K + k) * R + lane * VPT + j] = red[k][j];
-    __syncthreads();
-    const int nw = blockDim.x >> 5;
-    for (int idx = threadIdx.x; idx < K * R; idx += blockDim.x) {
-        const int k = idx / R, r = idx - k * R;
-        double2 sum = make_double2(0.0, 0.0);
-        for (int w = 0; w < nw; ++w) sum = cadd(sum, sm[(size_t(w) * K + k) * R + r]);
-        a.partials[((size_t)blockIdx.x * K + k) * R + r] = sum;
-    }
-}
-
 // Sums partials[nb][KR] in a fixed order into out[KR] (one block).
 __global__ void finish_sum_kernel(const double2 *__restrict__ partials, int nb, int KR, double2 *out)
 {
@@ -1296,7 +638,7 @@ cudaError_t allow_dynamic_smem(const void *kern, int device)
 // `smem` dynamic bytes (+ static and reserved bytes) need, so that the rest
 // of the SM's 256 KB stays L1, which catches partner rows re-read by the
 // terms of one partner tile.
-static cudaError_t set_carveout(const void *kern, int device, size_t smem, int blocks)
+cudaError_t set_carveout(const void *kern, int device, size_t smem, int blocks)
 {
     static std::mutex mu;
     static std::vector<std::pair<std::pair<const void *, int>, int>> last;
@@ -1315,7 +657,7 @@ static cudaError_t set_carveout(const void *kern, int device, size_t smem, int b
 
 // Persistent grid of the tiled kernels: all resident blocks, which sweep
 // consecutive tiles, so partner tiles on the fast outer bits are found in L2.
-static int tile_grid(const pned_model *m, int nblocks)
+int tile_grid(const pned_model *m, int nblocks)
 {
     const int per_sm = m->tile_stage == 2 ? 1 : m->tile_bps;
     return std::max(1, std::min(nblocks, per_sm * m->nsm));
@@ -1341,67 +683,8 @@ static cudaError_t launch_tile_j(const pned_model *m, const HvArgs &a, int nbloc
 }
 
 template <bool RC, bool RD, int K>
-static cudaError_t launch_tile_stage(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
-{
-    auto kern = hv_tile_stage_kernel<RC, RD, K>;
-    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
-    const size_t smem = sizeof(double2) * (size_t(3) * kThreads * 8 + std::max(1, m->ntab));
-    if (e == cudaSuccess && m->carveout) e = set_carveout(reinterpret_cast<const void *>(kern), m->device, smem, 2);
-    if (e != cudaSuccess) return e;
-    const int grid = tile_grid(m, nblocks);
-    HvArgs b = a;
-    for (size_t p = 0; p < m->tprogs.size(); ++p) {
-        b.partials = a.partials + size_t(p) * grid * K * a.R;
-        kern<<<grid, kThreads, smem, st>>>(*m->tprogs[p], b);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
-
-// Dynamic shared memory of the bulk-copy kernel: the ring of stages, the
-// table and the head (above the 200 KB the other kernels are allowed).
-static size_t bulk_smem_bytes(int nst, int ntab)
-{
-    return size_t(kBulkHead) + sizeof(double2) * (size_t(nst) * kBulkTile + std::max(1, ntab));
-}
-
-static cudaError_t bulk_smem_attr(const void *kern, int device, size_t smem)
-{
-    static std::mutex mu;
-    static std::vector<std::pair<std::pair<const void *, int>, size_t>> done;
-    std::lock_guard<std::mutex> lock(mu);
-    for (auto &d : done)
-        if (d.first.first == kern && d.first.second == device && d.second >= smem) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e == cudaSuccess) done.push_back({{kern, device}, smem});
-    return e;
-}
-
-template <bool RC, bool RD, int K>
-static cudaError_t launch_tile_bulk(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
-{
-    auto kern = hv_tile_bulk_kernel<kBulkConsumerWarps, RC, RD, K>;
-    const size_t smem = bulk_smem_bytes(m->bulk_stages, m->ntab);
-    cudaError_t e = bulk_smem_attr(reinterpret_cast<const void *>(kern), m->device, smem);
-    if (e != cudaSuccess) return e;
-    const int grid = tile_grid(m, nblocks);
-    HvArgs b = a;
-    for (size_t p = 0; p < m->tprogs.size(); ++p) {
-        b.partials = a.partials + size_t(p) * grid * K * a.R;
-        kern<<<grid, 32 * (kBulkConsumerWarps + 1), smem, st>>>(*m->tprogs[p], b, m->bulk_stages);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
-
-template <bool RC, bool RD, int K>
 static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
-    if (m->tile_stage == 2) return launch_tile_bulk<RC, RD, K>(m, a, nblocks, st);
-    if (m->tile_stage == 1 && m->tile_jb == 3) return launch_tile_stage<RC, RD, K>(m, a, nblocks, st);
     switch (m->tile_jb) {
     case 1: return launch_tile_j<1, RC, RD, K>(m, a, nblocks, st);
     case 2: return launch_tile_j<2, RC, RD, K>(m, a, nblocks, st);
@@ -1481,60 +764,6 @@ static cudaError_t launch_hv_k(const pned_model *m, const HvArgs &a, int nblocks
 
 static int rtile_grid(const pned_model *m, int nblocks) { return std::max(1, std::min(nblocks, 2 * m->nsm)); }
 
-// Tile set of the mixed-radix tiled kernel for R (null: the flat kernel runs).
-static const pned_model::QTileSet *find_qtiles(const pned_model *m, int R)
-{
-    std::lock_guard<std::mutex> lock(const_cast<pned_model *>(m)->rtiles_mu);
-    auto it = m->qtiles.find(R);
-    if (it == m->qtiles.end() || it->second.progs.empty()) return nullptr;
-    return &it->second;
-}
-
-static int qtile_grid(const pned_model *m, const pned_model::QTileSet &qs, int nblocks)
-{
-    const int per_sm = qs.smem + 1024 <= 113 * 1024 ? 2 : 1;
-    return std::max(1, std::min(nblocks, per_sm * m->nsm));
-}
-
-template <int VPT, bool RC, bool RD, int K>
-static cudaError_t launch_qtile_t(const pned_model *m, const pned_model::QTileSet &qs, const HvArgs &a, int nblocks,
-                                  cudaStream_t st)
-{
-    auto kern = hv_qtile_kernel<VPT, RC, RD, K>;
-    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
-    if (e != cudaSuccess) return e;
-    const int grid = qtile_grid(m, qs, nblocks);
-    HvArgs b = a;
-    for (size_t p = 0; p < qs.progs.size(); ++p) {
-        b.partials = a.partials + size_t(p) * grid * K * a.R;
-        kern<<<grid, kThreads, qs.smem, st>>>(*qs.progs[p], b);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
-
-template <int VPT, int K>
-static cudaError_t launch_qtile_v(const pned_model *m, const pned_model::QTileSet &qs, const HvArgs &a, int nblocks,
-                                  cudaStream_t st)
-{
-    if (m->real_coef && m->real_diag) return launch_qtile_t<VPT, true, true, K>(m, qs, a, nblocks, st);
-    if (m->real_diag) return launch_qtile_t<VPT, false, true, K>(m, qs, a, nblocks, st);
-    return launch_qtile_t<VPT, false, false, K>(m, qs, a, nblocks, st);
-}
-
-template <int K>
-static cudaError_t launch_qtile(const pned_model *m, const pned_model::QTileSet &qs, const HvArgs &a, int nblocks,
-                                cudaStream_t st)
-{
-    switch (qs.vpt) {   // 1, 2 or 3 (even R runs two vectors a thread)
-    case 3: return launch_qtile_v<3, K>(m, qs, a, nblocks, st);
-    case 2: return launch_qtile_v<2, K>(m, qs, a, nblocks, st);
-    case 1: return launch_qtile_v<1, K>(m, qs, a, nblocks, st);
-    default: return cudaErrorInvalidValue;
-    }
-}
-
 // Tile set of the multi-vector kernel for R (null: the flat kernel runs).
 static const pned_model::TileSet *find_rtiles(const pned_model *m, int R)
 {
@@ -1596,6 +825,7 @@ int hv_partial_blocks(const pned_model *m, int R, int nblocks)
 cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
     if (!m->tprogs.empty() && a.R == 1 && m->use_tile) {
+        if (tile_staged(m)) return launch_tile_staged(m, a, nblocks, st);
         if (a.K == 1) return launch_tile<1>(m, a, nblocks, st);
         if (a.K == 4) return launch_tile<4>(m, a, nblocks, st);
     }
@@ -1604,10 +834,7 @@ cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStr
         if (a.K == 4) return launch_rv<4>(m, *ts, a, nblocks, st);
     }
     if (a.slot_tables) return cudaErrorInvalidValue;
-    if (const pned_model::QTileSet *qs = find_qtiles(m, a.R)) {
-        if (a.K == 1) return launch_qtile<1>(m, *qs, a, nblocks, st);
-        if (a.K == 4) return launch_qtile<4>(m, *qs, a, nblocks, st);
-    }
+    if (const pned_model::QTileSet *qs = find_qtiles(m, a.R)) return launch_qtile(m, *qs, a, nblocks, st);
     switch (a.K) {
     case 1: return launch_hv_k<1>(m, a, nblocks, st);
     case 4: return launch_hv_k<4>(m, a, nblocks, st);
@@ -1802,68 +1029,6 @@ bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan 
     return true;
 }
 
-// Tiled mixed-radix passes for R vectors (q > 2, full basis, n >= 8): the
-// largest tile of q^k states whose [nt][R] values, tables and index arrays
-// fit 100 KB of shared memory (two blocks per SM), k <= n - 2.
-bool ensure_qtiles(pned_model *m, int R)
-{
-    const HostProgram &hp = m->hp;
-    if (hp.q <= 2 || hp.sector || hp.n < 8 || pick_vpt(R) == 0) return false;
-    std::lock_guard<std::mutex> lock(m->rtiles_mu);
-    if (m->qtiles.count(R)) return !m->qtiles[R].progs.empty();
-    pned_model::QTileSet &qs = m->qtiles[R];
-    // the C tile, the pass table, 32-bit offsets and digits
-    auto smem_of = [&](int k) {
-        int64_t nt = 1;
-        for (int i = 0; i < k; ++i) nt *= hp.q;
-        return size_t(nt) * (sizeof(double2) * R + 8) + sizeof(double2) * kQTileMaxTab + 64;
-    };
-    int64_t states = 1;
-    for (int i = 0; i < hp.n; ++i) states *= hp.q;
-    // digits are packed 2 bits each; state indices and tile offsets are 32-bit
-    if (hp.q > 4 || states >= (int64_t(1) << 32)) return false;
-    int k = 2;
-    while (k + 1 <= std::min(hp.n - 2, kQTileMaxSites) && smem_of(k + 1) <= 110 * 1024) ++k;
-    if (smem_of(k) > 110 * 1024) return false;
-    std::vector<QTilePass> passes;
-    // one vector: 16-byte states; keep site 0 in every tile for 3-state runs
-    if (plan_qtiles(hp, k, R == 1 ? 1 : 0, passes) != PNED_OK) return false;
-    int64_t pw[64];
-    pw[0] = 1;
-    for (int i = 1; i <= hp.n; ++i) pw[i] = pw[i - 1] * hp.q;
-    for (size_t p = 0; p < passes.size(); ++p) {
-        const QTilePass &ps = passes[p];
-        if (ps.terms.size() > size_t(kMaxTerms) || ps.outer.size() > 32) { qs.progs.clear(); return false; }
-        std::unique_ptr<QTileProgram> T(new QTileProgram());
-        T->q = hp.q;
-        T->k = int(ps.sites.size());
-        T->nt = int(pw[T->k]);
-        T->nouter = int(ps.outer.size());
-        T->nterms = int(ps.terms.size());
-        T->first = p == 0;
-        T->last = p + 1 == passes.size();
-        T->ntiles = pw[hp.n] / pw[T->k];
-        for (int i = 0; i < T->k; ++i) T->spow[i] = uint32_t(pw[ps.sites[i]]);
-        for (int i = 0; i < T->nouter; ++i) T->opow[i] = uint32_t(pw[ps.outer[i]]);
-        // the pass's own coefficient tables, q^2 entries a term
-        const int Q = hp.q * hp.q;
-        if (ps.terms.size() * size_t(Q) > size_t(kQTileMaxTab)) { qs.progs.clear(); return false; }
-        T->ntab = int(ps.terms.size()) * Q;
-        for (size_t t = 0; t < ps.terms.size(); ++t) {
-            T->t[t] = ps.terms[t];
-            T->t[t].tab = uint16_t(t * Q);
-            for (int e = 0; e < Q; ++e) {
-                const cd z = hp.table[ps.terms[t].tab + e];
-                T->tab[t * Q + e] = make_double2(z.real(), z.imag());
-            }
-        }
-        qs.progs.push_back(std::move(T));
-    }
-    // two vectors a thread where R is even (the K = 4 sums of four would spill)
-    qs.vpt = (R % 2 == 0 && R % 3 != 0) ? 2 : pick_vpt(R);
-    qs.smem = smem_of(k);
-    return true;
-}
 
 }  // namespace pned
 

@@ -106,6 +106,26 @@ struct pned_ctx {
 
 namespace pned {
 
+// cp.async (Ampere-style asynchronous global -> shared copies, 16 bytes a thread).
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Bulk-copy staging of the single-vector tile kernel: tiles of 2^kBulkJB
+// states a thread, up to kBulkMaxStages ring stages.
+constexpr int kBulkJB = 3;
+constexpr int kBulkTile = kThreads << kBulkJB;   // 2048 states, 32 KB
+constexpr int kBulkMaxStages = 8;
+constexpr int kBulkHead = 256;                   // bytes before the ring: mbarriers and bookkeeping
+constexpr int kBulkMinRunBits = 3;               // copies of at least 8 states (128 B)
+
 int cuda_fail(cudaError_t e, const char *what);
 int ctx_alloc_buffer(pned_ctx *c, int k);
 int stage_in(pned_ctx *c, const pned_c128 *src, int flags, int k, const double2 **dev);
@@ -130,6 +150,21 @@ bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan 
 // Shared memory of the tiled multi-vector kernel for R vectors.
 size_t rtile_smem(const pned_model *m, int R, bool slot_tables);
 bool ensure_qtiles(pned_model *m, int R);
+// Tile set of the mixed-radix tiled kernel for R (null: the flat kernel runs).
+const pned_model::QTileSet *find_qtiles(const pned_model *m, int R);
+// Resident-block grid of the mixed-radix tiled kernel.
+int qtile_grid(const pned_model *m, const pned_model::QTileSet &qs, int nblocks);
+// All passes of the mixed-radix tiled kernel for a.R vectors and a.K sums.
+cudaError_t launch_qtile(const pned_model *m, const pned_model::QTileSet &qs, const HvArgs &a, int nblocks,
+                         cudaStream_t st);
+// Persistent grid of the single-vector tiled kernels (all resident blocks).
+int tile_grid(const pned_model *m, int nblocks);
+// Sets a kernel's shared-memory carveout to what `blocks` blocks of `smem` bytes need.
+cudaError_t set_carveout(const void *kern, int device, size_t smem, int blocks);
+// True when the plan runs a staged variant of the single-vector tile kernel.
+inline bool tile_staged(const pned_model *m) { return m->tile_stage == 2 || (m->tile_stage == 1 && m->tile_jb == 3); }
+// All passes of the staged single-vector tile kernel (cp.async or bulk copies).
+cudaError_t launch_tile_staged(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
 // Number of partial-sum blocks launch_hv writes for this model, R and grid.
 int hv_partial_blocks(const pned_model *m, int R, int nblocks);
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);
