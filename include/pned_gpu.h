@@ -137,8 +137,9 @@ int pned_model_plan(const pned_model *m, int R, int *tile_passes, int *partner_t
  * global bits kept in the tile rows (8 for R = 1 by default: rows are runs
  * of 256 consecutive states; fewer lets the planner pick tile bits that
  * leave fewer partner tiles); window_bits: outer bits whose partner tiles a
- * pass expects in L2; max_passes: 1..4; j_bits (R = 1 only): 1..3, states
- * per thread 2^j_bits (fewer registers, more resident blocks).  Re-plans at
+ * pass expects in L2; max_passes: 1..4; j_bits (R = 1 only): 1..4, states
+ * per thread 2^j_bits (fewer: fewer registers, more resident blocks; 4: tiles
+ * of 4096 states, more flips inside the tile).  Re-plans at
  * once (plan NULL: defaults); call it between launches, not while other
  * threads launch on the model.  Used by the autotuner (pned_b200.tune).
  */

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kThreads, BPS)
     hv_tile_kernel(const __grid_constant__ TileProgram prog, const HvArgs a)
 {
     constexpr int SPT = 1 << JB;
+    constexpr int CH = SPT < 8 ? SPT : 8;   // rows loaded together (16 rows: two chunks, no spills)
     constexpr int TILE = kThreads * SPT;
     extern __shared__ double2 smem[];
     double2 *s_v = smem;
@@ -163,25 +164,27 @@ __global__ void __launch_bounds__(kThreads, BPS)
         uint32_t base = rowbase;
         for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
         double2 acc[SPT];
-        {
-            double2 v[SPT];
 #pragma unroll
-            for (int j = 0; j < SPT; ++j) v[j] = __ldg(a.C + (base | prog.jexp[j]));
-            __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+        for (int j0 = 0; j0 < SPT; j0 += CH) {
+            double2 v[CH];
 #pragma unroll
-            for (int j = 0; j < SPT; ++j) s_v[tid + kThreads * j] = v[j];
+            for (int jj = 0; jj < CH; ++jj) v[jj] = __ldg(a.C + (base | prog.jexp[j0 + jj]));
+            if (j0 == 0) __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
 #pragma unroll
-            for (int j = 0; j < SPT; ++j) {
+            for (int jj = 0; jj < CH; ++jj) s_v[tid + kThreads * (j0 + jj)] = v[jj];
+#pragma unroll
+            for (int jj = 0; jj < CH; ++jj) {
+                const int j = j0 + jj;
                 const uint32_t sj = base | prog.jexp[j];
                 if (!prog.first) {
                     acc[j] = make_double2(0.0, 0.0);
                 } else if (RD) {
                     const double dd = __ldcs(static_cast<const double *>(a.diag) + sj) - shift;
-                    acc[j] = cscale(dd, v[j]);
+                    acc[j] = cscale(dd, v[jj]);
                 } else {
                     double2 dd = __ldcs(static_cast<const double2 *>(a.diag) + sj);
                     dd.x -= shift;
-                    acc[j] = cmul(dd, v[j]);
+                    acc[j] = cmul(dd, v[jj]);
                 }
             }
         }
@@ -216,29 +219,34 @@ __global__ void __launch_bounds__(kThreads, BPS)
         // flip masks leaving the tile: partners through L1/L2
         for (int t = prog.nin; t < prog.nterms; ++t) {
             const TileTerm T = prog.t[t];
-            double2 w0[SPT];
             // (base | jexp) ^ mask == (base ^ mask) ^ jexp: base has no j bits
             const uint32_t pbx = base ^ T.mask;
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + (pbx ^ prog.jexp[j]));
             uint32_t ib = 0;
 #pragma unroll
             for (int d = 0; d < kMaxDeps; ++d)
                 if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
-            if (!T.hasj) {
-                const double2 c = s_tab[T.tab + ib];
 #pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
-                    else acc[j] = cfma(c, w0[j], acc[j]);
+            for (int j0 = 0; j0 < SPT; j0 += CH) {   // CH partner loads in flight
+                double2 w0[CH];
+#pragma unroll
+                for (int jj = 0; jj < CH; ++jj) w0[jj] = __ldg(a.C + (pbx ^ prog.jexp[j0 + jj]));
+                if (!T.hasj) {   // one coefficient for all rows of the thread
+                    const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                    for (int jj = 0; jj < CH; ++jj) {
+                        const int j = j0 + jj;
+                        if (RC) { acc[j].x = fma(c.x, w0[jj].x, acc[j].x); acc[j].y = fma(c.x, w0[jj].y, acc[j].y); }
+                        else acc[j] = cfma(c, w0[jj], acc[j]);
+                    }
+                    continue;
                 }
-                continue;
-            }
 #pragma unroll
-            for (int j = 0; j < SPT; ++j) {
-                const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
-                if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
-                else acc[j] = cfma(c, w0[j], acc[j]);
+                for (int jj = 0; jj < CH; ++jj) {
+                    const int j = j0 + jj;
+                    const double2 c = s_tab[T.tab + (ib | uint32_t((T.jtab >> (4 * j)) & 15u))];
+                    if (RC) { acc[j].x = fma(c.x, w0[jj].x, acc[j].x); acc[j].y = fma(c.x, w0[jj].y, acc[j].y); }
+                    else acc[j] = cfma(c, w0[jj], acc[j]);
+                }
             }
         }
 #pragma unroll
@@ -691,6 +699,7 @@ static cudaError_t launch_tile_t(const pned_model *m, const HvArgs &a, int nbloc
     case 3:   // 8 rows per thread: two resident blocks (121 registers) or three (85, some spills)
         if (m->tile_bps == 3) return launch_tile_j<3, RC, RD, K, 3>(m, a, nblocks, st);
         return launch_tile_j<3, RC, RD, K>(m, a, nblocks, st);
+    case 4: return launch_tile_j<4, RC, RD, K>(m, a, nblocks, st);
     default: return cudaErrorInvalidValue;
     }
 }

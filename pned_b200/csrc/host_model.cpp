@@ -608,7 +608,7 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
                         if ((j >> k) & 1) bits |= 1u << d;
                     }
                 }
-                q.jtab |= bits << (4 * j);
+                q.jtab |= uint64_t(bits) << (4 * j);
             }
             // in-tile terms: the local xor inside the tile; out-of-tile terms: the global xor
             if ((t.xmask & ~tilemask) == 0) {

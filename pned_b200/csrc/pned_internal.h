@@ -52,7 +52,7 @@ struct RadixTerm {
 struct TileTerm {
     uint32_t mask;   // in-tile: local xor (bits 0..7 thread part, bits 8.. j part); out-of-tile: global xor
     uint32_t pos4;   // dependency bit positions (global), 8 bits each
-    uint32_t jtab;   // coefficient-index bits contributed by j (4 bits per j)
+    uint64_t jtab;   // coefficient-index bits contributed by j (4 bits per j)
     uint16_t tab;    // coefficient table offset
     uint8_t nb;      // number of dependency bits
     uint8_t hasj;    // 1 if a dependency bit is a j-bit
@@ -68,7 +68,7 @@ struct QTileTerm {
     uint8_t ls1, ls2;   // local digit positions of the bond's sites
     uint16_t tab;    // coefficient table offset (q^2 entries by pair state)
 };
-constexpr int kTileMaxJB = 3;
+constexpr int kTileMaxJB = 4;
 constexpr int kTileWindowBits = 10;   // outer bits whose partner tiles stay in L2 during a sweep
 constexpr int kTileMaxPasses = 4;
 constexpr int kTileMaxGroups = 64;    // partner tiles per pass
@@ -105,7 +105,7 @@ struct HostProgram {
         int tbits = 8;                   // row bits of a tile (state rows of the thread index)
         std::vector<int> rowpos;         // global bit of row bit k (k < tbits)
         int jb = 0;
-        int jpos[kTileMaxJB] = {0, 0, 0};
+        int jpos[kTileMaxJB] = {};
         std::vector<int> outer;          // outer bit positions, fastest first
         int nin = 0;                     // in-tile terms first, then out-of-tile terms grouped by partner tile
         std::vector<TileTerm> tterms;

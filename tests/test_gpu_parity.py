@@ -390,7 +390,8 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
 
 @pytest.mark.parametrize("plan", [(8, 10, 4, 3, 1, 1), (5, 10, 2, 3, 1, 1), (3, 8, 1, 3, 1, 1), (5, 12, 2, 2, 1, 0),
                                   (5, 12, 2, 1, 0, 0), (8, 10, 4, 3, 1, 2), (5, 10, 2, 3, 1, 2), (3, 8, 1, 3, 1, 2),
-                                  (5, 6, 3, 3, 1, 2), (8, 8, 2, 3, 1, 0, 3), (5, 10, 2, 3, 1, 0, 3)])
+                                  (5, 6, 3, 3, 1, 2), (8, 8, 2, 3, 1, 0, 3), (5, 10, 2, 3, 1, 0, 3),
+                                  (5, 8, 2, 4, 1, 0), (8, 10, 4, 4, 1, 0), (3, 6, 1, 4, 0, 0)])
 def test_tile_plans_agree_with_oracle(plan):
     """Every tile plan the autotuner may pick (rows kept, window, passes, rows per
     thread, carveout, staged or bulk-streamed partner tiles) gives the oracle's
@@ -443,6 +444,34 @@ def test_bulk_streamed_tiles_match_gathered_tiles(plan):
     assert np.array_equal(out[0][0], out[2][0])
     assert abs(out[0][1][0] - out[2][1][0]) <= 1e-12 * abs(out[0][1][0])
     assert rel(out[0][2], out[2][2]) <= 1e-12 and rel(out[0][3], out[2][3]) <= 1e-12
+    gm.set_plan(1)
+
+
+@pytest.mark.parametrize("plan", [(5, 11, 2, 4), (8, 10, 3, 4)])
+def test_sixteen_row_tiles_match_eight_row_tiles(plan):
+    """N = 24 (4096 tiles of 4096 states): tiles of 16 rows a thread (two row
+    chunks per gather) give the H.v of the default 8-row tiles to 1e-12 and the
+    same Lanczos coefficients."""
+    cl = honeycomb(3, 4)
+    gm, _ = models(cl, 2, 0, KHGH, FIELD)
+    rng = np.random.default_rng(31)
+    v1 = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
+    v0 = 0.1 * (rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim))
+    v = O.gaussian(3, gm.dim)
+    v /= np.linalg.norm(v)
+    out = []
+    for pl in ((5, 12, 2, 3), plan):
+        got = gm.set_plan(1, *pl)
+        assert got["tile_states"] == 256 << pl[3]
+        ctx = P.Context(gm, R=1)
+        w = v0.copy()
+        pr = ctx.p_mltply_v3(v1, w, 0.0625)
+        run = ctx.lanczos(v, 20)
+        out.append((w, pr[0], run["alpha"][:, 0], run["beta"][:, 0]))
+        ctx.close()
+    assert rel(out[1][0], out[0][0]) <= 1e-12
+    assert abs(out[1][1] - out[0][1]) <= 1e-12 * abs(out[0][1])
+    assert rel(out[1][2], out[0][2]) <= 1e-10 and rel(out[1][3], out[0][3]) <= 1e-10
     gm.set_plan(1)
 
 
