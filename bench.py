@@ -518,9 +518,33 @@ def run_sector(args, rank, world, local_rank):
         hv_ms, step_ms = ctx.session_profile(args.profile_steps)
         res = ctx.session_read()
         ctx.session_end()
+        # the segment kernel against the flat gather on one vector: W bit for bit, H.v time
+        seg = {"active": m.sector_segments()}
+        if seg["active"]:
+            x = torch.empty(D, dtype=torch.complex128, device=dev)
+            ctx.fill_gaussian(SEED + 1, x)
+            ws = {}
+            for on in (True, False):
+                m.sector_segments(on)
+                w = torch.zeros_like(x)
+                ctx.p_mltply_v3(x, w)
+                ctx.synchronize()
+                ws[on] = w.clone()
+                t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                t0.record(st)
+                for _ in range(3):
+                    ctx.p_mltply_v3(x, w)
+                t1.record(st)
+                torch.cuda.synchronize()
+                seg["hv_ms" if on else "flat_hv_ms"] = t0.elapsed_time(t1) / 3
+            m.sector_segments(True)
+            seg["w_bit_identical"] = bool(torch.equal(ws[True], ws[False]))
+            del x, w, ws
         ctx.close()
         m.close()
     peak, peak_kind = load_peaks()
+    kernel = "hv_sector_kernel (segments, K=1)" if seg["active"] else "hv_xor_kernel (sector, K=1)"
     # per sector state: C 16 + P 16 + W 16 + real diagonal 8 = 56 B (as the full basis), plus the
     # state list entry (8 B); the Lin tables (2 x 2^ceil(n/2) entries) stay in L2
     bytes_hv = 64 * D
@@ -531,9 +555,10 @@ def run_sector(args, rank, world, local_rank):
         "config": {"workload": f"S=1/2 Heisenberg (J=1) honeycomb N={n} ({cl.L1}x{cl.L2}), Sz=0 sector "
                                f"D={D} (mk_list12 order), complex128, 1 Lanczos chain", "dim": D, "R": 1},
         "e0_per_site": float(P.bisec(res["alpha"][:, 0], res["beta"][:, 0], res["alpha"].shape[0], 1)[0]) / n,
-        "roofline": {"bound": "hbm", "kernel": "hv_xor_kernel (sector, K=1)", "achieved": bytes_hv / (hv_ms * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": bytes_hv / (hv_ms * 1e-3) / 1e9,
                      "peak": peak, "unit": "GB/s", "frac": bytes_hv / (hv_ms * 1e-3) / 1e9 / peak,
                      "peak_kind": peak_kind, "hv_ms": hv_ms, "algorithmic_bytes_per_hv": bytes_hv},
+        "segments": seg,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

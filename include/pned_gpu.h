@@ -163,6 +163,16 @@ int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
  * 1 cp.async, 2 bulk copies) and, for 2, the number of ring stages.
  */
 int pned_model_tile_staging(const pned_model *m, int *mode, int *ring_stages);
+/*
+ * Measurement hook (no counterpart in the reference): S = 1/2 Sz-sector models
+ * run the one-vector H.v per segment (the contiguous states sharing their high
+ * half; one block per segment, partner ranks from one table read, high-half
+ * flips rank for rank) when the largest segment has at least 256 states;
+ * enable = 0 selects the flat gather with two Lin-table reads per term
+ * instead, 1 the segment kernel again, -1 leaves the setting.  *active (may be
+ * NULL) = 1 when the segment kernel runs.  Both give the same W bit for bit.
+ */
+int pned_model_sector_segments(pned_model *m, int enable, int *active);
 
 /* ------------------------------------------------------------------------ */
 /* context: device vectors for R interleaved vectors                         */

@@ -313,6 +313,13 @@ class Model:
             out["staging"], out["ring_stages"] = md.value, ns.value
         return out
 
+    def sector_segments(self, enable: bool | None = None) -> bool:
+        """S = 1/2 Sz sector: selects the per-segment one-vector H.v (True) or the
+        flat gather (False); None leaves it.  Returns whether the segment kernel runs."""
+        act = C.c_int(0)
+        check(lib().pned_model_sector_segments(self._h, -1 if enable is None else int(bool(enable)), C.byref(act)))
+        return bool(act.value)
+
     def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
                  j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1):
         """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""

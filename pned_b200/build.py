@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpned_gpu.so")
-SOURCES = ["host_model.cpp", "host_io.cpp", "device.cu", "hv_staged.cu", "hv_qtile.cu", "krylov.cu", "slots.cu"]
+SOURCES = ["host_model.cpp", "host_io.cpp", "device.cu", "hv_staged.cu", "hv_qtile.cu", "hv_sector.cu", "krylov.cu", "slots.cu"]
 HEADERS = ["pned_internal.h", "kernels.cuh", "device.cuh", os.path.join("..", "..", "include", "pned_gpu.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

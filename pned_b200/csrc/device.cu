@@ -737,23 +737,28 @@ static cudaError_t launch_hv_t(const pned_model *m, const HvArgs &a, int nblocks
     return cudaGetLastError();
 }
 
+// The call's arguments with the model's sector tables (list1, Lin tables).
+static HvArgs sector_args(const pned_model *m, const HvArgs &a)
+{
+    HvArgs b = a;
+    b.list1 = m->d_list1;
+    b.lin_lo = m->d_lin_lo;
+    b.lin_hi = m->d_lin_hi;
+    b.lin_mod = m->lin_mod;
+    b.lin_pow2 = 0;
+    if ((m->lin_mod & (m->lin_mod - 1)) == 0) {
+        int sh = 0;
+        while ((int64_t(1) << sh) < m->lin_mod) ++sh;
+        b.lin_pow2 = sh + 1;
+    }
+    return b;
+}
+
 template <int VPT, int K>
 static cudaError_t launch_hv_v(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
-    if (m->hp.sector) {   // Sz sector: complex coefficients, real diagonal
-        HvArgs b = a;
-        b.list1 = m->d_list1;
-        b.lin_lo = m->d_lin_lo;
-        b.lin_hi = m->d_lin_hi;
-        b.lin_mod = m->lin_mod;
-        b.lin_pow2 = 0;
-        if ((m->lin_mod & (m->lin_mod - 1)) == 0) {
-            int sh = 0;
-            while ((int64_t(1) << sh) < m->lin_mod) ++sh;
-            b.lin_pow2 = sh + 1;
-        }
-        return launch_hv_t<VPT, false, true, K, true>(m, b, nblocks, st);
-    }
+    if (m->hp.sector)   // Sz sector: complex coefficients, real diagonal
+        return launch_hv_t<VPT, false, true, K, true>(m, sector_args(m, a), nblocks, st);
     if (m->real_coef && m->real_diag) return launch_hv_t<VPT, true, true, K>(m, a, nblocks, st);
     if (m->real_diag) return launch_hv_t<VPT, false, true, K>(m, a, nblocks, st);
     return launch_hv_t<VPT, false, false, K>(m, a, nblocks, st);
@@ -828,6 +833,7 @@ int hv_partial_blocks(const pned_model *m, int R, int nblocks)
     if (!m->tprogs.empty() && R == 1 && m->use_tile) return int(m->tprogs.size()) * tile_grid(m, nblocks);
     if (const pned_model::TileSet *ts = find_rtiles(m, R)) return int(ts->progs.size()) * rtile_grid(m, nblocks);
     if (const pned_model::QTileSet *qs = find_qtiles(m, R)) return int(qs->progs.size()) * qtile_grid(m, *qs, nblocks);
+    if (R == 1 && sector_segments_on(m)) return sector_grid(m, nblocks);
     return nblocks;
 }
 
@@ -844,6 +850,7 @@ cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStr
     }
     if (a.slot_tables) return cudaErrorInvalidValue;
     if (const pned_model::QTileSet *qs = find_qtiles(m, a.R)) return launch_qtile(m, *qs, a, nblocks, st);
+    if (a.R == 1 && sector_segments_on(m)) return launch_sector(m, sector_args(m, a), nblocks, st);
     switch (a.K) {
     case 1: return launch_hv_k<1>(m, a, nblocks, st);
     case 4: return launch_hv_k<4>(m, a, nblocks, st);
@@ -1098,6 +1105,8 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
             cudaFree(m->d_list1); cudaFree(m->d_lin_lo); cudaFree(m->d_lin_hi);
             return cuda_fail(e, "pned_model_create: sector tables");
         }
+        e = build_sector_segments(m.get());
+        if (e != cudaSuccess) return cuda_fail(e, "pned_model_create: sector segments");
     } else {
         build_tile_programs(m.get());
     }
@@ -1149,6 +1158,9 @@ extern "C" int pned_model_destroy(pned_model *m)
     cudaFree(m->d_list1);
     cudaFree(m->d_lin_lo);
     cudaFree(m->d_lin_hi);
+    cudaFree(m->d_seg_start);
+    cudaFree(m->d_seg_hi);
+    cudaFree(m->d_rank_lo);
     delete m;
     return PNED_OK;
 }
@@ -1159,6 +1171,14 @@ extern "C" int pned_model_tile_staging(const pned_model *m, int *mode, int *ring
     const int md = m->use_tile ? m->tile_stage : 0;
     if (mode) *mode = md;
     if (ring_stages) *ring_stages = md == 2 ? m->bulk_stages : 0;
+    return PNED_OK;
+}
+
+extern "C" int pned_model_sector_segments(pned_model *m, int enable, int *active)
+{
+    if (!m) return fail(PNED_EINVAL, "pned_model_sector_segments: null model");
+    if (enable >= 0) m->seg_enabled = enable != 0;
+    if (active) *active = sector_segments_on(m) ? 1 : 0;
     return PNED_OK;
 }
 

@@ -49,6 +49,13 @@ struct pned_model {
     // Sz sector: index -> state and the Lin tables
     int64_t *d_list1 = nullptr, *d_lin_lo = nullptr, *d_lin_hi = nullptr;
     int64_t lin_mod = 0;
+    // S = 1/2 sector segments (states sharing their high half): nseg starts + the
+    // dimension, and the high halves; nseg == 0 when the flat gather is used
+    int64_t *d_seg_start = nullptr;
+    int32_t *d_seg_hi = nullptr;
+    int32_t *d_rank_lo = nullptr;   // rank of each low half in its popcount class (lin_lo - 1)
+    int nseg = 0, seg_max = 0, seg_bps = 1;   // segments, the largest, resident blocks per SM
+    bool seg_enabled = true;   // pned_model_sector_segments switch
 };
 
 namespace pned {
@@ -161,6 +168,13 @@ cudaError_t launch_qtile(const pned_model *m, const pned_model::QTileSet &qs, co
 int tile_grid(const pned_model *m, int nblocks);
 // Sets a kernel's shared-memory carveout to what `blocks` blocks of `smem` bytes need.
 cudaError_t set_carveout(const void *kern, int device, size_t smem, int blocks);
+// Segment table of an S = 1/2 sector model (left empty where the flat gather is used).
+cudaError_t build_sector_segments(pned_model *m);
+inline bool sector_segments_on(const pned_model *m) { return m->nseg > 0 && m->seg_enabled; }
+// Resident-block grid of the sector segment kernel.
+int sector_grid(const pned_model *m, int nblocks);
+// Sector H.v for one vector over segments (a.* Lin fields set).
+cudaError_t launch_sector(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
 // True when the plan runs a staged variant of the single-vector tile kernel.
 inline bool tile_staged(const pned_model *m) { return m->tile_stage == 2 || (m->tile_stage == 1 && m->tile_jb == 3); }
 // All passes of the staged single-vector tile kernel (cp.async or bulk copies).

@@ -387,8 +387,14 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
             const Bond &b = bonds[bi];
             for (int f = 1; f < 4; ++f) {
                 bool any = false;
-                for (int st = 0; st < 4; ++st)
-                    if (elem(b.t, st ^ f, st) != cd(0, 0)) any = true;
+                for (int st = 0; st < 4; ++st) {
+                    if (elem(b.t, st ^ f, st) == cd(0, 0)) continue;
+                    any = true;
+                    // the sector's Lin lookup is only defined for partners inside it
+                    if (P.sector && __builtin_popcount(unsigned(st ^ f)) != __builtin_popcount(unsigned(st)))
+                        return fail(PNED_EINVAL, "pned_model_create: a nonzero element changes Sz, "
+                                                 "which parity_type 0 (the Sz sector basis) does not allow");
+                }
                 if (!any) continue;
                 uint32_t mask = ((f & 1) ? (1u << b.s1) : 0u) | ((f & 2) ? (1u << b.s2) : 0u);
                 if (!groups.count(mask)) order.push_back(mask);
@@ -456,6 +462,9 @@ int compile_program(const pned_model_desc *d, HostProgram &P)
                         cd v = elem(b.t, e1 + q * e2, st);
                         if (v != cd(0, 0)) { any = true; tab[st] = v; }
                     }
+                    if (any && P.sector && d1 + d2 != 0)
+                        return fail(PNED_EINVAL, "pned_model_create: a nonzero element changes Sz, "
+                                                 "which parity_type 0 (the Sz sector basis) does not allow");
                     if (!any) continue;
                     RadixTerm t{};
                     t.offset = d1 * pw[b.s1] + d2 * pw[b.s2];

@@ -212,6 +212,18 @@ def test_dsf_res_text_block(tmp_path):
     assert lines[3:7] == [" "] * 4 and lines[7].startswith("#")
 
 
+def test_sector_model_must_conserve_sz():
+    """parity_type 0 (Sz sector basis, Lin-table partners) is refused for a model
+    whose nonzero elements change Sz; the refusal comes before any device work."""
+    from pned_b200.lattice import honeycomb
+    cl = honeycomb(2, 2)
+    for q, tree in ((2, 0), (3, 1)):
+        X, skip, pt = P.build_xlocal(q, tree, CP.kitaev_heisenberg(0.3, -1.0))
+        assert pt != 0
+        with pytest.raises(P.PnedError, match="changes Sz"):
+            P.Model(cl.n, q, tree, cl.ipair, cl.ibond_type, X, skip, 0)
+
+
 def test_rejects_bad_arguments():
     with pytest.raises(ValueError):
         P.build_xlocal(2, 0, np.zeros(5))

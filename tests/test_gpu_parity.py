@@ -496,6 +496,49 @@ def test_torch_tensors_written_just_before_the_call_are_ready():
     ctx.close()
 
 
+@pytest.mark.parametrize("L1,L2", [(3, 4), (4, 3)])
+def test_sector_segments_match_flat_gather(L1, L2):
+    """S = 1/2 Heisenberg N = 24, Sz = 0 (2,704,156 states, segments of up to 924
+    states): the per-segment H.v gives the flat gather's W bit for bit, the
+    oracle's H.v to 1e-12, and Lanczos coefficients equal to the flat path's to
+    the summation order of the block sums."""
+    cl = honeycomb(L1, L2)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(1.0, 0.0))
+    gm = P.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    assert gm.sector_segments() is True
+    rng = np.random.default_rng(13)
+    D = gm.dim
+    v1 = rng.standard_normal(D) + 1j * rng.standard_normal(D)
+    v0 = 0.2 * (rng.standard_normal(D) + 1j * rng.standard_normal(D))
+    v = O.gaussian(11, D)
+    v /= np.linalg.norm(v)
+    out = {}
+    for seg in (True, False):
+        assert gm.sector_segments(seg) is seg
+        ctx = P.Context(gm, R=1)
+        w = v0.copy()
+        pr = ctx.p_mltply_v3(v1, w, 0.0625)
+        run = ctx.lanczos(v, 20)
+        out[seg] = (w, pr[0], run["alpha"][:, 0], run["beta"][:, 0])
+        ctx.close()
+    gm.sector_segments(True)
+    assert np.array_equal(out[True][0], out[False][0])
+    assert abs(out[True][1] - out[False][1]) <= 1e-12 * abs(out[False][1])
+    assert rel(out[True][2], out[False][2]) <= 1e-12 and rel(out[True][3], out[False][3]) <= 1e-12
+    om = O.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    ref = v0.copy()
+    prr = om.p_mltply_v3(v1, ref, 0.0625)
+    assert rel(out[True][0], ref) <= 1e-12 and abs(out[True][1] - prr) <= 1e-12 * abs(prr)
+
+
+def test_sector_segments_only_where_they_fill_a_block():
+    """Segments shorter than one block (N = 12: at most 20 states) keep the flat gather."""
+    cl = honeycomb(3, 2)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(1.0, 0.0))
+    gm = P.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    assert gm.sector_segments() is False and gm.sector_segments(True) is False
+
+
 XY_CASES = [
     # (L1, L2, q, tree, ipm, R, sector): S^{ipm}_q start vectors and DSF chains
     (3, 2, 2, 0, 1, 2, True),
