@@ -1,9 +1,11 @@
 """Autotuner of the tiled H.v plan.
 
-The tiled kernels (single-vector and R-vector) take three plan parameters:
-how many low global bits the tile rows keep (runs of consecutive states, for
-coalescing), how many outer bits a pass expects to find in L2, and at most
-how many passes the flip masks are split into.  Which combination is fastest
+The tiled kernels (single-vector and R-vector) take three main plan
+parameters: how many low global bits the tile rows keep (runs of consecutive
+states, for coalescing), how many outer bits a pass expects to find in L2, and
+at most how many passes the flip masks are split into.  The single-vector
+kernel also takes the rows per thread (2^j_bits: 2048-state tiles at 3,
+4096-state tiles at 4) and the resident blocks per SM.  Which combination is fastest
 depends on the lattice, the vector count and the device, so the tuner times
 the H.V of the actual model over a small candidate set and keeps the
 fastest.  Results are cached in-process per (lattice, terms, R, device), and

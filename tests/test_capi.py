@@ -89,6 +89,43 @@ def test_mk_list12_matches_oracle(n, q):
     assert np.array_equal(lo[:len(olo)], olo) and np.array_equal(hi[:len(ohi)], ohi)
 
 
+@pytest.mark.parametrize("n,tot", [(12, 6), (15, 7), (16, 5), (22, 11)])
+def test_sector_segments_layout(n, tot):
+    """The layout the S = 1/2 segment H.v relies on: the sector states sharing a
+    high half form one contiguous segment, in ascending order, of C(ihf, tot -
+    popcount(hi)) states; a state's index is lin_hi[hi] + rank with rank =
+    lin_lo[lo] - 1; and for every Sz-conserving two-site flip the segment
+    formulas (high-half flips: same rank in segment hi ^ mh; low-half or cross
+    flips: rank of lo ^ ml) give the flat Lin index of the flipped state."""
+    l1, lo_t, hi_t = P.mk_list12(n, 2, 0, tot)
+    ihf = (n + 1) // 2
+    lo = l1 & ((1 << ihf) - 1)
+    hi = l1 >> ihf
+    idx = np.arange(len(l1))
+    assert np.all(np.diff(l1) > 0)
+    starts = np.flatnonzero(np.r_[True, np.diff(hi) != 0])
+    assert np.array_equal(hi[starts], np.unique(hi))
+    lens = np.diff(np.r_[starts, len(l1)])
+    pc = np.array([bin(int(h)).count("1") for h in hi[starts]])
+    assert np.array_equal(lens, [math.comb(ihf, tot - p) for p in pc])
+    assert np.array_equal(hi_t[hi[starts]], starts)
+    rank = lo_t[lo] - 1
+    assert np.array_equal(idx, hi_t[hi] + rank)
+    assert np.array_equal(rank, idx - np.repeat(starts, lens))
+    pos = {int(s): i for i, s in enumerate(l1)}
+    rng = np.random.default_rng(n)
+    for a, b in rng.integers(0, n, size=(40, 2)):
+        if a == b:
+            continue
+        m = (1 << int(a)) | (1 << int(b))
+        ml, mh = m & ((1 << ihf) - 1), m >> ihf
+        ok = ((l1 >> a) & 1) != ((l1 >> b) & 1)          # the flip keeps Sz
+        part = np.array([pos[int(s) ^ m] for s in l1[ok]])
+        r = np.where(ml == 0, rank[ok], lo_t[lo[ok] ^ ml] - 1)
+        base = hi_t[hi[ok] ^ mh]
+        assert np.array_equal(base + r, part)
+
+
 def test_errors_are_reported_not_fatal():
     with pytest.raises(P.PnedError):
         P.build_xlocal(3, 0, CP.model20(10.0))         # tree 0 needs q = 2
