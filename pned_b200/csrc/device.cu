@@ -1052,7 +1052,19 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
 {
     if (!desc || !out) return fail(PNED_EINVAL, "pned_model_create: null argument");
     *out = nullptr;
-    std::unique_ptr<pned_model> m(new pned_model());
+    // a failure part-way frees what was allocated on the device; one before any
+    // allocation (a refused model) makes no CUDA call
+    struct Destroy {
+        void operator()(pned_model *p) const
+        {
+            if (p->d_table || p->d_diag || p->d_list1 || p->d_lin_lo || p->d_lin_hi || p->d_seg_start ||
+                p->d_seg_hi || p->d_rank_lo)
+                pned_model_destroy(p);
+            else
+                delete p;
+        }
+    };
+    std::unique_ptr<pned_model, Destroy> m(new pned_model());
     int rc = compile_program(desc, m->hp);
     if (rc) return rc;
     cudaError_t e = cudaSetDevice(g_device);
@@ -1101,10 +1113,7 @@ extern "C" int pned_model_create(const pned_model_desc *desc, pned_model **out)
             e = cudaMemcpy(m->d_lin_lo, hp.lin_lo.data(), sizeof(int64_t) * hp.lin_lo.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
             e = cudaMemcpy(m->d_lin_hi, hp.lin_hi.data(), sizeof(int64_t) * hp.lin_hi.size(), cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            cudaFree(m->d_list1); cudaFree(m->d_lin_lo); cudaFree(m->d_lin_hi);
-            return cuda_fail(e, "pned_model_create: sector tables");
-        }
+        if (e != cudaSuccess) return cuda_fail(e, "pned_model_create: sector tables");
         e = build_sector_segments(m.get());
         if (e != cudaSuccess) return cuda_fail(e, "pned_model_create: sector segments");
     } else {
