@@ -158,6 +158,19 @@ typedef struct {
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 /*
+ * Test and measurement hook (no counterpart in the reference): the
+ * single-vector tile plan (S = 1/2 full basis) that pned_model_set_plan would
+ * build for this model, computed on the host without device work.  out[0..cap)
+ * receives int64 values, *len the full count: the number of flip terms X, X
+ * records (xmask, pos4, tab, nb), the number of passes, and per pass (tbits, jb,
+ * nouter, nterms, nin, ngroups), rowpos[tbits], jpos[jb], outer[nouter], nterms
+ * records (mask, pos4, jtab, tab, nb, hasj, lmask), gstart[ngroups + 1],
+ * gxor[ngroups].  In-tile terms (the first nin) carry the local xor (row bits
+ * 0..7, then the j bits), the others the global xor.
+ */
+int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_plan *plan, int64_t *out, int64_t cap,
+                          int64_t *len);
+/*
  * Measurement hook (no counterpart in the reference): the partner-tile
  * staging the single-vector plan actually runs (0 gathered through L1/L2,
  * 1 cp.async, 2 bulk copies) and, for 2, the number of ring stages.

@@ -288,6 +288,35 @@ class ModelInput:
         return cls(cluster.n, 2, tree, cluster.ipair, cluster.ibond_type, X, None, 1)
 
 
+def tile_plan_export(desc: "ModelInput", row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
+                     j_bits: int = -1) -> dict:
+    """The single-vector tile plan (S = 1/2 full basis) that Model.set_plan would
+    build, computed on the host (pned_tile_plan_export): the program's flip terms
+    and, per pass, the tile bits, outer order, terms and partner-tile groups."""
+    tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1)
+    n = C.c_int64(0)
+    check(lib().pned_tile_plan_export(C.byref(desc.c), C.byref(tp), None, 0, C.byref(n)))
+    buf = np.zeros(n.value, dtype=np.int64)
+    check(lib().pned_tile_plan_export(C.byref(desc.c), C.byref(tp), buf.ctypes.data_as(C.POINTER(C.c_int64)),
+                                      n.value, C.byref(n)))
+    it = iter(buf.tolist())
+    nx = next(it)
+    xterms = [dict(zip(("xmask", "pos4", "tab", "nb"), (next(it) for _ in range(4)))) for _ in range(nx)]
+    passes = []
+    for _ in range(next(it)):
+        tbits, jb, nout, nt, nin, ng = (next(it) for _ in range(6))
+        ps = dict(tbits=tbits, jb=jb, nin=nin)
+        ps["rowpos"] = [next(it) for _ in range(tbits)]
+        ps["jpos"] = [next(it) for _ in range(jb)]
+        ps["outer"] = [next(it) for _ in range(nout)]
+        ps["terms"] = [dict(zip(("mask", "pos4", "jtab", "tab", "nb", "hasj", "lmask"), (next(it) for _ in range(7))))
+                       for _ in range(nt)]
+        ps["gstart"] = [next(it) for _ in range(ng + 1)]
+        ps["gxor"] = [next(it) for _ in range(ng)]
+        passes.append(ps)
+    return {"xterms": xterms, "passes": passes}
+
+
 class Model:
     """A compiled model on the current device (pned_model_create)."""
 

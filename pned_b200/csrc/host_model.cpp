@@ -773,6 +773,52 @@ int plan_qtiles(const HostProgram &P, int k, int low, std::vector<QTilePass> &pa
 // ---------------------------------------------------------------------------
 // Tridiagonal routines (CPU, as in the reference)
 // ---------------------------------------------------------------------------
+// Single-vector tile plan of a model as the tile kernels receive it, computed
+// on the host (no device work): the program's flip terms, then every pass.
+extern "C" int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_plan *plan, int64_t *out,
+                                     int64_t cap, int64_t *len)
+{
+    using namespace pned;
+    if (!d || !len || (cap > 0 && !out)) return fail(PNED_EINVAL, "pned_tile_plan_export: bad arguments");
+    HostProgram P;
+    int rc = compile_program(d, P);
+    if (rc) return rc;
+    if (P.q != 2 || P.sector) return fail(PNED_ENOTSUP, "pned_tile_plan_export: tiles are planned for the S = 1/2 full basis");
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1};
+    const pned_tile_plan &pl = plan ? *plan : def;
+    if (pl.max_passes > kTileMaxPasses || pl.window_bits > 30 || pl.row_fixed_bits > 8 || pl.j_bits > kTileMaxJB ||
+        pl.j_bits == 0)
+        return fail(PNED_EINVAL, "pned_tile_plan_export: plan out of range");
+    // the defaults of the model's own plan
+    const int fixed = pl.row_fixed_bits >= 0 ? pl.row_fixed_bits : 8;
+    const int window = pl.window_bits >= 0 ? pl.window_bits : kTileWindowBits;
+    const int mp = pl.max_passes > 0 ? pl.max_passes : kTileMaxPasses;
+    const int jb = pl.j_bits > 0 ? pl.j_bits : 3;
+    std::vector<HostProgram::TilePass> passes;
+    rc = plan_tiles(P, 8, jb, fixed, window, mp, passes);
+    if (rc) return fail(rc, "pned_tile_plan_export: no tile plan for this model and plan");
+    std::vector<int64_t> v;
+    v.push_back(int64_t(P.xterms.size()));
+    for (const XorTerm &t : P.xterms) v.insert(v.end(), {int64_t(t.xmask), int64_t(t.pos4), int64_t(t.tab), int64_t(t.nb)});
+    v.push_back(int64_t(passes.size()));
+    for (const auto &ps : passes) {
+        const int ng = int(ps.gxor.size());
+        v.insert(v.end(), {int64_t(ps.tbits), int64_t(ps.jb), int64_t(ps.outer.size()), int64_t(ps.tterms.size()),
+                           int64_t(ps.nin), int64_t(ng)});
+        for (int k = 0; k < ps.tbits; ++k) v.push_back(ps.rowpos[k]);
+        for (int k = 0; k < ps.jb; ++k) v.push_back(ps.jpos[k]);
+        for (int o : ps.outer) v.push_back(o);
+        for (const TileTerm &t : ps.tterms)
+            v.insert(v.end(), {int64_t(t.mask), int64_t(t.pos4), int64_t(t.jtab), int64_t(t.tab), int64_t(t.nb),
+                               int64_t(t.hasj), int64_t(t.lmask)});
+        for (int g = 0; g <= ng; ++g) v.push_back(ps.gstart[g]);
+        for (int g = 0; g < ng; ++g) v.push_back(int64_t(ps.gxor[g]));
+    }
+    *len = int64_t(v.size());
+    for (int64_t i = 0; i < std::min<int64_t>(cap, *len); ++i) out[i] = v[size_t(i)];
+    return PNED_OK;
+}
+
 extern "C" int pned_bisec(const double *alpha, const double *beta, int ndim, double *E, int ne, double eps)
 {
     // Sturm-sequence bisection, S1/2 basic.f90:25-107

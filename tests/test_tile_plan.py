@@ -1,0 +1,125 @@
+"""Host-side checks of the single-vector tile plans (no GPU).
+
+The tile kernel (pned_b200/csrc/device.cu, hv_tile_kernel) stages a tile of
+256 x 2^jb states: thread t holds row t (its 8 bits on the global bits rowpos)
+and j-th state base | jexp[j] (the j bits on jpos); the other (outer) bits
+number the tiles.  An in-tile term gathers element (t ^ mask_lo) + 256 (j ^
+mask_hi) of the staged tile, an out-of-tile term the state (base ^ mask) ^
+jexp[j]; the coefficient index takes the dependency bits of `base` and, for
+terms with a dependency on a j bit, the 4-bit field j of `jtab`.  These tests
+replay that arithmetic in numpy for every state of the basis and compare it
+with the direct global computation (partner s ^ xmask, index = the dependency
+bits of s), and check that the passes cover every flip term exactly once.
+"""
+import numpy as np
+import pytest
+
+import pned_b200 as P
+from pned_b200 import api
+from pned_b200 import couplings as CP
+from pned_b200.lattice import honeycomb
+
+
+def bits_to(values, positions):
+    """Scatter bit k of each value to global bit positions[k]."""
+    out = np.zeros_like(values)
+    for k, p in enumerate(positions):
+        out |= ((values >> k) & 1) << p
+    return out
+
+
+def gather_bits(states, positions):
+    """Bit k of the result = bit positions[k] of the state."""
+    out = np.zeros_like(states)
+    for k, p in enumerate(positions):
+        out |= ((states >> p) & 1) << k
+    return out
+
+
+def check_plan(n, plan, fixed):
+    want = sorted((t["xmask"], t["pos4"], t["tab"], t["nb"]) for t in plan["xterms"])
+    got = []
+    states = np.arange(1 << n, dtype=np.int64)
+    for ps in plan["passes"]:
+        tb, jb = ps["tbits"], ps["jb"]
+        rowpos, jpos, outer = ps["rowpos"], ps["jpos"], ps["outer"]
+        assert tb == 8
+        assert sorted(rowpos + jpos + outer) == list(range(n))
+        assert rowpos[:fixed] == list(range(fixed))
+        rowmask = sum(1 << b for b in rowpos)
+        jmask = sum(1 << b for b in jpos)
+        tilemask = rowmask | jmask
+        tid = gather_bits(states, rowpos)
+        j = gather_bits(states, jpos)
+        jexp = bits_to(np.arange(1 << jb, dtype=np.int64), jpos)
+        base = states & ~jmask
+        terms = ps["terms"]
+        for ti, T in enumerate(terms):
+            inner = ti < ps["nin"]
+            deps = [(T["pos4"] >> (8 * d)) & 0xFF for d in range(T["nb"])]
+            if inner:
+                gmask = int(bits_to(np.array([T["mask"] & 0xFF]), rowpos)[0]) | \
+                    int(bits_to(np.array([T["mask"] >> 8]), jpos)[0])
+                assert gmask & ~tilemask == 0
+                lt, lj = tid ^ (T["mask"] & 0xFF), j ^ (T["mask"] >> 8)
+                partner = (states & ~tilemask) | bits_to(lt, rowpos) | jexp[lj]
+            else:
+                gmask = T["mask"]
+                assert gmask & ~tilemask != 0
+                assert T["lmask"] == int(gather_bits(np.array([gmask & rowmask]), rowpos)[0]) | \
+                    (int(gather_bits(np.array([gmask & jmask]), jpos)[0]) << tb)
+                partner = (base ^ gmask) ^ jexp[j]
+            assert np.array_equal(partner, states ^ gmask)
+            got.append((gmask, T["pos4"], T["tab"], T["nb"]))
+            assert T["hasj"] == int(any(p in jpos for p in deps))
+            ib = gather_bits(base, deps)
+            jt = np.array([(T["jtab"] >> (4 * jj)) & 15 for jj in range(1 << jb)], dtype=np.int64)
+            kidx = ib | jt[j] if T["hasj"] else ib
+            assert np.array_equal(kidx, gather_bits(states, deps))
+        assert ps["gstart"][0] == ps["nin"] and ps["gstart"][-1] == len(terms)
+        assert len(set(ps["gxor"])) == len(ps["gxor"])
+        for g, gx in enumerate(ps["gxor"]):
+            for ti in range(ps["gstart"][g], ps["gstart"][g + 1]):
+                assert terms[ti]["mask"] & ~tilemask == gx
+    assert sorted(got) == want
+
+
+MODELS = [
+    ("KH", CP.kitaev_heisenberg(0.3, -1.0), None),
+    ("KHG-h111", CP.kitaev_heisenberg(0.3, -1.0, gamma=0.1), CP.field_111(0.05)),
+    ("slots", CP.slots(J1=0.4, K1=-0.3, I11=0.2, I12=-0.1, J1p=0.7, K1p=1.1, J1pp=-0.5, I11p=0.05, I12p=0.3,
+                       I12pp=-0.2, J2=0.15, K2=0.25, I21=0.01, I22=0.02, J3=0.3, ratio_l=0.8), [0.01, 0.02, 0.03]),
+]
+PLANS = [(8, 10, 4, 3), (5, 8, 2, 4), (3, 6, 1, 4), (5, 12, 2, 2), (5, 4, 3, 1), (0, 6, 3, 4), (8, 2, 4, 3)]
+
+
+@pytest.mark.parametrize("plan", PLANS, ids=[",".join(map(str, p)) for p in PLANS])
+@pytest.mark.parametrize("name,cpl,fld", MODELS, ids=[m[0] for m in MODELS])
+def test_tile_plan_index_arithmetic(name, cpl, fld, plan):
+    cl = honeycomb(2, 4)
+    X, skip, pt = P.build_xlocal(2, 0, cpl, field=fld)
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    out = api.tile_plan_export(d, *plan)
+    assert 1 <= len(out["passes"]) <= plan[2]
+    assert all(ps["jb"] == plan[3] for ps in out["passes"])
+    check_plan(cl.n, out, plan[0])
+
+
+def test_tile_plan_eighteen_sites_default_plan():
+    """N = 18 (3x3) with the default plan and the 16-row tiles."""
+    cl = honeycomb(3, 3)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(0.3, -1.0, gamma=0.1), field=CP.field_111(0.05))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    check_plan(cl.n, api.tile_plan_export(d), 8)
+    check_plan(cl.n, api.tile_plan_export(d, 5, 10, 2, 4), 5)
+
+
+def test_tile_plan_export_refuses_what_is_not_tiled():
+    cl = honeycomb(2, 4)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(1.0, 0.0))
+    assert pt == 0   # Sz sector: not tiled
+    with pytest.raises(P.PnedError):
+        api.tile_plan_export(P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt))
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(0.3, -1.0))
+    with pytest.raises(P.PnedError):
+        api.tile_plan_export(P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt), 5, 8, 2, 5)
