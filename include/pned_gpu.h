@@ -171,6 +171,16 @@ int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_plan *plan, int64_t *out, int64_t cap,
                           int64_t *len);
 /*
+ * Test hook (no counterpart in the reference): the mixed-radix tile passes of k
+ * sites (q > 2, full basis; the `low` lowest sites in every tile) that the tiled
+ * mixed-radix kernel runs, computed on the host.  out[0..cap) receives int64
+ * values, *len the full count: q, n, the number of radix terms X, X records
+ * (offset, s1, s2, tab), the table size T and T flags (entry nonzero), the
+ * number of passes, and per pass (k, nouter, nterms), sites[k], outer[nouter],
+ * nterms records (loff, ls1, ls2, tab).
+ */
+int pned_qtile_plan_export(const pned_model_desc *d, int k, int low, int64_t *out, int64_t cap, int64_t *len);
+/*
  * Measurement hook (no counterpart in the reference): the partner-tile
  * staging the single-vector plan actually runs (0 gathered through L1/L2,
  * 1 cp.async, 2 bulk copies) and, for 2, the number of ring stages.

@@ -53,7 +53,7 @@ _lib = None
 
 EXPORTS = [
     "pned_abi_version", "pned_last_error", "pned_set_device", "pned_build_xlocal", "pned_tps_transform",
-    "pned_mk_list12", "pned_model_create", "pned_model_destroy", "pned_model_info", "pned_model_plan", "pned_model_set_plan", "pned_tile_plan_export", "pned_model_tile_staging", "pned_model_sector_segments", "pned_ctx_create",
+    "pned_mk_list12", "pned_model_create", "pned_model_destroy", "pned_model_info", "pned_model_plan", "pned_model_set_plan", "pned_tile_plan_export", "pned_qtile_plan_export", "pned_model_tile_staging", "pned_model_sector_segments", "pned_ctx_create",
     "pned_ctx_destroy", "pned_ctx_set_stream", "pned_ctx_synchronize", "pned_ctx_buffer", "pned_ctx_bytes",
     "pned_hv", "pned_inprdct", "pned_calc_beta", "pned_fill_gaussian", "pned_lanczos_run", "pned_tps_run",
     "pned_dsf_run", "pned_dsf_xy_run", "pned_session_begin_dsf_xy", "pned_cg_run", "pned_bisec", "pned_vec12", "pned_exec_renbun", "pned_normalize_dsf",
@@ -95,6 +95,7 @@ def lib() -> C.CDLL:
     L.pned_model_sector_segments.argtypes = [vp, i32, ip]
     L.pned_model_set_plan.argtypes = [vp, i32, C.POINTER(TilePlan)]
     L.pned_tile_plan_export.argtypes = [vp, C.POINTER(TilePlan), C.POINTER(i64), i64, C.POINTER(i64)]
+    L.pned_qtile_plan_export.argtypes = [vp, i32, i32, C.POINTER(i64), i64, C.POINTER(i64)]
     L.pned_ctx_create.argtypes = [vp, i32, C.c_size_t, C.POINTER(vp)]
     L.pned_ctx_destroy.argtypes = [vp]
     L.pned_ctx_set_stream.argtypes = [vp, vp]

@@ -317,6 +317,27 @@ def tile_plan_export(desc: "ModelInput", row_fixed_bits: int = -1, window_bits: 
     return {"xterms": xterms, "passes": passes}
 
 
+def qtile_plan_export(desc: "ModelInput", k: int, low: int = 0) -> dict:
+    """The mixed-radix tile passes of k sites (q > 2, full basis) that the tiled
+    mixed-radix kernel runs, computed on the host (pned_qtile_plan_export)."""
+    n = C.c_int64(0)
+    check(lib().pned_qtile_plan_export(C.byref(desc.c), int(k), int(low), None, 0, C.byref(n)))
+    buf = np.zeros(n.value, dtype=np.int64)
+    check(lib().pned_qtile_plan_export(C.byref(desc.c), int(k), int(low), buf.ctypes.data_as(C.POINTER(C.c_int64)),
+                                       n.value, C.byref(n)))
+    it = iter(buf.tolist())
+    q, nsites, nr = next(it), next(it), next(it)
+    rterms = [dict(zip(("offset", "s1", "s2", "tab"), (next(it) for _ in range(4)))) for _ in range(nr)]
+    nonzero = [next(it) for _ in range(next(it))]
+    passes = []
+    for _ in range(next(it)):
+        kk, nout, nt = (next(it) for _ in range(3))
+        ps = {"sites": [next(it) for _ in range(kk)], "outer": [next(it) for _ in range(nout)]}
+        ps["terms"] = [dict(zip(("loff", "ls1", "ls2", "tab"), (next(it) for _ in range(4)))) for _ in range(nt)]
+        passes.append(ps)
+    return {"q": q, "n": nsites, "rterms": rterms, "nonzero": nonzero, "passes": passes}
+
+
 class Model:
     """A compiled model on the current device (pned_model_create)."""
 

@@ -819,6 +819,38 @@ extern "C" int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_p
     return PNED_OK;
 }
 
+// Mixed-radix tile passes of k sites (the `low` lowest sites kept in every
+// tile) as the tiled mixed-radix kernel receives them, computed on the host:
+// the program's radix terms, which table entries are nonzero, then every pass.
+extern "C" int pned_qtile_plan_export(const pned_model_desc *d, int k, int low, int64_t *out, int64_t cap,
+                                      int64_t *len)
+{
+    using namespace pned;
+    if (!d || !len || (cap > 0 && !out)) return fail(PNED_EINVAL, "pned_qtile_plan_export: bad arguments");
+    HostProgram P;
+    int rc = compile_program(d, P);
+    if (rc) return rc;
+    if (P.q <= 2 || P.sector) return fail(PNED_ENOTSUP, "pned_qtile_plan_export: mixed-radix tiles need q > 2, full basis");
+    std::vector<QTilePass> passes;
+    rc = plan_qtiles(P, k, low, passes);
+    if (rc) return fail(rc, "pned_qtile_plan_export: no tile passes for this k");
+    std::vector<int64_t> v{int64_t(P.q), int64_t(P.n), int64_t(P.rterms.size())};
+    for (const RadixTerm &t : P.rterms) v.insert(v.end(), {t.offset, int64_t(t.s1), int64_t(t.s2), int64_t(t.tab)});
+    v.push_back(int64_t(P.table.size()));
+    for (const cd &z : P.table) v.push_back(z != cd(0, 0) ? 1 : 0);
+    v.push_back(int64_t(passes.size()));
+    for (const QTilePass &ps : passes) {
+        v.insert(v.end(), {int64_t(ps.sites.size()), int64_t(ps.outer.size()), int64_t(ps.terms.size())});
+        for (int x : ps.sites) v.push_back(x);
+        for (int x : ps.outer) v.push_back(x);
+        for (const QTileTerm &t : ps.terms)
+            v.insert(v.end(), {int64_t(t.loff), int64_t(t.ls1), int64_t(t.ls2), int64_t(t.tab)});
+    }
+    *len = int64_t(v.size());
+    for (int64_t i = 0; i < std::min<int64_t>(cap, *len); ++i) out[i] = v[size_t(i)];
+    return PNED_OK;
+}
+
 extern "C" int pned_bisec(const double *alpha, const double *beta, int ndim, double *E, int ne, double eps)
 {
     // Sturm-sequence bisection, S1/2 basic.f90:25-107

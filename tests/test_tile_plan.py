@@ -1,4 +1,5 @@
-"""Host-side checks of the single-vector tile plans (no GPU).
+"""Host-side checks of the tile plans (no GPU): the single-vector S = 1/2 tiles
+and the mixed-radix (S >= 1) tiles.
 
 The tile kernel (pned_b200/csrc/device.cu, hv_tile_kernel) stages a tile of
 256 x 2^jb states: thread t holds row t (its 8 bits on the global bits rowpos)
@@ -10,6 +11,8 @@ terms with a dependency on a j bit, the 4-bit field j of `jtab`.  These tests
 replay that arithmetic in numpy for every state of the basis and compare it
 with the direct global computation (partner s ^ xmask, index = the dependency
 bits of s), and check that the passes cover every flip term exactly once.
+The mixed-radix replay (check_qplan) does the same for hv_qtile_kernel's
+base-q tile offsets and partner offsets.
 """
 import numpy as np
 import pytest
@@ -123,3 +126,56 @@ def test_tile_plan_export_refuses_what_is_not_tiled():
     X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(0.3, -1.0))
     with pytest.raises(P.PnedError):
         api.tile_plan_export(P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt), 5, 8, 2, 5)
+
+
+def check_qplan(r, low):
+    """Replays the tiled mixed-radix kernel's index arithmetic (hv_qtile.cu):
+    tile base from the outer digits, local index l from the tile sites' digits,
+    state = base + goff[l], pair state from the local digits ls1/ls2, partner =
+    base + goff[l + loff]; compared with the program's flat radix terms."""
+    q, n = r["q"], r["n"]
+    rt = {t["tab"]: t for t in r["rterms"]}
+    assert len(rt) == len(r["rterms"])
+    nonzero = np.array(r["nonzero"], dtype=bool)
+    states = np.arange(q ** n, dtype=np.int64)
+    digits = [(states // q ** i) % q for i in range(n)]
+    covered = []
+    for ps in r["passes"]:
+        sites, outer = ps["sites"], ps["outer"]
+        nt = q ** len(sites)
+        assert sites == sorted(sites) and outer == sorted(outer) and sorted(sites + outer) == list(range(n))
+        assert sites[:low] == list(range(low))
+        loc = sum(digits[x] * q ** i for i, x in enumerate(sites))
+        base = sum(digits[x] * q ** x for x in outer)
+        lidx = np.arange(nt, dtype=np.int64)
+        goff = sum(((lidx // q ** i) % q) * q ** x for i, x in enumerate(sites))
+        assert np.array_equal(base + goff[loc], states)
+        for T in ps["terms"]:
+            R = rt[T["tab"]]
+            covered.append(T["tab"])
+            assert (sites[T["ls1"]], sites[T["ls2"]]) == (R["s1"], R["s2"])
+            pair = (loc // q ** T["ls1"]) % q + q * ((loc // q ** T["ls2"]) % q)
+            assert np.array_equal(pair, digits[R["s1"]] + q * digits[R["s2"]])
+            nz = nonzero[R["tab"] + pair]
+            pl = loc[nz] + T["loff"]
+            assert np.all((pl >= 0) & (pl < nt))
+            assert np.array_equal(base[nz] + goff[pl], states[nz] + R["offset"])
+    assert sorted(covered) == sorted(rt)
+
+
+QMODELS = [
+    ("S1-KH", 3, CP.kitaev_heisenberg(0.2, -1.0), None, 2, 2),
+    ("S1-KHG-h111", 3, CP.kitaev_heisenberg(0.2, -1.0, gamma=0.1), CP.field_111(0.05), 2, 2),
+    ("S3/2-KHG", 4, CP.kitaev_heisenberg(-0.3, 0.6, gamma=0.2), None, 3, 1),
+]
+
+
+@pytest.mark.parametrize("k,low", [(3, 0), (4, 1), (5, 1), (6, 0)])
+@pytest.mark.parametrize("name,q,cpl,fld,L1,L2", QMODELS, ids=[m[0] for m in QMODELS])
+def test_qtile_plan_index_arithmetic(name, q, cpl, fld, L1, L2, k, low):
+    cl = honeycomb(L1, L2)
+    if k > cl.n - 2:
+        pytest.skip("tiles leave at least two outer sites")
+    X, skip, pt = P.build_xlocal(q, 1, cpl, field=fld)
+    d = P.ModelInput(cl.n, q, 1, cl.ipair, cl.ibond_type, X, skip, pt)
+    check_qplan(api.qtile_plan_export(d, k, low), low)
