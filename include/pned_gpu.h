@@ -158,18 +158,20 @@ typedef struct {
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 /*
- * Test and measurement hook (no counterpart in the reference): the
- * single-vector tile plan (S = 1/2 full basis) that pned_model_set_plan would
- * build for this model, computed on the host without device work.  out[0..cap)
+ * Test and measurement hook (no counterpart in the reference): the tile plan
+ * (S = 1/2 full basis) that the planner builds for this model with row_bits row
+ * bits a tile (8: the single-vector kernel, as pned_model_set_plan; fewer: the
+ * multi-vector kernel's 256 / G rows), computed on the host without device
+ * work; the default fixed row bits are min(row_bits, 8).  out[0..cap)
  * receives int64 values, *len the full count: the number of flip terms X, X
  * records (xmask, pos4, tab, nb), the number of passes, and per pass (tbits, jb,
  * nouter, nterms, nin, ngroups), rowpos[tbits], jpos[jb], outer[nouter], nterms
  * records (mask, pos4, jtab, tab, nb, hasj, lmask), gstart[ngroups + 1],
  * gxor[ngroups].  In-tile terms (the first nin) carry the local xor (row bits
- * 0..7, then the j bits), the others the global xor.
+ * 0..tbits-1, then the j bits), the others the global xor.
  */
-int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_plan *plan, int64_t *out, int64_t cap,
-                          int64_t *len);
+int pned_tile_plan_export(const pned_model_desc *d, int row_bits, const pned_tile_plan *plan, int64_t *out,
+                          int64_t cap, int64_t *len);
 /*
  * Test hook (no counterpart in the reference): the mixed-radix tile passes of k
  * sites (q > 2, full basis; the `low` lowest sites in every tile) that the tiled

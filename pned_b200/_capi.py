@@ -94,7 +94,7 @@ def lib() -> C.CDLL:
     L.pned_model_tile_staging.argtypes = [vp, ip, ip]
     L.pned_model_sector_segments.argtypes = [vp, i32, ip]
     L.pned_model_set_plan.argtypes = [vp, i32, C.POINTER(TilePlan)]
-    L.pned_tile_plan_export.argtypes = [vp, C.POINTER(TilePlan), C.POINTER(i64), i64, C.POINTER(i64)]
+    L.pned_tile_plan_export.argtypes = [vp, i32, C.POINTER(TilePlan), C.POINTER(i64), i64, C.POINTER(i64)]
     L.pned_qtile_plan_export.argtypes = [vp, i32, i32, C.POINTER(i64), i64, C.POINTER(i64)]
     L.pned_ctx_create.argtypes = [vp, i32, C.c_size_t, C.POINTER(vp)]
     L.pned_ctx_destroy.argtypes = [vp]

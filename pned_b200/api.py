@@ -289,16 +289,17 @@ class ModelInput:
 
 
 def tile_plan_export(desc: "ModelInput", row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
-                     j_bits: int = -1) -> dict:
-    """The single-vector tile plan (S = 1/2 full basis) that Model.set_plan would
-    build, computed on the host (pned_tile_plan_export): the program's flip terms
-    and, per pass, the tile bits, outer order, terms and partner-tile groups."""
+                     j_bits: int = -1, row_bits: int = 8) -> dict:
+    """The tile plan (S = 1/2 full basis) with row_bits row bits a tile (8: the
+    single-vector plan Model.set_plan builds), computed on the host
+    (pned_tile_plan_export): the program's flip terms and, per pass, the tile
+    bits, outer order, terms and partner-tile groups."""
     tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1)
     n = C.c_int64(0)
-    check(lib().pned_tile_plan_export(C.byref(desc.c), C.byref(tp), None, 0, C.byref(n)))
+    check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), C.byref(tp), None, 0, C.byref(n)))
     buf = np.zeros(n.value, dtype=np.int64)
-    check(lib().pned_tile_plan_export(C.byref(desc.c), C.byref(tp), buf.ctypes.data_as(C.POINTER(C.c_int64)),
-                                      n.value, C.byref(n)))
+    check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), C.byref(tp),
+                                      buf.ctypes.data_as(C.POINTER(C.c_int64)), n.value, C.byref(n)))
     it = iter(buf.tolist())
     nx = next(it)
     xterms = [dict(zip(("xmask", "pos4", "tab", "nb"), (next(it) for _ in range(4)))) for _ in range(nx)]

@@ -773,13 +773,15 @@ int plan_qtiles(const HostProgram &P, int k, int low, std::vector<QTilePass> &pa
 // ---------------------------------------------------------------------------
 // Tridiagonal routines (CPU, as in the reference)
 // ---------------------------------------------------------------------------
-// Single-vector tile plan of a model as the tile kernels receive it, computed
-// on the host (no device work): the program's flip terms, then every pass.
-extern "C" int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_plan *plan, int64_t *out,
-                                     int64_t cap, int64_t *len)
+// Tile plan of a model as the S = 1/2 tile kernels receive it (row_bits = 8:
+// the single-vector kernel; log2(256 / G): the multi-vector kernel), computed on
+// the host (no device work): the program's flip terms, then every pass.
+extern "C" int pned_tile_plan_export(const pned_model_desc *d, int row_bits, const pned_tile_plan *plan,
+                                     int64_t *out, int64_t cap, int64_t *len)
 {
     using namespace pned;
-    if (!d || !len || (cap > 0 && !out)) return fail(PNED_EINVAL, "pned_tile_plan_export: bad arguments");
+    if (!d || !len || (cap > 0 && !out) || row_bits < 1 || row_bits > 8)
+        return fail(PNED_EINVAL, "pned_tile_plan_export: bad arguments");
     HostProgram P;
     int rc = compile_program(d, P);
     if (rc) return rc;
@@ -789,13 +791,13 @@ extern "C" int pned_tile_plan_export(const pned_model_desc *d, const pned_tile_p
     if (pl.max_passes > kTileMaxPasses || pl.window_bits > 30 || pl.row_fixed_bits > 8 || pl.j_bits > kTileMaxJB ||
         pl.j_bits == 0)
         return fail(PNED_EINVAL, "pned_tile_plan_export: plan out of range");
-    // the defaults of the model's own plan
-    const int fixed = pl.row_fixed_bits >= 0 ? pl.row_fixed_bits : 8;
+    // the defaults of the model's own single-vector plan
+    const int fixed = std::min(row_bits, pl.row_fixed_bits >= 0 ? pl.row_fixed_bits : 8);
     const int window = pl.window_bits >= 0 ? pl.window_bits : kTileWindowBits;
     const int mp = pl.max_passes > 0 ? pl.max_passes : kTileMaxPasses;
     const int jb = pl.j_bits > 0 ? pl.j_bits : 3;
     std::vector<HostProgram::TilePass> passes;
-    rc = plan_tiles(P, 8, jb, fixed, window, mp, passes);
+    rc = plan_tiles(P, row_bits, jb, fixed, window, mp, passes);
     if (rc) return fail(rc, "pned_tile_plan_export: no tile plan for this model and plan");
     std::vector<int64_t> v;
     v.push_back(int64_t(P.xterms.size()));

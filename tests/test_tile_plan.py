@@ -46,7 +46,6 @@ def check_plan(n, plan, fixed):
     for ps in plan["passes"]:
         tb, jb = ps["tbits"], ps["jb"]
         rowpos, jpos, outer = ps["rowpos"], ps["jpos"], ps["outer"]
-        assert tb == 8
         assert sorted(rowpos + jpos + outer) == list(range(n))
         assert rowpos[:fixed] == list(range(fixed))
         rowmask = sum(1 << b for b in rowpos)
@@ -61,10 +60,11 @@ def check_plan(n, plan, fixed):
             inner = ti < ps["nin"]
             deps = [(T["pos4"] >> (8 * d)) & 0xFF for d in range(T["nb"])]
             if inner:
-                gmask = int(bits_to(np.array([T["mask"] & 0xFF]), rowpos)[0]) | \
-                    int(bits_to(np.array([T["mask"] >> 8]), jpos)[0])
+                tmask = (1 << tb) - 1
+                gmask = int(bits_to(np.array([T["mask"] & tmask]), rowpos)[0]) | \
+                    int(bits_to(np.array([T["mask"] >> tb]), jpos)[0])
                 assert gmask & ~tilemask == 0
-                lt, lj = tid ^ (T["mask"] & 0xFF), j ^ (T["mask"] >> 8)
+                lt, lj = tid ^ (T["mask"] & tmask), j ^ (T["mask"] >> tb)
                 partner = (states & ~tilemask) | bits_to(lt, rowpos) | jexp[lj]
             else:
                 gmask = T["mask"]
@@ -115,6 +115,24 @@ def test_tile_plan_eighteen_sites_default_plan():
     d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
     check_plan(cl.n, api.tile_plan_export(d), 8)
     check_plan(cl.n, api.tile_plan_export(d, 5, 10, 2, 4), 5)
+
+
+# the multi-vector kernel: G = R / VPT threads a state, 256 / G state rows, SPT = 2^jb rows a thread
+RV_SHAPES = [(16, 5, 2), (8, 6, 2), (4, 7, 2), (12, 5, 1), (6, 6, 1), (3, 7, 1)]   # (R, row bits, jb)
+
+
+@pytest.mark.parametrize("R,tbits,jb", RV_SHAPES, ids=[f"R{r}" for r, _, _ in RV_SHAPES])
+@pytest.mark.parametrize("fixed,window,passes", [(-1, 6, 2), (0, 10, 2), (2, 4, 3)])
+def test_multi_vector_tile_plan_index_arithmetic(R, tbits, jb, fixed, window, passes):
+    """The planner at the multi-vector kernel's tile shapes (hv_tile_rv_kernel:
+    row l = thread / G on rowpos, in-tile partner row l ^ (mask & (2^tbits - 1)),
+    j ^ (mask >> tbits))."""
+    cl = honeycomb(2, 4)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(0.3, -1.0, gamma=0.1), field=CP.field_111(0.05))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    out = api.tile_plan_export(d, fixed, window, passes, jb, row_bits=tbits)
+    assert all(ps["tbits"] == tbits and ps["jb"] == jb for ps in out["passes"])
+    check_plan(cl.n, out, tbits if fixed < 0 else min(fixed, tbits))
 
 
 def test_tile_plan_export_refuses_what_is_not_tiled():
