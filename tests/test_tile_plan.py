@@ -197,3 +197,19 @@ def test_qtile_plan_index_arithmetic(name, q, cpl, fld, L1, L2, k, low):
     X, skip, pt = P.build_xlocal(q, 1, cpl, field=fld)
     d = P.ModelInput(cl.n, q, 1, cl.ipair, cl.ibond_type, X, skip, pt)
     check_qplan(api.qtile_plan_export(d, k, low), low)
+
+
+def test_headline_plan_structure_n30():
+    """The N = 30 Kitaev-Heisenberg plans the measurements quote: the tuned plan
+    (5 fixed row bits, 12 window bits, 2 passes, 8 rows a thread) has 2 passes and
+    17 partner tiles; the 16-row tiles 14 (window 11) and 15 (window 10)."""
+    import math
+    from pned_b200.lattice import cluster_for_sites
+    cl = cluster_for_sites(30)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi)))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    for plan, groups in (((5, 12, 2, 3), 17), ((5, 11, 2, 4), 14), ((5, 10, 2, 4), 15)):
+        r = api.tile_plan_export(d, *plan)
+        assert len(r["xterms"]) == 45 and len(r["passes"]) == 2
+        assert sum(len(ps["gxor"]) for ps in r["passes"]) == groups
+        assert sum(len(ps["terms"]) for ps in r["passes"]) == 45
