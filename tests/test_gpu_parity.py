@@ -625,7 +625,8 @@ def test_larger_hv_parity_n24():
     assert abs(pr[0] - prr) <= 1e-12 * scale
 
 
-@pytest.mark.parametrize("name", ["s12_kh_n8", "s12_khg_h111_n12", "s1_kh_n6", "s1_khg_h111_n8"])
+@pytest.mark.parametrize("name", ["s12_kh_n8", "s12_khg_h111_n12", "s1_kh_n6", "s1_khg_h111_n8",
+                                  "s12_heis_sz0_n12", "s12_heis_sz0_n16", "s1_heis_sz0_n8"])
 def test_cuda_path_against_golden_fixtures(name):
     """The CUDA path, through the C ABI, reproduces the committed fixtures of
     tests/golden (H^T v and the ground-state energy from the independent dense

@@ -293,7 +293,8 @@ def test_inverse_iteration_ground_state():
 
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.npz")
-GOLDEN_CASES = ["s12_kh_n8", "s12_khg_h111_n12", "s1_kh_n6", "s1_khg_h111_n8"]
+GOLDEN_CASES = ["s12_kh_n8", "s12_khg_h111_n12", "s1_kh_n6", "s1_khg_h111_n8",
+                "s12_heis_sz0_n12", "s12_heis_sz0_n16", "s1_heis_sz0_n8"]
 
 
 def golden_case(name):
