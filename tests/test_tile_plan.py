@@ -213,3 +213,20 @@ def test_headline_plan_structure_n30():
         assert len(r["xterms"]) == 45 and len(r["passes"]) == 2
         assert sum(len(ps["gxor"]) for ps in r["passes"]) == groups
         assert sum(len(ps["terms"]) for ps in r["passes"]) == 45
+
+
+def test_every_tuner_candidate_plans_the_n30_model():
+    """Each single-vector candidate of the autotuner yields a plan for the N = 30
+    Kitaev-Heisenberg model within its pass limit (a candidate the planner
+    refuses would be skipped silently while tuning)."""
+    import math
+    from pned_b200 import tune
+    from pned_b200.lattice import cluster_for_sites
+    cl = cluster_for_sites(30)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi)))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    for c in tune.CANDIDATES_1:
+        jb = c[3] if len(c) > 3 else -1
+        r = api.tile_plan_export(d, c[0], c[1], c[2], jb)
+        assert 1 <= len(r["passes"]) <= c[2]
+        assert sum(len(ps["terms"]) for ps in r["passes"]) == 45
