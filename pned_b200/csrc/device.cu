@@ -1554,6 +1554,11 @@ extern "C" int pned_hv_noalloc(const pned_model *m, int R, const pned_c128 *v1, 
     nb = std::min<int64_t>(nb, (kNoAllocScratch - kNoAllocHead) / R);
     nb = std::max<int64_t>(1, nb);
     while (nb > 1 && int64_t(hv_partial_blocks(m, R, int(nb))) * R > kNoAllocScratch - kNoAllocHead) --nb;
+    if (int64_t(hv_partial_blocks(m, R, int(nb))) * R > kNoAllocScratch - kNoAllocHead)
+        return fail(PNED_EINVAL, "pned_hv_noalloc: this model's H.v writes " +
+                                     std::to_string(hv_partial_blocks(m, R, int(nb))) + " x " + std::to_string(R) +
+                                     " partial sums even with one block, more than the " +
+                                     std::to_string(kNoAllocScratch - kNoAllocHead) + "-value scratch holds");
     double *ones = reinterpret_cast<double *>(scr);
     double2 *sums = scr + 16;
     double2 *partials = scr + kNoAllocHead;

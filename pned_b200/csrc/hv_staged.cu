@@ -186,10 +186,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     }
     return false;
 }
-// The same wait for a whole warp: true only if every lane saw the phase.
-__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity)
+// The wait of a whole warp in the tile loop (true only if every lane saw the
+// phase): as mbar_wait, but it also gives up as soon as another warp of the
+// block has raised the block's abort flag, so that one warp that stopped does
+// not leave the others waiting out their own limits.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, volatile int *abort_flag)
 {
-    return __all_sync(0xffffffffu, mbar_wait(bar, parity));
+    for (uint32_t i = 0; i < kBulkSpins; ++i) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(ok)
+                     : "r"(bar), "r"(parity), "r"(1000u)
+                     : "memory");
+        if (ok) return true;
+        if (*abort_flag) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ bool warp_wait_or_abort(uint32_t bar, uint32_t parity, volatile int *abort_flag)
+{
+    return __all_sync(0xffffffffu, mbar_wait_or_abort(bar, parity, abort_flag));
 }
 // One contiguous global -> shared copy by the bulk-copy (TMA) engine, no
 // multicast; completion is counted in bytes on the mbarrier.
@@ -264,7 +282,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1)
             for (int k = 0; k < prog.nouter; ++k) ob |= uint32_t((tile >> k) & 1) << prog.outer[k];
             for (int item = 0; item < items; ++item, ++it) {
                 const uint32_t s = it % uint32_t(nst), round = it / uint32_t(nst);
-                if (round > 0 && !warp_wait(smem_addr(empty + s), (round - 1) & 1u)) {
+                if (round > 0 && !warp_wait_or_abort(smem_addr(empty + s), (round - 1) & 1u, s_abort)) {
                     ok = false;
                     break;
                 }
@@ -324,7 +342,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1)
             // own tile: its values, the diagonal and the in-tile terms
             {
                 const uint32_t s = it % uint32_t(nst);
-                if (!warp_wait(smem_addr(full + s), (it / uint32_t(nst)) & 1u)) {
+                if (!warp_wait_or_abort(smem_addr(full + s), (it / uint32_t(nst)) & 1u, s_abort)) {
                     ok = false;
                     break;
                 }
@@ -375,7 +393,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1)
             // partner tiles, one per group, in the program's term order
             for (int g = 0; g < prog.ngroups; ++g, ++it) {
                 const uint32_t s = it % uint32_t(nst);
-                if (!warp_wait(smem_addr(full + s), (it / uint32_t(nst)) & 1u)) {
+                if (!warp_wait_or_abort(smem_addr(full + s), (it / uint32_t(nst)) & 1u, s_abort)) {
                     ok = false;
                     break;
                 }
