@@ -517,9 +517,12 @@ int pned_tpq_thermo(int num_data1, int n_seeds, const double *beta, const double
                     double t_min, double t_max, int num_div, double *out);
 /*
  * The ground-state vector file basisme%05d (readwrite_vec_data, S1/2
- * output.f90:12-36): two records, the energy e (double) and x[ll] (complex);
- * records above 2^31 bytes (ll > 2^27) would need Fortran subrecords and are
- * refused (PNED_ENOTSUP).
+ * output.f90:12-36): two records, the energy e (double) and x[ll] (complex).
+ * Records longer than one subrecord (2^31 - 9 bytes: ll > 134217727, every
+ * vector from N = 27 on) are written and read as gfortran writes them: split
+ * into subrecords, each framed by 4-byte length markers, the leading marker
+ * negative when another subrecord follows and the trailing one negative when
+ * one precedes.
  */
 int pned_write_vec_data(const char *path, double e, const pned_c128 *x, int64_t ll);
 int pned_read_vec_data(const char *path, double *e, pned_c128 *x, int64_t ll);
@@ -533,9 +536,15 @@ int pned_append_dsf_res(const char *path, double sq_re, const double *q2, const 
  * ' q = ', iq, q(1), q(2), Re sq in '(A,I3,2F12.6,F25.18)'. */
 int pned_append_sq(const char *path, int iq, double q1, double q2, double norm_re);
 /* vec_q%05dme%05d<comp> (dump_alpha_beta / read_alpha_beta2, S1/2 DSF.f90:374-379, 399-405):
- * records indx (int32), v1 [ll], v2 [ll]; vectors above 2^31 bytes are refused. */
+ * records indx (int32), v1 [ll], v2 [ll]; long records in subrecords as pned_write_vec_data. */
 int pned_write_dsf_vectors(const char *path, int indx, const pned_c128 *v1, const pned_c128 *v2, int64_t ll);
 int pned_read_dsf_vectors(const char *path, int *indx, pned_c128 *v1, pned_c128 *v2, int64_t ll);
+/*
+ * Largest payload of one subrecord for the writers above (no counterpart in the
+ * reference; gfortran's -fmax-subrecord-length): 1 .. 2147483639 bytes, default
+ * 2147483639.  The readers accept any subrecord split.  Process-wide.
+ */
+int pned_set_max_subrecord(int64_t bytes);
 
 #ifdef __cplusplus
 }

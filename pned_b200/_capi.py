@@ -65,7 +65,7 @@ EXPORTS = [
     "pned_write_salphasbeta", "pned_read_salphasbeta", "pned_tpq_thermo", "pned_session_save",
     "pned_session_load", "pned_session_info", "pned_write_vec_data", "pned_read_vec_data",
     "pned_write_dsf_alpha_beta", "pned_read_dsf_alpha_beta", "pned_append_dsf_res", "pned_append_sq",
-    "pned_write_dsf_vectors", "pned_read_dsf_vectors",
+    "pned_write_dsf_vectors", "pned_read_dsf_vectors", "pned_set_max_subrecord",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -154,6 +154,7 @@ def lib() -> C.CDLL:
     L.pned_append_sq.argtypes = [C.c_char_p, i32, dbl, dbl, dbl]
     L.pned_write_dsf_vectors.argtypes = [C.c_char_p, i32, vp, vp, i64]
     L.pned_read_dsf_vectors.argtypes = [C.c_char_p, ip, vp, vp, i64]
+    L.pned_set_max_subrecord.argtypes = [i64]
     _lib = L
     return L
 

@@ -223,6 +223,12 @@ def write_dsf_vectors(path: str, indx: int, v1, v2):
                                        C.c_void_p(b.ctypes.data), a.size))
 
 
+def set_max_subrecord(nbytes: int = 2147483639):
+    """Largest subrecord payload of the Fortran record writers (gfortran's
+    -fmax-subrecord-length; default 2^31 - 9 bytes)."""
+    check(lib().pned_set_max_subrecord(int(nbytes)))
+
+
 def read_dsf_vectors(path: str, ll: int):
     i = C.c_int(0)
     a = np.zeros(int(ll), dtype=np.complex128)

@@ -16,23 +16,69 @@ using namespace pned;
 
 namespace {
 
-// One Fortran unformatted sequential record: 4-byte length, payload, 4-byte length.
+// Largest payload of one subrecord: gfortran's default, 2^31 - 9 bytes
+// (its -fmax-subrecord-length); settable for tests.
+int64_t g_max_subrecord = 2147483639;
+
+// One Fortran unformatted sequential record (gfortran's documented layout):
+// the payload is split into subrecords of at most g_max_subrecord bytes, each
+// framed by 4-byte markers holding its length; the leading marker is negated
+// when another subrecord follows, the trailing one when a subrecord precedes.
+// A record that fits one subrecord is the plain length / payload / length.
 bool put_record(FILE *f, const void *data, size_t bytes)
 {
-    if (bytes > 0x7fffffffu) return false;
-    const int32_t len = int32_t(bytes);
-    return fwrite(&len, 4, 1, f) == 1 && (bytes == 0 || fwrite(data, 1, bytes, f) == bytes) &&
-           fwrite(&len, 4, 1, f) == 1;
+    const char *p = static_cast<const char *>(data);
+    size_t off = 0;
+    do {
+        const size_t n = std::min<size_t>(bytes - off, size_t(g_max_subrecord));
+        const bool more = off + n < bytes, first = off == 0;
+        const int32_t lead = more ? -int32_t(n) : int32_t(n), tail = first ? int32_t(n) : -int32_t(n);
+        if (fwrite(&lead, 4, 1, f) != 1 || (n && fwrite(p + off, 1, n, f) != n) || fwrite(&tail, 4, 1, f) != 1)
+            return false;
+        off += n;
+    } while (off < bytes);
+    return true;
+}
+
+// Reads one record, subrecord by subrecord, into `dst` (capacity `cap` bytes;
+// nullptr: only measure); *len receives the record's payload length.  False
+// on a malformed record or one longer than cap.
+bool read_record(FILE *f, char *dst, size_t cap, size_t *len)
+{
+    size_t total = 0;
+    for (bool first = true;; first = false) {
+        int32_t lead = 0, tail = 0;
+        if (fread(&lead, 4, 1, f) != 1 || lead == INT32_MIN) return false;
+        const size_t n = size_t(lead < 0 ? -int64_t(lead) : int64_t(lead));
+        if (dst) {
+            if (total + n > cap || (n && fread(dst + total, 1, n, f) != n)) return false;
+        } else if (n && std::fseek(f, long(n), SEEK_CUR) != 0) {
+            return false;
+        }
+        total += n;
+        if (fread(&tail, 4, 1, f) != 1) return false;
+        if (tail != (first ? int32_t(n) : -int32_t(n))) return false;
+        if (lead > 0) break;
+    }
+    *len = total;
+    return true;
 }
 
 // Reads one record into `out` (resized to the record length).
 bool get_record(FILE *f, std::vector<char> &out)
 {
-    int32_t len = 0, tail = 0;
-    if (fread(&len, 4, 1, f) != 1 || len < 0) return false;
-    out.resize(size_t(len));
-    if (len && fread(out.data(), 1, size_t(len), f) != size_t(len)) return false;
-    return fread(&tail, 4, 1, f) == 1 && tail == len;
+    const long pos = std::ftell(f);
+    size_t len = 0;
+    if (pos < 0 || !read_record(f, nullptr, 0, &len) || std::fseek(f, pos, SEEK_SET) != 0) return false;
+    out.resize(len);
+    return read_record(f, out.data(), len, &len);
+}
+
+// Reads one record of exactly `bytes` bytes into dst.
+bool get_record_exact(FILE *f, void *dst, size_t bytes)
+{
+    size_t len = 0;
+    return read_record(f, static_cast<char *>(dst), bytes, &len) && len == bytes;
 }
 
 // calc_fac (S_one_half/Hybrid_TPS_eval_mpi.f90:236-281): log-weights of the
@@ -182,11 +228,16 @@ extern "C" int pned_tpq_thermo(int num_data1, int n_seeds, const double *beta, c
 // ---------------------------------------------------------------------------
 // the reference's other output files
 // ---------------------------------------------------------------------------
+extern "C" int pned_set_max_subrecord(int64_t bytes)
+{
+    if (bytes < 1 || bytes > 2147483639) return fail(PNED_EINVAL, "pned_set_max_subrecord: 1 .. 2147483639 bytes");
+    g_max_subrecord = bytes;
+    return PNED_OK;
+}
+
 extern "C" int pned_write_vec_data(const char *path, double e, const pned_c128 *x, int64_t ll)
 {
     if (!path || !x || ll < 1) return fail(PNED_EINVAL, "pned_write_vec_data: bad arguments");
-    if (uint64_t(ll) * 16 > 0x7fffffffu)
-        return fail(PNED_ENOTSUP, "pned_write_vec_data: vectors above 2^31 bytes need Fortran subrecords");
     FILE *f = std::fopen(path, "wb");
     if (!f) return fail(PNED_EINVAL, std::string("pned_write_vec_data: cannot open ") + path);
     bool ok = put_record(f, &e, 8) && put_record(f, x, size_t(ll) * 16);
@@ -199,12 +250,9 @@ extern "C" int pned_read_vec_data(const char *path, double *e, pned_c128 *x, int
     if (!path || !e || !x || ll < 1) return fail(PNED_EINVAL, "pned_read_vec_data: bad arguments");
     FILE *f = std::fopen(path, "rb");
     if (!f) return fail(PNED_EINVAL, std::string("pned_read_vec_data: cannot open ") + path);
-    std::vector<char> r1, r2;
-    const bool ok = get_record(f, r1) && r1.size() == 8 && get_record(f, r2) && r2.size() == size_t(ll) * 16;
+    const bool ok = get_record_exact(f, e, 8) && get_record_exact(f, x, size_t(ll) * 16);
     std::fclose(f);
     if (!ok) return fail(PNED_EINVAL, "pned_read_vec_data: not a vector file of this length");
-    std::memcpy(e, r1.data(), 8);
-    std::memcpy(x, r2.data(), r2.size());
     return PNED_OK;
 }
 
@@ -268,8 +316,6 @@ extern "C" int pned_append_sq(const char *path, int iq, double q1, double q2, do
 extern "C" int pned_write_dsf_vectors(const char *path, int indx, const pned_c128 *v1, const pned_c128 *v2, int64_t ll)
 {
     if (!path || !v1 || !v2 || ll < 1) return fail(PNED_EINVAL, "pned_write_dsf_vectors: bad arguments");
-    if (uint64_t(ll) * 16 > 0x7fffffffu)
-        return fail(PNED_ENOTSUP, "pned_write_dsf_vectors: vectors above 2^31 bytes need Fortran subrecords");
     FILE *f = std::fopen(path, "wb");
     if (!f) return fail(PNED_EINVAL, std::string("pned_write_dsf_vectors: cannot open ") + path);
     const int32_t i4 = indx;
@@ -283,16 +329,11 @@ extern "C" int pned_read_dsf_vectors(const char *path, int *indx, pned_c128 *v1,
     if (!path || !indx || !v1 || !v2 || ll < 1) return fail(PNED_EINVAL, "pned_read_dsf_vectors: bad arguments");
     FILE *f = std::fopen(path, "rb");
     if (!f) return fail(PNED_EINVAL, std::string("pned_read_dsf_vectors: cannot open ") + path);
-    std::vector<char> r1, r2, r3;
     const size_t n = size_t(ll) * 16;
-    const bool ok = get_record(f, r1) && r1.size() == 4 && get_record(f, r2) && r2.size() == n &&
-                    get_record(f, r3) && r3.size() == n;
+    int32_t i4 = 0;
+    const bool ok = get_record_exact(f, &i4, 4) && get_record_exact(f, v1, n) && get_record_exact(f, v2, n);
     std::fclose(f);
     if (!ok) return fail(PNED_EINVAL, "pned_read_dsf_vectors: not a DSF vector file of this length");
-    int32_t i4 = 0;
-    std::memcpy(&i4, r1.data(), 4);
     *indx = i4;
-    std::memcpy(v1, r2.data(), n);
-    std::memcpy(v2, r3.data(), n);
     return PNED_OK;
 }

@@ -214,6 +214,59 @@ def test_vector_and_dsf_files_layout(tmp_path):
     assert sq == 0.5 - 0.25j and np.array_equal(sa2, sa) and np.array_equal(sb2, sb)
 
 
+def test_long_records_are_written_as_fortran_subrecords(tmp_path):
+    """Records longer than one subrecord (from N = 27 on, a vector is above
+    gfortran's 2^31 - 9 bytes) are split as gfortran splits them: each
+    subrecord framed by its length, the leading marker negative when another
+    follows, the trailing marker negative when one precedes.  A small limit
+    stands in for 2^31 - 9 bytes here."""
+    import struct
+
+    def subrecords(payload, limit):
+        out, off, n = b"", 0, len(payload)
+        while True:
+            k = min(limit, n - off)
+            lead = -k if off + k < n else k
+            tail = k if off == 0 else -k
+            out += struct.pack("<i", lead) + payload[off:off + k] + struct.pack("<i", tail)
+            off += k
+            if off >= n:
+                return out
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal(10) + 1j * rng.standard_normal(10)
+    v2 = rng.standard_normal(10) + 1j * rng.standard_normal(10)
+    try:
+        for limit in (48, 40, 160, 7):
+            P.api.set_max_subrecord(limit)
+            p = str(tmp_path / f"basisme{limit:05d}")
+            P.api.write_vec_data(p, 1.5, x)
+            want = subrecords(struct.pack("<d", 1.5), limit) + subrecords(x.astype("<c16").tobytes(), limit)
+            assert open(p, "rb").read() == want, limit
+            P.api.set_max_subrecord()
+            e, x2 = P.api.read_vec_data(p, 10)   # readers take any split
+            assert e == 1.5 and np.array_equal(x2, x)
+            with pytest.raises(P.PnedError):
+                P.api.read_vec_data(p, 9)
+        P.api.set_max_subrecord(64)
+        q = str(tmp_path / "vec_q00001me00000zz")
+        P.api.write_dsf_vectors(q, 7, x, v2)
+        assert open(q, "rb").read() == (subrecords(struct.pack("<i", 7), 64) + subrecords(x.astype("<c16").tobytes(), 64)
+                                        + subrecords(v2.astype("<c16").tobytes(), 64))
+        i, a, b = P.api.read_dsf_vectors(q, 10)
+        assert i == 7 and np.array_equal(a, x) and np.array_equal(b, v2)
+        # a trailing marker whose sign disagrees with the split is refused
+        raw = bytearray(open(q, "rb").read())
+        off = 12 + (4 + 64 + 4) + 4 + 64   # record 1, then the trailing marker of record 2's second subrecord
+        struct.pack_into("<i", raw, off, 64)
+        open(q, "wb").write(bytes(raw))
+        with pytest.raises(P.PnedError):
+            P.api.read_dsf_vectors(q, 10)
+        with pytest.raises(P.PnedError):
+            P.api.set_max_subrecord(0)
+    finally:
+        P.api.set_max_subrecord()
+
+
 def test_dsf_vectors_file_and_sq_line(tmp_path):
     import struct
 
