@@ -155,6 +155,9 @@ typedef struct {
                                     tile rows that keep >= 3 low global bits, else the plan uses 0 */
     int32_t blocks_per_sm; /* R = 1, j_bits 3: 3 builds the gather kernel for three resident blocks per SM
                               (85 registers, faster up to about 2^26 states); else two (the default) */
+    int32_t objective;     /* how a pass picks its tile bits: 0 (default) the fewest partner tiles; 1 the
+                              most flip terms inside the tile (each then gathers from shared memory instead
+                              of through L1/L2) and window bits that take the most terms into the pass */
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 /*

@@ -295,12 +295,12 @@ class ModelInput:
 
 
 def tile_plan_export(desc: "ModelInput", row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
-                     j_bits: int = -1, row_bits: int = 8) -> dict:
+                     j_bits: int = -1, row_bits: int = 8, objective: int = -1) -> dict:
     """The tile plan (S = 1/2 full basis) with row_bits row bits a tile (8: the
     single-vector plan Model.set_plan builds), computed on the host
     (pned_tile_plan_export): the program's flip terms and, per pass, the tile
     bits, outer order, terms and partner-tile groups."""
-    tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1)
+    tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1, int(objective))
     n = C.c_int64(0)
     check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), C.byref(tp), None, 0, C.byref(n)))
     buf = np.zeros(n.value, dtype=np.int64)
@@ -378,10 +378,11 @@ class Model:
         return bool(act.value)
 
     def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
-                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1):
+                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1,
+                 objective: int = -1):
         """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""
         tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles), int(blocks_per_sm))
+                            int(stage_partner_tiles), int(blocks_per_sm), int(objective))
         check(lib().pned_model_set_plan(self._h, int(R), C.byref(tp)))
         return self.plan(R)
 
@@ -762,9 +763,10 @@ class SlotBatch:
         return {"tile_passes": p.value, "partner_tiles": g.value, "tile_states": t.value}
 
     def set_plan(self, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
-                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1) -> dict:
+                 j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1,
+                 objective: int = -1) -> dict:
         tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles), int(blocks_per_sm))
+                            int(stage_partner_tiles), int(blocks_per_sm), int(objective))
         check(lib().pned_slots_set_plan(self._h, C.byref(tp)))
         return self.plan()
 

@@ -968,7 +968,8 @@ void build_tile_programs(pned_model *m)
     const int window = m->plan1.window_bits >= 0 ? m->plan1.window_bits : kTileWindowBits;
     const int mp = m->plan1.max_passes > 0 ? m->plan1.max_passes : kTileMaxPasses;
     const int jb = m->plan1.j_bits > 0 ? m->plan1.j_bits : 3;
-    if (hp.q == 2 && !hp.sector && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes) == PNED_OK) {
+    const int obj = m->plan1.objective > 0 ? m->plan1.objective : 0;
+    if (hp.q == 2 && !hp.sector && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes, obj) == PNED_OK) {
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
         m->tile_bps = (jb == 3 && m->plan1.blocks_per_sm == 3) ? 3 : tile_blocks_per_sm(jb);
@@ -1033,14 +1034,15 @@ bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan 
     while ((1 << lr) < R) ++lr;
     int window = std::max(4, 21 - lr - tbits - jb);
     int fixed = tbits;
-    int mp = kTileMaxPasses;
+    int mp = kTileMaxPasses, obj = 0;
     if (plan) {
         if (plan->row_fixed_bits >= 0) fixed = std::min(tbits, plan->row_fixed_bits);
         if (plan->window_bits >= 0) window = plan->window_bits;
         if (plan->max_passes > 0) mp = std::min(kTileMaxPasses, plan->max_passes);
+        if (plan->objective > 0) obj = plan->objective;
     }
     std::vector<HostProgram::TilePass> passes;
-    if (plan_tiles(hp, tbits, jb, fixed, window, mp, passes) != PNED_OK) return false;
+    if (plan_tiles(hp, tbits, jb, fixed, window, mp, passes, obj) != PNED_OK) return false;
     ts.progs = tile_programs(hp, passes, m->ntab);
     return true;
 }
@@ -1225,15 +1227,15 @@ extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *p
 {
     if (!m || pick_vpt(R) == 0) return fail(PNED_EINVAL, "pned_model_set_plan: bad arguments");
     if (plan && (plan->max_passes > kTileMaxPasses || plan->window_bits > 30 || plan->row_fixed_bits > 8 ||
-                 plan->j_bits > kTileMaxJB || plan->j_bits == 0))
+                 plan->j_bits > kTileMaxJB || plan->j_bits == 0 || plan->objective > 1))
         return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
     if (R == 1) {
-        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1, -1};
+        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1, -1, -1};
         m->carveout = m->plan1.l1_carveout != 0;
         build_tile_programs(m);
         return PNED_OK;
     }
-    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1};
     if (plan) m->carveout = plan->l1_carveout != 0;
     ensure_rtiles(m, R, false, plan ? plan : &def);
     return PNED_OK;

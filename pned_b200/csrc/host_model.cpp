@@ -502,12 +502,56 @@ int count_groups(const std::vector<uint32_t> &masks, uint32_t tm)
     return int(std::unique(parts.begin(), parts.end()) - parts.begin());
 }
 
+// Masks of the set that lie inside tile bits `tm`.
+int count_inside(const std::vector<uint32_t> &masks, uint32_t tm)
+{
+    int c = 0;
+    for (uint32_t m : masks) c += (m & ~tm) == 0;
+    return c;
+}
+
+// Tile bits that hold the most masks (objective 1): the `fixed` low bits, then
+// greedily the bit that brings the most masks inside (ties: the bit that the
+// most masks use), then pairwise exchanges while they bring more masks
+// inside, or as many with fewer partner tiles.
+uint32_t tile_most_inside(const std::vector<uint32_t> &masks, int n, int target, int fixed)
+{
+    uint32_t tm = (1u << fixed) - 1u;
+    for (int k = fixed; k < target; ++k) {
+        int best = -1, bi = -1, bu = -1;
+        for (int b = fixed; b < n; ++b) {
+            if (tm & (1u << b)) continue;
+            const int in = count_inside(masks, tm | (1u << b));
+            int u = 0;
+            for (uint32_t m : masks) u += (m >> b) & 1u;
+            if (in > bi || (in == bi && u > bu)) { bi = in; bu = u; best = b; }
+        }
+        tm |= 1u << best;
+    }
+    int in = count_inside(masks, tm), g = count_groups(masks, tm);
+    for (int round = 0; round < 32; ++round) {
+        bool better = false;
+        for (int a = fixed; a < n && !better; ++a) {
+            if (!(tm & (1u << a))) continue;
+            for (int b = fixed; b < n; ++b) {
+                if (tm & (1u << b)) continue;
+                const uint32_t t2 = (tm & ~(1u << a)) | (1u << b);
+                const int in2 = count_inside(masks, t2), g2 = count_groups(masks, t2);
+                if (in2 > in || (in2 == in && g2 < g)) { tm = t2; in = in2; g = g2; better = true; break; }
+            }
+        }
+        if (!better) break;
+    }
+    return tm;
+}
+
 // Tile bits for a set of masks: the `fixed` low bits, then tbits + jb - fixed
-// bits chosen to minimise the partner tiles (greedy, then pairwise exchanges
-// while they help); rows take the fixed bits and the lowest chosen ones, the
+// bits chosen to minimise the partner tiles (objective 0: greedy, then
+// pairwise exchanges while they help) or to hold the most masks (objective 1,
+// tile_most_inside); rows take the fixed bits and the lowest chosen ones, the
 // j bits the rest.  Outer order: bits most used by out-of-tile masks first.
-void choose_tile(const std::vector<uint32_t> &masks, int n, int tbits, int jb, int fixed, std::vector<int> &rowpos,
-                 std::vector<int> &jpos, std::vector<int> &outer, uint32_t &tilemask)
+void choose_tile(const std::vector<uint32_t> &masks, int n, int tbits, int jb, int fixed, int objective,
+                 std::vector<int> &rowpos, std::vector<int> &jpos, std::vector<int> &outer, uint32_t &tilemask)
 {
     const int target = tbits + jb;
     tilemask = (1u << fixed) - 1u;
@@ -516,7 +560,8 @@ void choose_tile(const std::vector<uint32_t> &masks, int n, int tbits, int jb, i
         for (uint32_t m : masks) if (m & (1u << b)) ++u;
         return u;
     };
-    for (int k = fixed; k < target; ++k) {
+    if (objective == 1) tilemask = tile_most_inside(masks, n, target, fixed);
+    for (int k = __builtin_popcount(tilemask); k < target; ++k) {
         int best = -1, bestg = 1 << 30, bestu = -1;
         for (int b = fixed; b < n; ++b) {
             if (tilemask & (1u << b)) continue;
@@ -527,7 +572,7 @@ void choose_tile(const std::vector<uint32_t> &masks, int n, int tbits, int jb, i
         tilemask |= 1u << best;
     }
     int g = count_groups(masks, tilemask);
-    for (int round = 0; round < 16; ++round) {
+    for (int round = 0; round < 16 && objective != 1; ++round) {
         bool better = false;
         for (int a = fixed; a < n && !better; ++a) {
             if (!(tilemask & (1u << a))) continue;
@@ -559,7 +604,7 @@ void choose_tile(const std::vector<uint32_t> &masks, int n, int tbits, int jb, i
 }  // namespace
 
 int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bits, int max_passes,
-               std::vector<HostProgram::TilePass> &passes)
+               std::vector<HostProgram::TilePass> &passes, int objective)
 {
     if (P.q != 2 || jb < 0 || jb > kTileMaxJB || tbits < 1 || tbits > 8 || fixed < 0 || fixed > tbits ||
         P.n < tbits + jb + 1)
@@ -573,9 +618,26 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
         for (int i : remaining) rm.push_back(P.xterms[i].xmask);
         std::vector<int> rowpos, jpos, outer;
         uint32_t tilemask;
-        choose_tile(rm, n, tbits, jb, fixed, rowpos, jpos, outer, tilemask);
+        choose_tile(rm, n, tbits, jb, fixed, objective, rowpos, jpos, outer, tilemask);
         uint32_t nearmask = tilemask;
-        for (int k = 0; k < window_bits && k < int(outer.size()); ++k) nearmask |= 1u << outer[k];
+        if (objective == 1) {
+            // window bits one by one: the bit that brings the most masks into the pass
+            // (ties: the bit that the most masks use)
+            for (int k = 0; k < window_bits; ++k) {
+                int best = -1, bi = -1, bu = -1;
+                for (int b = 0; b < n; ++b) {
+                    if (nearmask & (1u << b)) continue;
+                    const int in = count_inside(rm, nearmask | (1u << b));
+                    int u = 0;
+                    for (uint32_t m : rm) u += (m >> b) & 1u;
+                    if (in > bi || (in == bi && u > bu)) { bi = in; bu = u; best = b; }
+                }
+                if (best < 0) break;
+                nearmask |= 1u << best;
+            }
+        } else {
+            for (int k = 0; k < window_bits && k < int(outer.size()); ++k) nearmask |= 1u << outer[k];
+        }
         std::vector<int> take, rest;
         const bool last = int(passes.size()) + 1 >= max_passes;
         for (int i : remaining) {
@@ -586,7 +648,7 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
         // re-plan the tile for the masks of this pass only
         std::vector<uint32_t> tm;
         for (int i : take) tm.push_back(P.xterms[i].xmask);
-        choose_tile(tm, n, tbits, jb, fixed, rowpos, jpos, outer, tilemask);
+        choose_tile(tm, n, tbits, jb, fixed, objective, rowpos, jpos, outer, tilemask);
         HostProgram::TilePass pass;
         pass.tbits = tbits;
         pass.jb = jb;
@@ -653,7 +715,7 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
         pass.jb = jb;
         std::vector<int> rowpos, jpos, outer;
         uint32_t tilemask;
-        choose_tile({}, n, tbits, jb, fixed, rowpos, jpos, outer, tilemask);
+        choose_tile({}, n, tbits, jb, fixed, objective, rowpos, jpos, outer, tilemask);
         pass.rowpos = rowpos;
         for (int k = 0; k < kTileMaxJB; ++k) pass.jpos[k] = k < jb ? jpos[k] : 0;
         pass.outer = outer;
@@ -786,10 +848,10 @@ extern "C" int pned_tile_plan_export(const pned_model_desc *d, int row_bits, con
     int rc = compile_program(d, P);
     if (rc) return rc;
     if (P.q != 2 || P.sector) return fail(PNED_ENOTSUP, "pned_tile_plan_export: tiles are planned for the S = 1/2 full basis");
-    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1};
     const pned_tile_plan &pl = plan ? *plan : def;
     if (pl.max_passes > kTileMaxPasses || pl.window_bits > 30 || pl.row_fixed_bits > 8 || pl.j_bits > kTileMaxJB ||
-        pl.j_bits == 0)
+        pl.j_bits == 0 || pl.objective > 1)
         return fail(PNED_EINVAL, "pned_tile_plan_export: plan out of range");
     // the defaults of the model's own single-vector plan
     const int fixed = std::min(row_bits, pl.row_fixed_bits >= 0 ? pl.row_fixed_bits : 8);
@@ -797,7 +859,7 @@ extern "C" int pned_tile_plan_export(const pned_model_desc *d, int row_bits, con
     const int mp = pl.max_passes > 0 ? pl.max_passes : kTileMaxPasses;
     const int jb = pl.j_bits > 0 ? pl.j_bits : 3;
     std::vector<HostProgram::TilePass> passes;
-    rc = plan_tiles(P, row_bits, jb, fixed, window, mp, passes);
+    rc = plan_tiles(P, row_bits, jb, fixed, window, mp, passes, pl.objective > 0 ? pl.objective : 0);
     if (rc) return fail(rc, "pned_tile_plan_export: no tile plan for this model and plan");
     std::vector<int64_t> v;
     v.push_back(int64_t(P.xterms.size()));

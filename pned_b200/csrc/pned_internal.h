@@ -117,7 +117,7 @@ struct HostProgram {
 // Splits the flip masks into passes for the tiled kernels (q == 2,
 // n >= tbits + jb + 1).  A tile holds the states that agree on all bits but
 // its tbits row bits and jb j bits, chosen per pass to minimise the partner
-// tiles; the row bits include the global bits 0..fixed-1, so that a warp's
+// tiles (objective 0) or to hold the most masks (objective 1); the row bits include the global bits 0..fixed-1, so that a warp's
 // loads come in contiguous segments.  Each pass takes the masks whose partner
 // tiles lie within `window_bits` outer bits of its own tile order (so they are
 // found in L2), the last pass takes what is left.  In-tile terms carry the
@@ -129,7 +129,7 @@ struct HostProgram {
 // lowest sites, kept in every tile for contiguous runs of states).
 int plan_qtiles(const HostProgram &P, int k, int low, std::vector<QTilePass> &passes);
 int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bits, int max_passes,
-               std::vector<HostProgram::TilePass> &out);
+               std::vector<HostProgram::TilePass> &out, int objective = 0);
 
 // Coefficient tables and diagonal tables of `d` evaluated on the term
 // structure of S (same lattice and bonds; q == 2): table[i] for the entries of

@@ -18,7 +18,7 @@ import os
 
 from . import api
 
-# (row_fixed_bits, window_bits, max_passes[, j_bits[, l1_carveout, stage_partner_tiles, blocks_per_sm]]);
+# (row_fixed_bits, window_bits, max_passes[, j_bits[, l1_carveout, stage_partner_tiles, blocks_per_sm[, objective]]]);
 # -1 = the library default.  Three resident blocks per SM pay up to about 2^26 states,
 # 16-row tiles (j_bits 4) about 2^28.
 CANDIDATES_1 = [(8, 10, 4, 3), (8, 8, 2, 3), (8, 10, 1, 3), (5, 8, 1, 3), (5, 10, 2, 3), (5, 12, 2, 3),
@@ -26,7 +26,11 @@ CANDIDATES_1 = [(8, 10, 4, 3), (8, 8, 2, 3), (8, 10, 1, 3), (5, 8, 1, 3), (5, 10
                 (5, 12, 2, 2), (5, 10, 2, 2), (8, 10, 2, 2), (5, 13, 2, 2), (5, 12, 1, 2),
                 (5, 12, 2, 1), (5, 10, 2, 1), (8, 10, 2, 1), (5, 13, 2, 1),
                 (8, 8, 2, 3, 1, 0, 3), (5, 10, 2, 3, 1, 0, 3), (5, 11, 2, 3, 1, 0, 3), (8, 10, 4, 3, 1, 0, 3),
-                (5, 11, 2, 4), (5, 10, 2, 4), (4, 11, 2, 4)]
+                (5, 11, 2, 4), (5, 10, 2, 4), (4, 11, 2, 4),
+                # objective 1: tiles that hold the most flip terms
+                (5, 10, 2, 3, 1, 0, -1, 1), (5, 8, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1),
+                (5, 9, 2, 4, 1, 0, -1, 1), (5, 11, 2, 4, 1, 0, -1, 1), (5, 10, 2, 3, 1, 0, 3, 1),
+                (8, 8, 2, 3, 1, 0, -1, 1), (5, 10, 3, 4, 1, 0, -1, 1)]
 CANDIDATES_R = [(-1, -1, -1), (0, 6, 2), (0, 8, 2), (0, 10, 2), (1, 10, 2), (3, 10, 2), (0, 10, 1)]
 
 _cache: dict = {}

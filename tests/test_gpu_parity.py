@@ -391,11 +391,12 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
 @pytest.mark.parametrize("plan", [(8, 10, 4, 3, 1, 1), (5, 10, 2, 3, 1, 1), (3, 8, 1, 3, 1, 1), (5, 12, 2, 2, 1, 0),
                                   (5, 12, 2, 1, 0, 0), (8, 10, 4, 3, 1, 2), (5, 10, 2, 3, 1, 2), (3, 8, 1, 3, 1, 2),
                                   (5, 6, 3, 3, 1, 2), (8, 8, 2, 3, 1, 0, 3), (5, 10, 2, 3, 1, 0, 3),
-                                  (5, 8, 2, 4, 1, 0), (8, 10, 4, 4, 1, 0), (3, 6, 1, 4, 0, 0)])
+                                  (5, 8, 2, 4, 1, 0), (8, 10, 4, 4, 1, 0), (3, 6, 1, 4, 0, 0),
+                                  (5, 6, 2, 3, 1, 0, -1, 1), (5, 4, 2, 4, 1, 0, -1, 1), (5, 6, 2, 3, 1, 0, 3, 1)])
 def test_tile_plans_agree_with_oracle(plan):
     """Every tile plan the autotuner may pick (rows kept, window, passes, rows per
-    thread, carveout, staged or bulk-streamed partner tiles) gives the oracle's
-    H.v to 1e-12."""
+    thread, carveout, staged or bulk-streamed partner tiles, tiles that hold the
+    most terms) gives the oracle's H.v to 1e-12."""
     cl = honeycomb(2, 4)
     gm, om = models(cl, 2, 0, KHGH, FIELD)
     got = gm.set_plan(1, *plan)

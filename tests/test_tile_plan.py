@@ -93,7 +93,9 @@ MODELS = [
     ("slots", CP.slots(J1=0.4, K1=-0.3, I11=0.2, I12=-0.1, J1p=0.7, K1p=1.1, J1pp=-0.5, I11p=0.05, I12p=0.3,
                        I12pp=-0.2, J2=0.15, K2=0.25, I21=0.01, I22=0.02, J3=0.3, ratio_l=0.8), [0.01, 0.02, 0.03]),
 ]
-PLANS = [(8, 10, 4, 3), (5, 8, 2, 4), (3, 6, 1, 4), (5, 12, 2, 2), (5, 4, 3, 1), (0, 6, 3, 4), (8, 2, 4, 3)]
+# (row_fixed_bits, window_bits, max_passes, j_bits[, objective]); objective 1: tiles that hold the most terms
+PLANS = [(8, 10, 4, 3), (5, 8, 2, 4), (3, 6, 1, 4), (5, 12, 2, 2), (5, 4, 3, 1), (0, 6, 3, 4), (8, 2, 4, 3),
+         (5, 6, 2, 3, 1), (5, 4, 3, 4, 1), (8, 6, 2, 3, 1), (3, 8, 2, 2, 1)]
 
 
 @pytest.mark.parametrize("plan", PLANS, ids=[",".join(map(str, p)) for p in PLANS])
@@ -102,7 +104,7 @@ def test_tile_plan_index_arithmetic(name, cpl, fld, plan):
     cl = honeycomb(2, 4)
     X, skip, pt = P.build_xlocal(2, 0, cpl, field=fld)
     d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
-    out = api.tile_plan_export(d, *plan)
+    out = api.tile_plan_export(d, *plan[:4], objective=plan[4] if len(plan) > 4 else -1)
     assert 1 <= len(out["passes"]) <= plan[2]
     assert all(ps["jb"] == plan[3] for ps in out["passes"])
     check_plan(cl.n, out, plan[0])
@@ -227,6 +229,31 @@ def test_every_tuner_candidate_plans_the_n30_model():
     d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
     for c in tune.CANDIDATES_1:
         jb = c[3] if len(c) > 3 else -1
-        r = api.tile_plan_export(d, c[0], c[1], c[2], jb)
+        r = api.tile_plan_export(d, c[0], c[1], c[2], jb, objective=c[7] if len(c) > 7 else -1)
         assert 1 <= len(r["passes"]) <= c[2]
         assert sum(len(ps["terms"]) for ps in r["passes"]) == 45
+
+
+def test_most_terms_objective_n30():
+    """Objective 1 at N = 30 (the measured Kitaev-Heisenberg model): the tiles
+    take the rings of low sites, so more of the 45 flip terms gather from
+    shared memory -- 13 + 9 with 8 rows a thread, 15 + 10 with 16 -- than the
+    fewest-partner-tile plan's 6 + 0, and the terms left to gather through
+    L1/L2 drop from 39 to 23 and 20; every term still in exactly one pass (the
+    index arithmetic is checked for every state, here on an 18-site copy of the
+    plan shape)."""
+    import math
+    from pned_b200.lattice import cluster_for_sites
+    cl = cluster_for_sites(30)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi)))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    base = api.tile_plan_export(d, 5, 12, 2, 3)
+    assert [ps["nin"] for ps in base["passes"]] == [6, 0]
+    for plan, nin in (((5, 10, 2, 3), [13, 9]), ((5, 10, 2, 4), [15, 10])):
+        r = api.tile_plan_export(d, *plan, objective=1)
+        assert [ps["nin"] for ps in r["passes"]] == nin
+        assert sum(len(ps["terms"]) for ps in r["passes"]) == 45
+        assert r["passes"][0]["rowpos"][:5] == [0, 1, 2, 3, 4]
+    c18 = cluster_for_sites(18)
+    d18 = P.ModelInput(c18.n, 2, 0, c18.ipair, c18.ibond_type, X, skip, pt)
+    check_plan(c18.n, api.tile_plan_export(d18, 5, 6, 2, 3, objective=1), 5)
