@@ -125,45 +125,17 @@ def build_model(n_sites=30, R=1):
 TILE_KERNELS = {0: "hv_tile_kernel", 1: "hv_tile_stage_kernel", 2: "hv_tile_bulk_kernel"}
 
 
-class CpuSample:
-    """Reference CPU algorithm on a bounded sample of the workload: one Lanczos
-    step's p_mltply_v3 restricted to 2^slice_log2 output states (all bond x
-    element passes, gathering from a full-size input vector) plus the step's
-    vector updates on the same slice; a sample's time is scaled to the whole
-    basis."""
-
-    def __init__(self, n_sites: int, threads: int, slice_log2: int = 24):
-        import numpy as np
-        from oracle import oracle as O
-        from pned_b200 import couplings as CP
-        from pned_b200.lattice import cluster_for_sites
-        self.O = O
-        O.set_num_threads(threads)
-        cl = cluster_for_sites(n_sites)
-        cpl = CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi))
-        X = O.xlocal(2, 0, cpl)
-        skip, _, pt = O.parity_skip(2, 0, X)
-        self.om = O.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
-        self.D = self.om.ldim
-        self.v1 = O.gaussian(SEED, self.D)          # full-size gather source
-        self.hi = 1 << min(slice_log2, n_sites)
-        self.v0 = np.zeros(self.hi, dtype=np.complex128)
-        self.scale = self.D / self.hi
-        self.desc = (f"p_mltply_v3 (all {self.om.nbond * 4} bond x element passes) + the step's vector updates "
-                     f"over 2^{int(math.log2(self.hi))} of the 2^{n_sites} output states, full-size input vector, "
-                     f"time scaled x{int(self.scale)}")
-
-    def step_seconds(self) -> float:
-        O = self.O
-        self.v0[:] = 0
-        t0 = time.perf_counter()
-        self.om.p_mltply_v3_slice(self.v1, self.v0, 0, self.hi)
-        # swap (4 vector passes) + calc_beta (2 passes) on the slice
-        a = self.v1[:self.hi]
-        tmp = (self.v0 - 0.5 * a) / 1.5
-        self.v0[:] = -1.5 * a
-        O.inprdct(tmp, tmp)
-        return (time.perf_counter() - t0) * self.scale
+def cpu_step_timing(n_sites: int, threads: int, samples: int, warmup: int, full: int, slice_log2: int) -> dict:
+    """The reference CPU algorithm (the oracle port of parallelized_lnc1z's step)
+    timed by oracle/cpu_step.py in a process of its own, so that torch's OpenMP
+    threads do not share the cores with the oracle's: `samples` bounded samples
+    (one step on 2^slice_log2 output states, scaled) and `full` whole steps."""
+    cmd = [sys.executable, "-m", "oracle.cpu_step", "--n-sites", str(n_sites), "--threads", str(threads),
+           "--samples", str(samples), "--warmup", str(warmup), "--full", str(full), "--slice-log2", str(slice_log2)]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    out = subprocess.run(cmd, cwd=os.path.dirname(os.path.abspath(__file__)), env=env, capture_output=True, text=True,
+                         check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
 
 
 def replica_aggregate(ms_local: float, steps: int, world: int, device="cuda"):
@@ -181,21 +153,26 @@ def replica_aggregate(ms_local: float, steps: int, world: int, device="cuda"):
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference CPU algorithm, timed on the host cores."""
+    """--impl reference: the reference CPU algorithm, timed on the host cores --
+    args.steps bounded samples (after args.warmup) and one whole step."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    cs = CpuSample(args.n_sites, threads, slice_log2=args.ref_slice_log2)
-    for _ in range(args.warmup):
-        cs.step_seconds()
-    secs = [cs.step_seconds() for _ in range(args.steps)]
-    value = args.steps / sum(secs)
+    t = cpu_step_timing(args.n_sites, threads, args.steps, args.warmup, args.ref_full_steps, args.ref_slice_log2)
+    sampled = len(t["sample_step_s"]) / sum(t["sample_step_s"])
+    full = len(t["full_step_s"]) / sum(t["full_step_s"]) if t["full_step_s"] else None
+    value = full if full is not None else sampled
+    sample = (f"{len(t['full_step_s'])} whole Lanczos step(s) over all 2^{args.n_sites} states timed as they are "
+              f"(value); beside them {len(t['sample_step_s'])} bounded samples: {t['sample']}")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128", "data": "synthetic (seeded complex Gaussian)", "impl": "reference",
         "config": workload_config(args.n_sites),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": cs.desc},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "cpu": t["cpu"], "full_steps_executed": len(t["full_step_s"]),
+                         "full_step_s": t["full_step_s"], "sampled_steps_executed": len(t["sample_step_s"]),
+                         "sampled_value": sampled, "sample_step_s": t["sample_step_s"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -353,12 +330,12 @@ def run_ours(args, rank, world, local_rank):
             line["dense_check"] = {"error": str(exc)}
     if rank == 0 and args.cpu_baseline:
         try:
-            cs = CpuSample(args.n_sites, os.cpu_count() or 1, slice_log2=args.ref_slice_log2)
-            cs.step_seconds()
-            secs = [cs.step_seconds() for _ in range(3)]
-            line["cpu_baseline"] = {"value": 3 / sum(secs), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                    "sample": cs.desc + "; mean of 3 samples after 1 warm-up"}
-            del cs
+            threads = os.cpu_count() or 1
+            t = cpu_step_timing(args.n_sites, threads, 3, 1, 0, args.ref_slice_log2)
+            line["cpu_baseline"] = {"value": len(t["sample_step_s"]) / sum(t["sample_step_s"]), "unit": UNIT,
+                                    "cores": threads, "kind": "port", "cpu": t["cpu"],
+                                    "sample": t["sample"] + "; mean of 3 samples after 1 warm-up, in a process "
+                                              "without torch"}
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
     # the batched and served workloads are one-GPU measurements beside the headline
@@ -368,7 +345,8 @@ def run_ours(args, rank, world, local_rank):
         model.close()
         torch.cuda.empty_cache()
         if args.batched:
-            line["batched"] = {"tpq": batched_tpq(dev, args), "dsf": batched_dsf(dev, args)}
+            line["batched"] = {"tpq": batched_tpq(dev, args), "dsf": batched_dsf(dev, args),
+                               "by_size": batch_table(dev, args)}
         if args.served:
             line["served"] = served_section(args, local_rank, args.served_requests, args.served_rate)
     if rank == 0:
@@ -430,6 +408,42 @@ def batched_tpq(dev, args):
     out["vs_plain"] = out["vector_steps_per_s"] / out["plain_vector_steps_per_s"]
     m.close()
     return out
+
+
+def batch_table(dev, args, sizes=(18, 20, 22, 24, 26), widths=(1, 4, 16), steps=None):
+    """mTPQ steps (KH + Gamma 0.1 + h 0.05 [111], l = 2) per lattice size N and
+    batch width R: vector-steps/s of R interleaved vectors in one session
+    against R = 1 (the plain path, one vector at a time)."""
+    import torch
+    import pned_b200 as P
+    from pned_b200 import couplings as CP
+    from pned_b200.lattice import cluster_for_sites
+    from pned_b200.tune import autotune
+    rows = []
+    for n in sizes:
+        cl = cluster_for_sites(n)
+        L = 2.0 * cl.n
+        m = P.Model.from_couplings(cl, _kh(0.1), field=CP.field_111(0.05), tps_L=L)
+        plain = None
+        for R in widths:
+            autotune(m, R)
+            st = torch.cuda.Stream(device=dev)
+            ctx = P.Context(m, R=R, stream=st)
+            v = torch.empty(m.dim * R, dtype=torch.complex128, device=dev)
+            ctx.fill_gaussian(SEED, v)
+            k = steps or max(10, min(200, int(2 ** 26 / (m.dim * R)) * 4))
+            ms, _ = _timed_session(ctx, st, "tps", v, 3, k, L=L)
+            vps = 1000.0 * R / ms
+            if R == 1:
+                plain = vps
+            rows.append({"n_sites": n, "R": R, "ms_per_step": ms, "vector_steps_per_s": vps,
+                         "vs_plain": vps / plain if plain else None, "steps_timed": k, "plan": m.plan(R)})
+            ctx.close()
+            del v
+            torch.cuda.empty_cache()
+        m.close()
+    return {"workload": "mTPQ steps, S=1/2 KH+Gamma=0.1+h=0.05[111] honeycomb, l=2.0, complex128, R interleaved "
+                        "vectors [D][R] in one session; R=1 is the plain path", "rows": rows}
 
 
 def batched_dsf(dev, args):
@@ -713,10 +727,11 @@ def main():
     ap.add_argument("--n-sites", type=int, default=30)
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--ref-slice-log2", type=int, default=24)
+    ap.add_argument("--ref-full-steps", type=int, default=1, help="--impl reference: whole steps timed")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
-    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1", "sector"])
+    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1", "sector", "batch"])
     ap.add_argument("--sector-sites", type=int, default=30)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits[,l1_carveout[,stage]]' "
@@ -757,6 +772,12 @@ def main():
             run_s1(args, rank, world, local_rank)
         elif args.workload == "sector":
             run_sector(args, rank, world, local_rank)
+        elif args.workload == "batch":
+            if rank == 0:
+                import torch
+                torch.cuda.set_device(local_rank)
+                print(json.dumps({"batched": {"by_size": batch_table(torch.device("cuda", local_rank), args)}}),
+                      flush=True)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -83,6 +83,8 @@ def lib():
         L.oracle_normalization_dsf.argtypes = [C.c_int, C.c_double, C.c_double, c_dbl_p]
         L.oracle_inverse_iteration.argtypes = [vp, C.c_double, vp, vp, C.c_int, C.c_int, c_int_p, c_int_p]
         L.oracle_lanczos_vector.argtypes = [vp, vp, C.c_int, c_dbl_p, c_dbl_p, c_dbl_p, vp]
+        L.oracle_lanczos_step.argtypes = [vp, vp, vp, c_dbl_p, c_dbl_p]
+        L.oracle_lanczos_step_slice.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, c_dbl_p, c_dbl_p]
         L.oracle_gaussian.argtypes = [C.c_uint64, C.c_int64, C.c_int, vp]
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_num_threads.argtypes = [C.c_int]
@@ -260,6 +262,20 @@ class Model:
         pr = np.zeros(1, dtype=np.complex128)
         lib().oracle_p_mltply_v3_slice(self._h, _p(v1), _p(v0_slice), eperbd, lo, hi, _p(pr))
         return complex(pr[0])
+
+    def lanczos_step(self, v1, v0, alpha, beta):
+        """One step of the Lanczos loop on (v1, v0) in place: the swap with the
+        previous alpha/beta, then p_mltply_v3 and calc_beta; returns (alpha, beta)."""
+        a, b = C.c_double(alpha), C.c_double(beta)
+        lib().oracle_lanczos_step(self._h, _p(v1), _p(v0), C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def lanczos_step_slice(self, v1, v0_slice, lo, hi, alpha, beta):
+        """The same step on the output states [lo, hi) (v0_slice holds them);
+        returns the slice's parts (alpha, sqrt of the beta sum)."""
+        a, b = C.c_double(alpha), C.c_double(beta)
+        lib().oracle_lanczos_step_slice(self._h, _p(v1), _p(v0_slice), lo, hi, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def lanczos(self, v1, nsteps, check_conv=False):
         v = _c128(v1).copy()

@@ -868,6 +868,51 @@ int oracle_lanczos(const omodel *m, cplx *v1, int nsteps, int check_conv, double
 }
 
 /*
+ * One step of parallelized_lnc1z's loop (S_one_half/Hybrid_TPS_Lanczos.f90:
+ * 111-122): the swap with the previous step's alpha/beta (in *alpha, *beta),
+ * then p_mltply_v3 and calc_beta; *alpha, *beta receive the new values.  The
+ * CPU timing of a whole step at full size calls this.
+ */
+void oracle_lanczos_step(const omodel *m, cplx *v1, cplx *v0, double *alpha, double *beta)
+{
+    const int64_t ldim = m->ldim;
+    const double a = *alpha, b = *beta;
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < ldim; ++j) {
+        cplx temp1 = v1[j];
+        cplx temp2 = (v0[j] - a * v1[j]) / b;
+        v0[j] = -b * temp1;
+        v1[j] = temp2;
+    }
+    calc_alpha_beta(m, alpha, beta, v1, v0);
+}
+
+/*
+ * The same step restricted to the output states [lo, hi) (a bounded sample
+ * of a step): the swap on the slice of v1 and of v0s (v0s holds states lo ..
+ * hi-1), p_mltply_v3 on the slice gathering from the whole v1, and calc_beta on
+ * the slice.  *alpha receives the slice's part of Re prdct, *beta the square
+ * root of the slice's part of calc_beta's sum.
+ */
+void oracle_lanczos_step_slice(const omodel *m, cplx *v1, cplx *v0s, int64_t lo, int64_t hi, double *alpha,
+                               double *beta)
+{
+    const double a = *alpha, b = *beta;
+#pragma omp parallel for schedule(static)
+    for (int64_t j = lo; j < hi; ++j) {
+        cplx temp1 = v1[j];
+        cplx temp2 = (v0s[j - lo] - a * v1[j]) / b;
+        v0s[j - lo] = -b * temp1;
+        v1[j] = temp2;
+    }
+    cplx pr;
+    oracle_p_mltply_v3_slice(m, v1, v0s, 0.0, lo, hi, &pr);
+    const double bb = oracle_calc_beta(hi - lo, pr, v1 + lo, v0s);
+    *alpha = creal(pr);
+    *beta = sqrt(bb);
+}
+
+/*
  * Eigenvector by the Lanczos method, parallelized_lncv1z
  * (S_one_half/Hybrid_TPS_Lanczos.f90:183-329): the chain of the initial
  * vector is replayed with the alpha/beta stored by the first pass and
