@@ -160,7 +160,18 @@ __global__ void __launch_bounds__(kThreads, BPS)
     uint32_t rowbase = 0;   // the thread's row on its global bits
 #pragma unroll
     for (int k = 0; k < 8; ++k) rowbase |= ((tid >> k) & 1u) << prog.rowpos[k];
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // dynamic order: the block's next tile comes from the pass's counter (taken by
+    // thread 0 during the current tile, read after the tile's last barrier)
+    __shared__ uint32_t s_next;
+    __shared__ double2 s_red[kThreads / 32][K];
+    uint32_t *const ctr = a.tile_counter ? a.tile_counter + prog.pass : nullptr;
+    int64_t tile = blockIdx.x;
+    if (ctr) {
+        if (tid == 0) s_next = atomicAdd(ctr, 1u);
+        __syncthreads();
+        tile = s_next;
+    }
+    while (tile < ntiles) {
         uint32_t base = rowbase;
         for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
         double2 acc[SPT];
@@ -169,7 +180,10 @@ __global__ void __launch_bounds__(kThreads, BPS)
             double2 v[CH];
 #pragma unroll
             for (int jj = 0; jj < CH; ++jj) v[jj] = __ldg(a.C + (base | prog.jexp[j0 + jj]));
-            if (j0 == 0) __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+            if (j0 == 0) {
+                __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+                if (ctr && tid == 0) s_next = atomicAdd(ctr, 1u);   // every thread has read s_next
+            }
 #pragma unroll
             for (int jj = 0; jj < CH; ++jj) s_v[tid + kThreads * (j0 + jj)] = v[jj];
 #pragma unroll
@@ -274,8 +288,30 @@ __global__ void __launch_bounds__(kThreads, BPS)
                 red[3][0] = cadd(red[3][0], cconjmul(gv, vv));
             }
         }
+        if (!ctr) {
+            tile += gridDim.x;
+            continue;
+        }
+        // the tile's sums (fixed order: lanes, then warps), written at the tile's slot,
+        // so that the total does not depend on which block took which tile
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            for (int off = 16; off >= 1; off >>= 1) {
+                red[k][0].x += __shfl_xor_sync(0xffffffffu, red[k][0].x, off);
+                red[k][0].y += __shfl_xor_sync(0xffffffffu, red[k][0].y, off);
+            }
+            if ((tid & 31u) == 0) s_red[tid >> 5][k] = red[k][0];
+            red[k][0] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        if (tid < uint32_t(K)) {
+            double2 sum = make_double2(0.0, 0.0);
+            for (int w = 0; w < kThreads / 32; ++w) sum = cadd(sum, s_red[w][tid]);
+            a.partials[size_t(tile) * K + tid] = sum;
+        }
+        tile = s_next;
     }
-    block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
+    if (!ctr) block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
 }
 
 // Tiled multi-vector H.V (R > 1 interleaved vectors, S = 1/2 full basis), one
@@ -680,9 +716,15 @@ static cudaError_t launch_tile_j(const pned_model *m, const HvArgs &a, int nbloc
         e = set_carveout(reinterpret_cast<const void *>(kern), m->device, m->tile_smem, BPS);
     if (e != cudaSuccess) return e;
     const int grid = tile_grid(m, nblocks);
+    const bool dyn = tile_dynamic(m, a);
     HvArgs b = a;
+    if (!dyn) b.tile_counter = nullptr;
+    else if ((e = cudaMemsetAsync(a.tile_counter, 0, sizeof(uint32_t) * kTileMaxPasses, st)) != cudaSuccess)
+        return e;
+    size_t off = 0;
     for (size_t p = 0; p < m->tprogs.size(); ++p) {
-        b.partials = a.partials + size_t(p) * grid * K * a.R;
+        b.partials = a.partials + off;
+        off += dyn ? (size_t(1) << m->tprogs[p]->nouter) * K : size_t(grid) * K * a.R;
         kern<<<grid, kThreads, m->tile_smem, st>>>(*m->tprogs[p], b);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -828,6 +870,25 @@ static cudaError_t launch_rv(const pned_model *m, const pned_model::TileSet &ts,
     return cudaErrorInvalidValue;
 }
 
+int64_t tile_dynamic_partials(const pned_model *m)
+{
+    int64_t n = 0;
+    for (const auto &t : m->tprogs) n += int64_t(1) << t->nouter;
+    return n;
+}
+
+bool tile_dynamic(const pned_model *m, const HvArgs &a)
+{
+    if (!a.tile_counter || a.R != 1 || m->tprogs.empty() || !m->use_tile || tile_staged(m)) return false;
+    return tile_dynamic_partials(m) * a.K <= a.partials_cap;
+}
+
+int64_t hv_partials(const pned_model *m, const HvArgs &a, int nblocks)
+{
+    if (tile_dynamic(m, a)) return tile_dynamic_partials(m);
+    return hv_partial_blocks(m, a.R, nblocks);
+}
+
 int hv_partial_blocks(const pned_model *m, int R, int nblocks)
 {
     if (!m->tprogs.empty() && R == 1 && m->use_tile) return int(m->tprogs.size()) * tile_grid(m, nblocks);
@@ -941,6 +1002,7 @@ static std::vector<std::unique_ptr<TileProgram>> tile_programs(const HostProgram
         T->nouter = int(ps.outer.size());
         T->first = p == 0;
         T->last = p + 1 == passes.size();
+        T->pass = int(p);
         for (int j = 0; j < (1 << ps.jb); ++j) {
             uint32_t e = 0;
             for (int k = 0; k < ps.jb; ++k) if ((j >> k) & 1) e |= 1u << ps.jpos[k];
@@ -1295,9 +1357,17 @@ extern "C" int pned_ctx_create(pned_model *m, int R, size_t budget, pned_ctx **o
     // tiled kernels write one partial sum per block and pass
     if (R > 1) ensure_rtiles(m, R, false, nullptr);
     ensure_qtiles(m, R);
-    const size_t pbytes =
-        sizeof(double2) * size_t(c->nblocks) * std::max(kTileMaxPasses, kQTileMaxPasses) * kMaxK * kMaxR;
+    // room for per-block sums, and for R = 1 for the per-tile sums of the dynamic tile
+    // order: the current plan, or any plan of two passes with tiles of >= 2048 states
+    size_t pslots = size_t(c->nblocks) * std::max(kTileMaxPasses, kQTileMaxPasses) * kMaxK * kMaxR;
+    if (R == 1 && m->use_tile) {
+        pslots = std::max<size_t>(pslots, size_t(tile_dynamic_partials(m)) * kMaxK);
+        pslots = std::max<size_t>(pslots, size_t(m->dim / 2048) * 2 * kMaxK);
+    }
+    const size_t pbytes = sizeof(double2) * pslots;
+    c->partials_cap = int64_t(pslots);
     e = cudaMalloc(&c->partials, pbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->tile_ctr, sizeof(uint32_t) * kTileMaxPasses);
     if (e == cudaSuccess) e = cudaMalloc(&c->sums, sizeof(double2) * kMaxK * kMaxR * 4);
     if (e == cudaSuccess) e = cudaMalloc(&c->scal, sizeof(double) * kScalSlots * kMaxR);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_sums, sizeof(double2) * kMaxK * kMaxR * 4);
@@ -1324,6 +1394,7 @@ extern "C" int pned_ctx_destroy(pned_ctx *c)
     session_release(c);
     for (int k = 0; k < kMaxBuffers; ++k) cudaFree(c->buf[k]);
     cudaFree(c->partials);
+    cudaFree(c->tile_ctr);
     cudaFree(c->sums);
     cudaFree(c->scal);
     cudaFree(c->flag);
@@ -1438,9 +1509,10 @@ extern "C" int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double e
     a.table = c->m->d_table; a.partials = c->partials;
     a.dim = c->m->dim; a.R = c->R; a.K = 1;
     a.err = c->flag;
+    ctx_tile_args(c, a);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (e == cudaSuccess)
-        e = launch_finish(c->partials, hv_partial_blocks(c->m, c->R, c->nblocks), c->R, c->sums, c->stream);
+        e = launch_finish(c->partials, int(hv_partials(c->m, a, c->nblocks)), c->R, c->sums, c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pned_hv launch");
     if (!(flags & PNED_PTR_DEVICE)) {
         e = cudaMemcpyAsync(v0, dv0, sizeof(double2) * size_t(c->m->dim) * c->R, cudaMemcpyDeviceToHost, c->stream);

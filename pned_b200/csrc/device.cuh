@@ -103,7 +103,9 @@ struct pned_ctx {
     int nsm = 148, nblocks = 1;
     cudaStream_t stream = nullptr, own_stream = nullptr;
     double2 *buf[pned::kMaxBuffers] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    double2 *partials = nullptr;   // [nblocks][kMaxK][kMaxR]
+    double2 *partials = nullptr;   // [nblocks][kMaxK][kMaxR], or per-tile sums of the single-vector tile kernel
+    int64_t partials_cap = 0;      // double2 slots at `partials`
+    uint32_t *tile_ctr = nullptr;  // [kTileMaxPasses] tile counters of the dynamic tile order
     double2 *sums = nullptr;       // [4][kMaxK*kMaxR]
     double *scal = nullptr;        // [kScalSlots][kMaxR]
     int *flag = nullptr;
@@ -179,8 +181,22 @@ cudaError_t launch_sector(const pned_model *m, const HvArgs &a, int nblocks, cud
 inline bool tile_staged(const pned_model *m) { return m->tile_stage == 2 || (m->tile_stage == 1 && m->tile_jb == 3); }
 // All passes of the staged single-vector tile kernel (cp.async or bulk copies).
 cudaError_t launch_tile_staged(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
-// Number of partial-sum blocks launch_hv writes for this model, R and grid.
+// Number of partial-sum blocks launch_hv writes for this model, R and grid
+// (static tile order).
 int hv_partial_blocks(const pned_model *m, int R, int nblocks);
+// Tiles of all passes of the single-vector tile plan (the per-tile sums of the dynamic order).
+int64_t tile_dynamic_partials(const pned_model *m);
+// True when launch_hv runs the single-vector tile kernel in dynamic tile order
+// for these arguments (tile counters given and room for the per-tile sums).
+bool tile_dynamic(const pned_model *m, const HvArgs &a);
+// Partial sums launch_hv writes for these arguments (per tile or per block).
+int64_t hv_partials(const pned_model *m, const HvArgs &a, int nblocks);
+// The context's tile counters and partial-sum capacity into a.
+inline void ctx_tile_args(const pned_ctx *c, HvArgs &a)
+{
+    a.tile_counter = c->tile_ctr;
+    a.partials_cap = c->partials_cap;
+}
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st);
 cudaError_t launch_dot(const pned_ctx *c, const double2 *x1, const double2 *x2, const double2 *alpha, int mode,
                        double2 *out, cudaStream_t st);

@@ -67,6 +67,7 @@ struct QTileProgram {
 struct TileProgram {
     int n, tbits, jb, nin, nterms, ntab, nouter;
     int first, last;                  // pass flags: first adds diagonal and P, last forms the K >= 2 sums
+    int pass;                         // index of the pass (its tile counter under dynamic tile order)
     uint32_t jexp[1 << kTileMaxJB];   // global bits of the thread's j-th state
     uint8_t rowpos[8];                // row bit k -> global bit rowpos[k]
     uint8_t outer[32];                // tile-id bit k -> global bit outer[k]
@@ -100,6 +101,13 @@ struct HvArgs {
     // tiled multi-vector kernel only: per-vector coefficient tables ([ntab][R])
     // and real diagonals ([dim][R]) instead of shared ones
     int slot_tables;
+    // tiled single-vector kernel only: per-pass tile counters, zeroed before the
+    // passes; when set, blocks take tiles in order from the counter (all blocks
+    // stay on neighbouring tiles, so the L2 window holds) and the sums are
+    // written per tile ([tile][K]) instead of per block.  Null: the static
+    // order (tile = block + k * grid) with per-block sums.
+    uint32_t *tile_counter;
+    int64_t partials_cap;   // double2 slots available at `partials` (per-tile sums need sum(tiles) * K)
     // Sz sector (set by launch_hv from the model): index -> state, and the Lin
     // tables, state -> index = lin_lo[state mod lin_mod] + lin_hi[state / lin_mod] - 1
     const int64_t *list1;

@@ -289,11 +289,12 @@ static cudaError_t lanczos_step(pned_ctx *c, Session &S, bool first)
     a.R = R;
     a.K = 1;
     a.err = c->flag;
+    ctx_tile_args(c, a);
     double2 *sa = c->sums, *sb = c->sums + kMaxK * kMaxR;
     if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
-    if (e == cudaSuccess) e = launch_finish(c->partials, hv_partial_blocks(c->m, R, c->nblocks), R, sa, c->stream);
+    if (e == cudaSuccess) e = launch_finish(c->partials, int(hv_partials(c->m, a, c->nblocks)), R, sa, c->stream);
     if (e == cudaSuccess)
         e = launch_residual(c, c->buf[S.b2], c->buf[S.b0], c->buf[S.b1], slot(c, kSlotSc), sa, c->stream);
     if (e == cudaSuccess) e = launch_finish(c->partials, c->nblocks, R, sb, c->stream);
@@ -320,11 +321,12 @@ static cudaError_t tps_step(pned_ctx *c, Session &S, bool first)
     a.G = first ? nullptr : c->buf[S.b2]; a.gsc = slot(c, kSlotGsc);
     a.dim = c->m->dim; a.R = R; a.K = 4;
     a.err = c->flag;
+    ctx_tile_args(c, a);
     if (S.ev_hv0) cudaEventRecord(S.ev_hv0, c->stream);
     cudaError_t e = launch_hv(c->m, a, c->nblocks, c->stream);
     if (S.ev_hv1) cudaEventRecord(S.ev_hv1, c->stream);
     if (e == cudaSuccess)
-        e = launch_finish(c->partials, hv_partial_blocks(c->m, R, c->nblocks), 4 * R, c->sums, c->stream);
+        e = launch_finish(c->partials, int(hv_partials(c->m, a, c->nblocks)), 4 * R, c->sums, c->stream);
     if (first && e == cudaSuccess) e = cudaMemsetAsync(c->sums + 2 * R, 0, sizeof(double2) * 2 * R, c->stream);
     for (int o = 0; o < S.nobs && e == cudaSuccess; ++o) {
         const DevObs &ob = S.obs[o];
@@ -816,6 +818,7 @@ extern "C" int pned_lanczos_vector(pned_ctx *c, const pned_c128 *v_init, int n_s
         a.diag = c->m->d_diag; a.shift = 0.0;
         a.table = c->m->d_table; a.partials = c->partials;
         a.dim = n; a.R = 1; a.K = 1; a.err = c->flag;
+        ctx_tile_args(c, a);
         e = launch_hv(c->m, a, nb, c->stream);
         if (e != cudaSuccess) break;
         lncv_kernel<<<nb, kThreads, 0, c->stream>>>(W, Cb, Pb, x, slot(c, kSlotSc), alpha[k], coef[k], n);
@@ -885,6 +888,7 @@ extern "C" int pned_cg_run(pned_ctx *c, double E, const pned_c128 *b_init, int i
             a.table = c->m->d_table; a.partials = c->partials;
             a.dim = n; a.R = 1; a.K = 1;
             a.err = c->flag;
+            ctx_tile_args(c, a);
             e = launch_hv(c->m, a, nb, c->stream);
             if (e != cudaSuccess) return cuda_fail(e, "cg hv");
             double2 crp, cyp, rc1, rc2;
