@@ -339,7 +339,7 @@ def run_ours(args, rank, world, local_rank):
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
     # the batched and served workloads are one-GPU measurements beside the headline
-    if world == 1 and (args.batched or args.served):
+    if world == 1 and (args.batched or args.served or args.configs):
         del v
         ctx.close()
         model.close()
@@ -347,6 +347,8 @@ def run_ours(args, rank, world, local_rank):
         if args.batched:
             line["batched"] = {"tpq": batched_tpq(dev, args), "dsf": batched_dsf(dev, args),
                                "by_size": batch_table(dev, args)}
+        if args.configs:
+            line["configs"] = configs_section(dev, args)
         if args.served:
             line["served"] = served_section(args, local_rank, args.served_requests, args.served_rate)
     if rank == 0:
@@ -362,7 +364,8 @@ def _timed_session(ctx, st, kind, v, warm, steps, L=0.0):
     """Times `steps` session steps on the context's stream `st` (CUDA events)."""
     import torch
     ctx.session_begin(kind, v, warm + steps + 1, L=L)
-    ctx.session_step(warm)
+    if warm > 0:
+        ctx.session_step(warm)
     ctx.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -444,6 +447,99 @@ def batch_table(dev, args, sizes=(18, 20, 22, 24, 26), widths=(1, 4, 16), steps=
         m.close()
     return {"workload": "mTPQ steps, S=1/2 KH+Gamma=0.1+h=0.05[111] honeycomb, l=2.0, complex128, R interleaved "
                         "vectors [D][R] in one session; R=1 is the plain path", "rows": rows}
+
+
+def configs_section(dev, args):
+    """The other configurations as they are stated: config 0 (N=24 Lanczos, 300
+    steps, E0 and the eigenvector's residual), config 1 (N=24 mTPQ, R=16, 2000
+    steps, E(T) and C(T) of eval_mpi over the 16 seeds) and config 3 (S=1 N=18:
+    a 300-step Lanczos E0 and mTPQ with R=4; of its 1500 steps a bounded number
+    is timed, the rest projected)."""
+    import numpy as np
+    import torch
+    import pned_b200 as P
+    from pned_b200 import couplings as CP
+    from pned_b200.lattice import cluster_for_sites
+    from pned_b200.tune import autotune
+    out = {}
+    # config 0
+    cl = cluster_for_sites(24)
+    m = P.Model.from_couplings(cl, _kh())
+    autotune(m, 1)
+    st = torch.cuda.Stream(device=dev)
+    ctx = P.Context(m, R=1, stream=st)
+    v = torch.empty(m.dim, dtype=torch.complex128, device=dev)
+    ctx.fill_gaussian(SEED, v)
+    ms, res = _timed_session(ctx, st, "lanczos", v, 0, 300)
+    a, b = res["alpha"][:, 0], res["beta"][:, 0]
+    E = P.bisec(a, b, 300, 1)
+    c = P.vec12(a, b, E, 300, 1)[0]
+    t0 = time.perf_counter()
+    x = ctx.lanczos_vector(v, a, b, c)
+    t_vec = time.perf_counter() - t0
+    hx = torch.zeros_like(x)
+    ctx.p_mltply_v3(x, hx)
+    out["config0"] = {"workload": "Lanczos ground state, S=1/2 KH honeycomb N=24 (3x4), D=2^24, complex128, "
+                                  "300 steps from the seeded Gaussian",
+                      "steps": 300, "ms_per_step": ms, "e0": float(E[0]),
+                      "residual": float(torch.linalg.vector_norm(hx - float(E[0]) * x).item()),
+                      "eigenvector_pass_s": t_vec}
+    ctx.close()
+    m.close()
+    del v, x, hx
+    torch.cuda.empty_cache()
+    # config 1
+    L = 2.0 * cl.n
+    R = 16
+    m = P.Model.from_couplings(cl, _kh(0.1), field=CP.field_111(0.05), tps_L=L)
+    autotune(m, R)
+    ctx = P.Context(m, R=R, stream=st)
+    v = torch.empty(m.dim * R, dtype=torch.complex128, device=dev)
+    ctx.fill_gaussian(SEED, v)
+    ms, res = _timed_session(ctx, st, "tps", v, 0, args.cfg1_steps, L=L)
+    beta = res["beta"].T
+    energy = res["coef"][:, :, 3].T
+    hmix = res["coef"][:, :, 4].T
+    th = P.api.tpq_thermo(beta, energy, hmix, 0.05, 10.0, 12)
+    out["config1"] = {"workload": "mTPQ R=16, S=1/2 KH+Gamma=0.1+h=0.05[111] honeycomb N=24, l=2.0 (L=48), "
+                                  f"{args.cfg1_steps} steps, E(T) and C(T) of eval_mpi averaged over the 16 seeds",
+                      "steps": args.cfg1_steps, "ms_per_step": ms, "run_s": ms * args.cfg1_steps / 1000.0,
+                      "T": th[:, 0].tolist(), "E": th[:, 1].tolist(), "C": th[:, 2].tolist()}
+    ctx.close()
+    m.close()
+    del v
+    torch.cuda.empty_cache()
+    # config 3
+    cl = cluster_for_sites(18)
+    cpl = CP.kitaev_heisenberg(0.2, -1.0)
+    L3 = 3.0 * cl.n
+    m = P.Model.from_couplings(cl, cpl, q=3, tree=1)
+    ctx = P.Context(m, R=1, stream=st)
+    v = torch.empty(m.dim, dtype=torch.complex128, device=dev)
+    ctx.fill_gaussian(SEED, v)
+    ms_l, res = _timed_session(ctx, st, "lanczos", v, 0, 300)
+    a, b = res["alpha"][:, 0], res["beta"][:, 0]
+    e0 = float(P.bisec(a, b, 300, 1)[0])
+    ctx.close()
+    m.close()
+    del v
+    torch.cuda.empty_cache()
+    m = P.Model.from_couplings(cl, cpl, q=3, tree=1, tps_L=L3)
+    ctx = P.Context(m, R=4, stream=st)
+    v = torch.empty(m.dim * 4, dtype=torch.complex128, device=dev)
+    ctx.fill_gaussian(SEED, v)
+    ms_t, res = _timed_session(ctx, st, "tps", v, 3, args.cfg3_tpq_steps, L=L3)
+    out["config3"] = {"workload": "S=1 KH honeycomb N=18 (3x3), K=-1, J=0.2, D=3^18, complex128: 300-step Lanczos "
+                                  "E0 and mTPQ R=4, l=3.0 (L=54)",
+                      "lanczos": {"steps": 300, "ms_per_step": ms_l, "e0": e0},
+                      "tpq": {"steps_timed": args.cfg3_tpq_steps, "ms_per_step": ms_t,
+                              "projected_1500_steps_s": ms_t * 1.5,
+                              "vector_steps_per_s": 4000.0 / ms_t}}
+    ctx.close()
+    m.close()
+    del v
+    torch.cuda.empty_cache()
+    return out
 
 
 def batched_dsf(dev, args):
@@ -644,7 +740,7 @@ def served_section(args, local_rank, n_requests, rate, sweep=()):
     same requests run alone through the plain path."""
     import torch
     from pned_b200 import serve
-    reqs = serve.make_stream(n_requests, rate=rate, seed=SEED, p30=args.p30)
+    reqs = serve.make_stream(n_requests, rate=rate, seed=SEED, p30=args.p30, min_n30=args.min_n30)
     free, _ = torch.cuda.mem_get_info()
     budget = int(0.85 * free)
     cap_reqs = [serve.Request(**{**q.__dict__, "arrival": 0.0}) for q in reqs]
@@ -676,7 +772,10 @@ def served_section(args, local_rank, n_requests, rate, sweep=()):
         "workload": "Poisson stream of Lanczos E0 (300 steps), mTPQ (R=4, 500 steps), DSF (4 momenta, 100 steps) "
                     "requests, S=1/2 honeycomb N uniform in {18..26} + p30 at N=30, random phi, Gamma, h[111]; "
                     "HBM-budget admission, co-batching by N",
-        "requests": len(reqs), "kinds": {kd: sum(1 for q in reqs if q.kind == kd) for kd in ("lanczos", "tpq", "dsf")},
+        "requests": len(reqs), "of_config_requests": 2000,
+        "sample_note": f"{len(reqs)} of the configuration's 2000 requests (same mix and arrival law); at least "
+                       f"{args.min_n30} at N=30 in the sample",
+        "kinds": {kd: sum(1 for q in reqs if q.kind == kd) for kd in ("lanczos", "tpq", "dsf")},
         "sizes": {str(n): sum(1 for q in reqs if q.n == n) for n in sorted({q.n for q in reqs})},
         "hbm_budget_bytes": budget,
         "solves_per_s": capacity,
@@ -731,7 +830,7 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--traffic", type=float, default=None, help="DRAM bytes per H.v launch from an ncu capture")
-    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1", "sector", "batch"])
+    ap.add_argument("--workload", default="lanczos", choices=["lanczos", "serve", "s1", "sector", "batch", "configs"])
     ap.add_argument("--sector-sites", type=int, default=30)
     ap.add_argument("--no-tune", dest="tune", action="store_false")
     ap.add_argument("--plan", default=None, help="fixed tile plan 'row_fixed_bits,window_bits,max_passes,j_bits[,l1_carveout[,stage]]' "
@@ -743,6 +842,10 @@ def main():
     ap.add_argument("--rates", default=None, help="serve workload: further arrival rates, comma-separated "
                                                   "(the same requests, arrival times rescaled)")
     ap.add_argument("--p30", type=float, default=0.02)
+    ap.add_argument("--min-n30", type=int, default=1, help="served sample: at least this many N=30 requests")
+    ap.add_argument("--no-configs", dest="configs", action="store_false")
+    ap.add_argument("--cfg1-steps", type=int, default=2000)
+    ap.add_argument("--cfg3-tpq-steps", type=int, default=30)
     ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--no-served", dest="served", action="store_false")
     ap.add_argument("--no-dense-check", dest="dense_check", action="store_false")
@@ -772,6 +875,11 @@ def main():
             run_s1(args, rank, world, local_rank)
         elif args.workload == "sector":
             run_sector(args, rank, world, local_rank)
+        elif args.workload == "configs":
+            if rank == 0:
+                import torch
+                torch.cuda.set_device(local_rank)
+                print(json.dumps({"configs": configs_section(torch.device("cuda", local_rank), args)}), flush=True)
         elif args.workload == "batch":
             if rank == 0:
                 import torch

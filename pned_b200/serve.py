@@ -61,10 +61,12 @@ class Request:
 
 def make_stream(n_requests: int, rate: float, seed: int = 20261203, sizes=(18, 20, 22, 24, 26), p30: float = 0.02,
                 mix=(0.80, 0.15, 0.05), lanczos_steps: int = 300, tpq_steps: int = 500, tpq_vectors: int = 4,
-                dsf_steps: int = 100, dsf_momenta: int = 4, dsf_gs_steps: int = 100) -> list:
+                dsf_steps: int = 100, dsf_momenta: int = 4, dsf_gs_steps: int = 100, min_n30: int = 0) -> list:
     """Poisson arrivals (rate per second) of the mixed request stream: N uniform over
     `sizes` plus a fraction p30 at N = 30; phi ~ U[0, 2 pi), Gamma ~ U[-0.2, 0.2],
-    |h| ~ U[0, 0.1] along [111]; one seed per request id."""
+    |h| ~ U[0, 0.1] along [111]; one seed per request id.  min_n30: a short
+    sample that drew fewer N = 30 requests has its middle ones moved to N = 30
+    (Lanczos requests first), so that the sample holds at least that many."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -78,6 +80,14 @@ def make_stream(n_requests: int, rate: float, seed: int = 20261203, sizes=(18, 2
         out.append(Request(rid=rid, kind=kind, n=n, phi=phi, gamma=gamma, h=h, arrival=t, steps=steps,
                            nvec=tpq_vectors if kind == "tpq" else 1, nq=dsf_momenta, gs_steps=dsf_gs_steps,
                            seed=seed * 7919 + rid))
+    short = min_n30 - sum(1 for q in out if q.n == 30)
+    order = sorted(range(len(out)), key=lambda i: (out[i].kind != "lanczos", abs(i - len(out) // 2)))
+    for i in order:
+        if short <= 0:
+            break
+        if out[i].n != 30:
+            out[i].n = 30
+            short -= 1
     return out
 
 

@@ -31,7 +31,11 @@ CANDIDATES_1 = [(8, 10, 4, 3), (8, 8, 2, 3), (8, 10, 1, 3), (5, 8, 1, 3), (5, 10
                 (5, 10, 2, 3, 1, 0, -1, 1), (5, 8, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1),
                 (5, 9, 2, 4, 1, 0, -1, 1), (5, 11, 2, 4, 1, 0, -1, 1), (5, 10, 2, 3, 1, 0, 3, 1),
                 (8, 8, 2, 3, 1, 0, -1, 1), (5, 10, 3, 4, 1, 0, -1, 1)]
-CANDIDATES_R = [(-1, -1, -1), (0, 6, 2), (0, 8, 2), (0, 10, 2), (1, 10, 2), (3, 10, 2), (0, 10, 1)]
+CANDIDATES_R = [(-1, -1, -1), (0, 6, 2), (0, 8, 2), (0, 10, 2), (1, 10, 2), (3, 10, 2), (0, 10, 1),
+                # objective 1: tiles on the bits that hold the most flip terms (rows need no low
+                # bits: a state's R values are already a contiguous run)
+                (0, 6, 2, -1, 1, 0, -1, 1), (0, 8, 2, -1, 1, 0, -1, 1), (0, 10, 2, -1, 1, 0, -1, 1),
+                (1, 8, 2, -1, 1, 0, -1, 1), (0, 8, 3, -1, 1, 0, -1, 1), (0, 12, 1, -1, 1, 0, -1, 1)]
 
 _cache: dict = {}
 

@@ -645,3 +645,38 @@ def test_cuda_path_against_golden_fixtures(name):
     v /= np.linalg.norm(v)
     run = ctx.lanczos(v, 250, check_conv=True)
     assert abs(run["ene"][0] - c["e"][0]) <= 1e-10 * abs(c["e"][0])
+
+
+@pytest.mark.parametrize("R", [2, 4, 12, 16])
+@pytest.mark.parametrize("plan", [(0, 6, 2, -1, 1, 0, -1, 1), (1, 8, 2, -1, 1, 0, -1, 1), (0, 4, 3, -1, 1, 0, -1, 1)])
+def test_multi_vector_plans_agree_with_oracle(plan, R):
+    """The multi-vector kernel with tiles on the bits that hold the most flip terms
+    (rows on any bits: a state's R values are one contiguous run) gives each
+    column the oracle's H.v to 1e-12, and its TPS coefficients to 1e-10."""
+    cl = honeycomb(2, 4)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    got = gm.set_plan(R, *plan)
+    assert got["tile_passes"] >= 1
+    ctx = P.Context(gm, R=R)
+    rng = np.random.default_rng(41)
+    D = gm.dim
+    v1 = (rng.standard_normal((D, R)) + 1j * rng.standard_normal((D, R))).astype(np.complex128)
+    v0 = (0.2 * rng.standard_normal((D, R)) + 0.1j * rng.standard_normal((D, R))).astype(np.complex128)
+    w = np.ascontiguousarray(v0).reshape(-1).copy()
+    pr = ctx.p_mltply_v3(np.ascontiguousarray(v1).reshape(-1), w, 0.0625)
+    w = w.reshape(D, R)
+    for r in range(R):
+        ref = np.ascontiguousarray(v0[:, r]).copy()
+        prr = om.p_mltply_v3(np.ascontiguousarray(v1[:, r]), ref, 0.0625)
+        assert rel(w[:, r], ref) <= 1e-12
+        assert abs(pr[r] - prr) <= 1e-12 * abs(prr)
+    L = 2.0 * cl.n
+    gt, ot = models(cl, 2, 0, KHGH, FIELD, tps_L=L)
+    gt.set_plan(R, *plan)
+    V = O.gaussian(13, gt.dim, R).reshape(gt.dim, R)
+    V /= np.linalg.norm(V, axis=0)
+    out = P.Context(gt, R=R).tps(L, np.ascontiguousarray(V).reshape(-1), 20)
+    for r in (0, R - 1):
+        ref = ot.tps(L, np.ascontiguousarray(V[:, r]), 20)
+        assert rel(out["beta"][:, r], ref["beta"]) <= 1e-10
+        assert rel(out["coef"][:, r, :5], ref["coef"][:, :5]) <= 1e-10
