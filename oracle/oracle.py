@@ -17,7 +17,10 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "_build", "libpned_oracle.so")
+# PNED_ORACLE_BUILD=fma loads the build with fused multiply-adds (see the Makefile):
+# the same algorithm with other rounding, used to measure the spread of long chains
+_VARIANT = os.environ.get("PNED_ORACLE_BUILD", "")
+_LIB_PATH = os.path.join(_HERE, "_build", "libpned_oracle_fma.so" if _VARIANT == "fma" else "libpned_oracle.so")
 _lib = None
 
 c_int_p = C.POINTER(C.c_int)

@@ -462,6 +462,21 @@ omodel *oracle_model_create(int n, int q, int tree_sa, int nbond, const int *ipa
         }
     }
     free(p1); free(p2); free(ty);
+    /* PNED_ORACLE_ITEM_ORDER=reverse sums the items in the reverse order.  The
+       order in which p_mltply_v3 sums its items is what the reference's rank
+       decomposition changes (make_cpu_list2 groups the items by class,
+       S_one_half/Hybrid_TPS_MPIlib.f90:104-341); a test uses it to measure how
+       far long chains depend on that order.  Unset: the lnp = 1 order. */
+    const char *ord = getenv("PNED_ORACLE_ITEM_ORDER");
+    if (ord && strcmp(ord, "reverse") == 0) {
+        for (int i = 0, j = m->nitem - 1; i < j; ++i, --j) {
+            int t;
+            t = m->it_s1[i]; m->it_s1[i] = m->it_s1[j]; m->it_s1[j] = t;
+            t = m->it_s2[i]; m->it_s2[i] = m->it_s2[j]; m->it_s2[j] = t;
+            t = m->it_t[i]; m->it_t[i] = m->it_t[j]; m->it_t[j] = t;
+            t = m->it_e[i]; m->it_e[i] = m->it_e[j]; m->it_e[j] = t;
+        }
+    }
     m->ihf0 = n / 2; m->ihf = (n + 1) / 2;
     if (!tree_sa) {
         int64_t ihfbit = (int64_t)1 << m->ihf;

@@ -125,6 +125,29 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
     block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
 }
 
+// Block sum of one vector's K sums (lanes, then warps, in a fixed order) into
+// dst[0 .. K-1]; the thread's sums are reset.  All threads of the block call it.
+template <int K>
+__device__ __forceinline__ void tile_sums_store(double2 (&red)[K][1], double2 (*s_red)[K], double2 *dst)
+{
+    const uint32_t tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        for (int off = 16; off >= 1; off >>= 1) {
+            red[k][0].x += __shfl_xor_sync(0xffffffffu, red[k][0].x, off);
+            red[k][0].y += __shfl_xor_sync(0xffffffffu, red[k][0].y, off);
+        }
+        if ((tid & 31u) == 0) s_red[tid >> 5][k] = red[k][0];
+        red[k][0] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (tid < uint32_t(K)) {
+        double2 sum = make_double2(0.0, 0.0);
+        for (int w = 0; w < kThreads / 32; ++w) sum = cadd(sum, s_red[w][tid]);
+        dst[tid] = sum;
+    }
+}
+
 // Tiled single-vector (R = 1) H.v on the S = 1/2 full basis, one pass of a
 // multi-pass program (each pass owns a subset of the flip masks).  A block owns
 // a tile of 256 * 2^JB states: thread t holds the states of row t (its 8 bits
@@ -145,12 +168,17 @@ __global__ void __launch_bounds__(kThreads, BPS)
     constexpr int SPT = 1 << JB;
     constexpr int CH = SPT < 8 ? SPT : 8;   // rows loaded together (16 rows: two chunks, no spills)
     constexpr int TILE = kThreads * SPT;
+    // up to 8 rows a thread the epilogue's rows of P or W are staged too (16 rows:
+    // two tiles would not leave room for two blocks per SM)
+    constexpr bool PWS = SPT <= 8;
     extern __shared__ double2 smem[];
     double2 *s_v = smem;
-    double2 *s_tab = smem + TILE;
+    double2 *s_pw = smem + TILE;   // the thread's own rows of P (first pass) or W (later passes)
+    double2 *s_tab = smem + (PWS ? 2 : 1) * TILE;
     for (int i = threadIdx.x; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
     const uint32_t tid = threadIdx.x;
     const int64_t ntiles = int64_t(1) << prog.nouter;
+    const double2 *pw_src = PWS ? (prog.first ? a.P : a.W) : nullptr;   // staged rows of the epilogue
     double2 red[K][1];
 #pragma unroll
     for (int k = 0; k < K; ++k) red[k][0] = make_double2(0.0, 0.0);
@@ -183,6 +211,15 @@ __global__ void __launch_bounds__(kThreads, BPS)
             if (j0 == 0) {
                 __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
                 if (ctr && tid == 0) s_next = atomicAdd(ctr, 1u);   // every thread has read s_next
+                // the epilogue's rows of P or W are requested now and land in the thread's own
+                // slots while the terms run (the thread read its slots of the previous tile
+                // before this point)
+                if (pw_src) {
+#pragma unroll
+                    for (int j = 0; j < SPT; ++j)
+                        cp_async16(s_pw + tid + kThreads * j, pw_src + (base | prog.jexp[j]));
+                    cp_async_commit();
+                }
             }
 #pragma unroll
             for (int jj = 0; jj < CH; ++jj) s_v[tid + kThreads * (j0 + jj)] = v[jj];
@@ -263,17 +300,18 @@ __global__ void __launch_bounds__(kThreads, BPS)
                 }
             }
         }
+        if (pw_src) cp_async_wait<0>();
 #pragma unroll
         for (int j = 0; j < SPT; ++j) {
             const int64_t e = base | prog.jexp[j];
             const double2 hv = cscale(hs, acc[j]);
             double2 out = hv;
             if (!prog.first) {
-                const double2 w0 = __ldcs(a.W + e);
+                const double2 w0 = PWS ? s_pw[tid + kThreads * j] : __ldcs(a.W + e);
                 out.x += w0.x;
                 out.y += w0.y;
             } else if (a.P) {
-                const double2 p = __ldcs(a.P + e);
+                const double2 p = PWS ? s_pw[tid + kThreads * j] : __ldcs(a.P + e);
                 out.x = fma(pc, p.x, out.x);
                 out.y = fma(pc, p.y, out.y);
             }
@@ -294,24 +332,11 @@ __global__ void __launch_bounds__(kThreads, BPS)
         }
         // the tile's sums (fixed order: lanes, then warps), written at the tile's slot,
         // so that the total does not depend on which block took which tile
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            for (int off = 16; off >= 1; off >>= 1) {
-                red[k][0].x += __shfl_xor_sync(0xffffffffu, red[k][0].x, off);
-                red[k][0].y += __shfl_xor_sync(0xffffffffu, red[k][0].y, off);
-            }
-            if ((tid & 31u) == 0) s_red[tid >> 5][k] = red[k][0];
-            red[k][0] = make_double2(0.0, 0.0);
-        }
-        __syncthreads();
-        if (tid < uint32_t(K)) {
-            double2 sum = make_double2(0.0, 0.0);
-            for (int w = 0; w < kThreads / 32; ++w) sum = cadd(sum, s_red[w][tid]);
-            a.partials[size_t(tile) * K + tid] = sum;
-        }
+        tile_sums_store<K>(red, s_red, a.partials + size_t(tile) * K);
         tile = s_next;
     }
-    if (!ctr) block_reduce_store<K, 1>(red, 1, 1, 1, a.partials);
+    // static order: the block's sums over its tiles (same reduction order)
+    if (!ctr) tile_sums_store<K>(red, s_red, a.partials + size_t(blockIdx.x) * K);
 }
 
 // Tiled multi-vector H.V (R > 1 interleaved vectors, S = 1/2 full basis), one
@@ -331,12 +356,15 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
     const int R = a.R, G = R / VPT, NS = kThreads / G;
     const int tbits = prog.tbits;
     const uint32_t tmask = (1u << tbits) - 1u;
+    const size_t TS = size_t(SPT) * NS * R;   // elements of a tile
     double2 *s_v = smem;
-    double2 *s_tab = smem + size_t(SPT) * NS * R;
+    double2 *s_pw = smem + TS;   // the thread's own elements of P (first pass) or W (later passes)
+    double2 *s_tab = smem + 2 * TS;
     const int tabw = SLOT ? R : 1;
     for (int i = threadIdx.x; i < prog.ntab * tabw; i += blockDim.x) s_tab[i] = a.table[i];
     const int g = threadIdx.x % G, l = threadIdx.x / G;   // vectors g, g + G, ..., g + (VPT-1) G
     const int64_t ntiles = int64_t(1) << prog.nouter;
+    const double2 *pw_src = prog.first ? a.P : a.W;   // staged rows of the epilogue (null: none)
     double2 red[K][VPT];
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -344,7 +372,22 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
         for (int q = 0; q < VPT; ++q) red[k][q] = make_double2(0.0, 0.0);
     uint32_t rowbase = 0;   // the thread's row on its global bits
     for (int k = 0; k < tbits; ++k) rowbase |= ((uint32_t(l) >> k) & 1u) << prog.rowpos[k];
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // dynamic order: blocks take chunks of consecutive tiles (>= 2048 states) from the
+    // pass's counter and write the chunk's sums at the chunk's slot; null counter: the
+    // static order (tile = block + k * grid) with per-block sums
+    __shared__ uint32_t s_next;
+    uint32_t *const ctr = a.tile_counter ? a.tile_counter + prog.pass : nullptr;
+    const int64_t ctiles = ctr ? int64_t(max(1, a.rv_chunk)) : 1;   // tiles per chunk
+    const int64_t nchunks = (ntiles + ctiles - 1) / ctiles;
+    int64_t chunk = blockIdx.x;
+    if (ctr) {
+        if (threadIdx.x == 0) s_next = atomicAdd(ctr, 1u);
+        __syncthreads();
+        chunk = s_next;
+    }
+    for (; ctr ? chunk < nchunks : chunk < ntiles;) {
+      const int64_t tile_end = ctr ? min(ntiles, (chunk + 1) * ctiles) : chunk + 1;
+      for (int64_t tile = ctr ? chunk * ctiles : chunk; tile < tile_end; ++tile) {
         uint32_t base = rowbase;
         for (int k = 0; k < prog.nouter; ++k) base |= uint32_t((tile >> k) & 1) << prog.outer[k];
         double2 acc[SPT][VPT];
@@ -355,6 +398,18 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
 #pragma unroll
                 for (int q = 0; q < VPT; ++q) v[j][q] = __ldg(a.C + int64_t(base | prog.jexp[j]) * R + g + q * G);
             __syncthreads();   // the previous tile's shared reads are done (first tile: table staged)
+            // the chunk's first tile: every thread has read s_next, so the next chunk is taken now
+            if (ctr && threadIdx.x == 0 && tile == chunk * ctiles) s_next = atomicAdd(ctr, 1u);
+            // the epilogue's elements of P or W land in the thread's own slots while the terms run
+            if (pw_src) {
+#pragma unroll
+                for (int j = 0; j < SPT; ++j)
+#pragma unroll
+                    for (int q = 0; q < VPT; ++q)
+                        cp_async16(s_pw + (j * NS + l) * R + g + q * G,
+                                   pw_src + int64_t(base | prog.jexp[j]) * R + g + q * G);
+                cp_async_commit();
+            }
 #pragma unroll
             for (int j = 0; j < SPT; ++j)
 #pragma unroll
@@ -435,6 +490,7 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
                 }
             }
         }
+        if (pw_src) cp_async_wait<0>();
 #pragma unroll
         for (int j = 0; j < SPT; ++j) {
 #pragma unroll
@@ -445,12 +501,12 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
                 const double2 hv = cscale(a.hsc ? a.hsc[r] : sc, acc[j][q]);
                 double2 out = hv;
                 if (!prog.first) {
-                    const double2 w0 = __ldcs(a.W + e);
+                    const double2 w0 = s_pw[(j * NS + l) * R + r];
                     out.x += w0.x;
                     out.y += w0.y;
                 } else if (a.P) {
                     const double pc = a.pc[r];
-                    const double2 p = __ldcs(a.P + e);
+                    const double2 p = s_pw[(j * NS + l) * R + r];
                     out.x = fma(pc, p.x, out.x);
                     out.y = fma(pc, p.y, out.y);
                 }
@@ -466,8 +522,21 @@ __global__ void __launch_bounds__(kThreads, 2) hv_tile_rv_kernel(const __grid_co
                 }
             }
         }
+      }
+        if (!ctr) {
+            chunk += gridDim.x;
+            continue;
+        }
+        // the chunk's sums at the chunk's slot (fixed order), so that the total does not
+        // depend on which block took which chunk; s_next is visible after its barrier
+        block_reduce_store<K, VPT, true>(red, G, VPT, R, a.partials, chunk);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int q = 0; q < VPT; ++q) red[k][q] = make_double2(0.0, 0.0);
+        chunk = s_next;
     }
-    block_reduce_store<K, VPT, true>(red, G, VPT, R, a.partials);
+    if (!ctr) block_reduce_store<K, VPT, true>(red, G, VPT, R, a.partials);
 }
 
 // Mixed-radix (q > 2) variant: partner = s + offset, coefficient indexed by
@@ -716,7 +785,7 @@ static cudaError_t launch_tile_j(const pned_model *m, const HvArgs &a, int nbloc
         e = set_carveout(reinterpret_cast<const void *>(kern), m->device, m->tile_smem, BPS);
     if (e != cudaSuccess) return e;
     const int grid = tile_grid(m, nblocks);
-    const bool dyn = tile_dynamic(m, a);
+    const bool dyn = tile_dynamic(m, a, nblocks);
     HvArgs b = a;
     if (!dyn) b.tile_counter = nullptr;
     else if ((e = cudaMemsetAsync(a.tile_counter, 0, sizeof(uint32_t) * kTileMaxPasses, st)) != cudaSuccess)
@@ -820,6 +889,22 @@ static cudaError_t launch_hv_k(const pned_model *m, const HvArgs &a, int nblocks
 
 static int rtile_grid(const pned_model *m, int nblocks) { return std::max(1, std::min(nblocks, 2 * m->nsm)); }
 
+// Tiles per chunk of one multi-vector pass in the dynamic order: chunks of about
+// 2048 states (one partial-sum record each), but at least four chunks per block
+// of the grid, so that small bases still spread over the whole device.
+int64_t rtile_chunk_tiles(const TileProgram &t, int grid)
+{
+    const int64_t states = int64_t(1) << (t.tbits + t.jb);   // (256 / G) rows x SPT
+    const int64_t ntiles = int64_t(1) << t.nouter;
+    return std::max<int64_t>(1, std::min<int64_t>(2048 / states, ntiles / (4 * int64_t(std::max(1, grid)))));
+}
+
+int64_t rtile_chunks(const TileProgram &t, int grid)
+{
+    const int64_t per = rtile_chunk_tiles(t, grid);
+    return ((int64_t(1) << t.nouter) + per - 1) / per;
+}
+
 // Tile set of the multi-vector kernel for R (null: the flat kernel runs).
 static const pned_model::TileSet *find_rtiles(const pned_model *m, int R)
 {
@@ -841,9 +926,16 @@ static cudaError_t launch_rv_t(const pned_model *m, const pned_model::TileSet &t
     if (e != cudaSuccess) return e;
     const int grid = rtile_grid(m, nblocks);
     const size_t smem = rtile_smem(m, a.R, SLOT);
+    const bool dyn = tile_dynamic(m, a, nblocks);
     HvArgs b = a;
+    if (!dyn) b.tile_counter = nullptr;
+    else if ((e = cudaMemsetAsync(a.tile_counter, 0, sizeof(uint32_t) * kTileMaxPasses, st)) != cudaSuccess)
+        return e;
+    size_t off = 0;
     for (size_t p = 0; p < ts.progs.size(); ++p) {
-        b.partials = a.partials + size_t(p) * grid * K * a.R;
+        b.partials = a.partials + off;
+        b.rv_chunk = dyn ? int(rtile_chunk_tiles(*ts.progs[p], grid)) : 1;
+        off += (dyn ? size_t(rtile_chunks(*ts.progs[p], grid)) : size_t(grid)) * K * a.R;
         kern<<<grid, kThreads, smem, st>>>(*ts.progs[p], b);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -877,15 +969,31 @@ int64_t tile_dynamic_partials(const pned_model *m)
     return n;
 }
 
-bool tile_dynamic(const pned_model *m, const HvArgs &a)
+int64_t rtile_dynamic_partials(const pned_model *m, int R, int nblocks)
 {
-    if (!a.tile_counter || a.R != 1 || m->tprogs.empty() || !m->use_tile || tile_staged(m)) return false;
-    return tile_dynamic_partials(m) * a.K <= a.partials_cap;
+    const pned_model::TileSet *ts = find_rtiles(m, R);
+    if (!ts) return 0;
+    const int grid = rtile_grid(m, nblocks);
+    int64_t n = 0;
+    for (const auto &t : ts->progs) n += rtile_chunks(*t, grid);
+    return n;
+}
+
+bool tile_dynamic(const pned_model *m, const HvArgs &a, int nblocks)
+{
+    if (!a.tile_counter) return false;
+    if (a.R == 1) {
+        if (m->tprogs.empty() || !m->use_tile || tile_staged(m)) return false;
+        return tile_dynamic_partials(m) * a.K <= a.partials_cap;
+    }
+    if (a.slot_tables || !find_rtiles(m, a.R)) return false;
+    return rtile_dynamic_partials(m, a.R, nblocks) * a.K * a.R <= a.partials_cap;
 }
 
 int64_t hv_partials(const pned_model *m, const HvArgs &a, int nblocks)
 {
-    if (tile_dynamic(m, a)) return tile_dynamic_partials(m);
+    if (tile_dynamic(m, a, nblocks))
+        return a.R == 1 ? tile_dynamic_partials(m) : rtile_dynamic_partials(m, a.R, nblocks);
     return hv_partial_blocks(m, a.R, nblocks);
 }
 
@@ -1036,7 +1144,8 @@ void build_tile_programs(pned_model *m)
         m->tile_jb = jb;
         m->tile_bps = (jb == 3 && m->plan1.blocks_per_sm == 3) ? 3 : tile_blocks_per_sm(jb);
         m->tile_stage = std::max(0, std::min(2, m->plan1.stage_partner_tiles));
-        m->tile_smem = sizeof(double2) * (size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
+        // own tile, and for up to 8 rows a thread the staged epilogue rows, then the table
+        m->tile_smem = sizeof(double2) * ((jb <= 3 ? 2 : 1) * size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
         m->use_tile = true;
         if (m->tile_stage == 2) {
             // bulk copies: 8 rows per thread, runs of >= 8 consecutive states,
@@ -1073,7 +1182,8 @@ size_t rtile_smem(const pned_model *m, int R, bool slot_tables)
     rtile_shape(R, vpt, spt);
     const int G = R / vpt;
     const size_t tile = size_t(kThreads / G) * spt * R;
-    return sizeof(double2) * (tile + size_t(std::max(1, m->ntab)) * (slot_tables ? R : 1));
+    // the tile, the staged epilogue elements (same size), the coefficient tables
+    return sizeof(double2) * (2 * tile + size_t(std::max(1, m->ntab)) * (slot_tables ? R : 1));
 }
 
 bool ensure_rtiles(pned_model *m, int R, bool slot_tables, const pned_tile_plan *plan)
@@ -1363,6 +1473,10 @@ extern "C" int pned_ctx_create(pned_model *m, int R, size_t budget, pned_ctx **o
     if (R == 1 && m->use_tile) {
         pslots = std::max<size_t>(pslots, size_t(tile_dynamic_partials(m)) * kMaxK);
         pslots = std::max<size_t>(pslots, size_t(m->dim / 2048) * 2 * kMaxK);
+    }
+    if (R > 1) {   // per-chunk sums of the multi-vector kernel: the current plan, or two passes
+        pslots = std::max<size_t>(pslots, size_t(rtile_dynamic_partials(m, R, c->nblocks)) * kMaxK * R);
+        pslots = std::max<size_t>(pslots, size_t(m->dim / 2048 + 1) * 2 * kMaxK * R);
     }
     const size_t pbytes = sizeof(double2) * pslots;
     c->partials_cap = int64_t(pslots);

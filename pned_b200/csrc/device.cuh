@@ -186,9 +186,15 @@ cudaError_t launch_tile_staged(const pned_model *m, const HvArgs &a, int nblocks
 int hv_partial_blocks(const pned_model *m, int R, int nblocks);
 // Tiles of all passes of the single-vector tile plan (the per-tile sums of the dynamic order).
 int64_t tile_dynamic_partials(const pned_model *m);
-// True when launch_hv runs the single-vector tile kernel in dynamic tile order
-// for these arguments (tile counters given and room for the per-tile sums).
-bool tile_dynamic(const pned_model *m, const HvArgs &a);
+// Tiles per chunk and chunks of one multi-vector pass on a grid, and the chunks of
+// all passes for R vectors (the per-chunk sums of the dynamic order; 0: no
+// multi-vector plan).
+int64_t rtile_chunk_tiles(const TileProgram &t, int grid);
+int64_t rtile_chunks(const TileProgram &t, int grid);
+int64_t rtile_dynamic_partials(const pned_model *m, int R, int nblocks);
+// True when launch_hv runs a tile kernel in dynamic tile order for these
+// arguments (tile counters given and room for the per-tile or per-chunk sums).
+bool tile_dynamic(const pned_model *m, const HvArgs &a, int nblocks);
 // Partial sums launch_hv writes for these arguments (per tile or per block).
 int64_t hv_partials(const pned_model *m, const HvArgs &a, int nblocks);
 // The context's tile counters and partial-sum capacity into a.
@@ -236,10 +242,12 @@ __device__ __forceinline__ int digit_at(uint64_t digits, int j) { return int((di
 
 // Block-level reduction of red[K][VPT] (vector r = g*vpt + j, or g + j*G when
 // STRIDED; g = lane % G, G a power of two dividing 32) into
-// partials[blockIdx.x][K][R].
+// partials[slot][K][R] (slot < 0: blockIdx.x).
 template <int K, int VPT, bool STRIDED = false>
-__device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G, int vpt, int R, double2 *partials)
+__device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G, int vpt, int R, double2 *partials,
+                                                   int64_t slot = -1)
 {
+    const size_t sl = slot < 0 ? size_t(blockIdx.x) : size_t(slot);
     __shared__ double2 sm[kThreads / 32][kMaxK][kMaxR];
     for (int off = 16; off >= G; off >>= 1)
 #pragma unroll
@@ -262,7 +270,7 @@ __device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G
         const int k = idx / R, r = idx - k * R;
         double2 s = make_double2(0.0, 0.0);
         for (int w = 0; w < nw; ++w) s = cadd(s, sm[w][k][r]);
-        partials[((size_t)blockIdx.x * K + k) * R + r] = s;
+        partials[(sl * K + k) * R + r] = s;
     }
 }
 

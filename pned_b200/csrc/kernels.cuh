@@ -108,6 +108,7 @@ struct HvArgs {
     // order (tile = block + k * grid) with per-block sums.
     uint32_t *tile_counter;
     int64_t partials_cap;   // double2 slots available at `partials` (per-tile sums need sum(tiles) * K)
+    int rv_chunk;           // multi-vector kernel, dynamic order: tiles per chunk (set by the launcher)
     // Sz sector (set by launch_hv from the model): index -> state, and the Lin
     // tables, state -> index = lin_lo[state mod lin_mod] + lin_hi[state / lin_mod] - 1
     const int64_t *list1;

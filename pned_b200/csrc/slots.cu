@@ -355,6 +355,8 @@ struct pned_slots {
     double *hist_a = nullptr, *hist_b = nullptr, *coef = nullptr;
     double *vcoef = nullptr;         // [R][max_steps]
     double2 *partials = nullptr, *sums = nullptr, *scratch = nullptr;   // scratch: [R][n] phases + [R][nbond*4] dtab
+    int64_t partials_cap = 0;        // double2 slots at `partials`
+    uint32_t *tile_ctr = nullptr;    // R = 1: tile counters of the single-vector kernel's dynamic order
     cudaGraphExec_t graph = nullptr;
     int64_t enqueued = 0;
     // R = 1: the batch's table and diagonal have the layout of a model's, so the
@@ -398,8 +400,10 @@ cudaError_t slot_step(pned_slots *S)
         a.diag = S->diag; a.shift = 0.0; a.table = S->table;
         a.partials = S->partials; a.dim = S->dim; a.R = R; a.K = 4;
         a.slot_tables = R > 1;
+        a.tile_counter = S->tile_ctr;
+        a.partials_cap = S->partials_cap;
         e = launch_hv(&S->tm, a, S->nblocks, S->stream);
-        nb_hv = hv_partial_blocks(&S->tm, R, S->nblocks);
+        nb_hv = int(hv_partials(&S->tm, a, S->nblocks));
     } else {
         SlotHvArgs a{};
         a.C = C; a.P = P; a.W = W;
@@ -452,7 +456,7 @@ void slots_free(pned_slots *S)
     for (double2 *b : S->buf) cudaFree(b);
     cudaFree(S->diag); cudaFree(S->table); cudaFree(S->s1); cudaFree(S->s2); cudaFree(S->st); cudaFree(S->cf);
     cudaFree(S->hist_a); cudaFree(S->hist_b); cudaFree(S->coef); cudaFree(S->vcoef);
-    cudaFree(S->partials); cudaFree(S->sums); cudaFree(S->scratch);
+    cudaFree(S->partials); cudaFree(S->sums); cudaFree(S->scratch); cudaFree(S->tile_ctr);
     if (S->own_stream) cudaStreamDestroy(S->own_stream);
 }
 
@@ -610,7 +614,12 @@ extern "C" int pned_slots_create(const pned_model_desc *structure, int R, int ma
     if (e == cudaSuccess) e = salloc(S.get(), &S->hist_b, size_t(R) * max_steps);
     if (e == cudaSuccess) e = salloc(S.get(), &S->coef, size_t(R) * max_steps * 5);
     if (e == cudaSuccess) e = salloc(S.get(), &S->vcoef, size_t(R) * max_steps);
-    if (e == cudaSuccess) e = salloc(S.get(), &S->partials, size_t(S->nblocks) * kTileMaxPasses * kMaxK * kMaxR);
+    // per-block sums, and for R = 1 the per-tile sums of the single-vector kernel's
+    // dynamic order (any plan of two passes with tiles of >= 2048 states)
+    S->partials_cap = int64_t(S->nblocks) * kTileMaxPasses * kMaxK * kMaxR;
+    if (R == 1) S->partials_cap = std::max<int64_t>(S->partials_cap, (S->dim / 2048 + 1) * 2 * kMaxK);
+    if (e == cudaSuccess) e = salloc(S.get(), &S->partials, size_t(S->partials_cap));
+    if (e == cudaSuccess) e = cudaMalloc(&S->tile_ctr, sizeof(uint32_t) * kTileMaxPasses);
     if (e == cudaSuccess) e = salloc(S.get(), &S->sums, size_t(12) * kMaxR);
     if (e == cudaSuccess) e = salloc(S.get(), &S->scratch, size_t(R) * 64 + size_t(R) * S->nbond * 4);
     if (e == cudaSuccess) e = cudaMemcpy(S->s1, hp.dsite1.data(), sizeof(int) * S->nbond, cudaMemcpyHostToDevice);

@@ -302,8 +302,12 @@ class Server:
     chunk, so that arrivals wait at most about that long for admission."""
 
     def __init__(self, budget: int, lane_factory=None, lane_slots=default_lane_slots, max_steps: int = 512,
-                 chunk_ms: float = 30.0, clock=time.perf_counter, sleep=time.sleep, max_lanes=default_max_lanes):
+                 chunk_ms: float = 30.0, clock=time.perf_counter, sleep=time.sleep, max_lanes=default_max_lanes,
+                 exclusive_n: int = 20):
         self.budget = int(budget)
+        # lanes of exclusive_n sites and more run their chunks one at a time: their H.V
+        # holds a window of the vector in L2, which a second such kernel beside it evicts
+        self.exclusive_n = exclusive_n
         self.lane_factory = lane_factory or (lambda n, R, ms: GpuLane(n, R, ms))
         self.lane_slots = lane_slots
         self.max_lanes = max_lanes
@@ -412,6 +416,9 @@ class Server:
                 q.extendleft(reversed(skipped))
                 active = [s for s in range(len(ls.occ)) if ls.occ[s] is not None]
                 if not active:
+                    continue
+                if n >= self.exclusive_n and any(o is not ls and o.busy and o.n >= self.exclusive_n
+                                                 for o in self.lanes):
                     continue
                 k = min(ls.left[s] for s in active)
                 if ls.step_ms > 0:

@@ -152,3 +152,19 @@ def test_several_lanes_per_size_run_side_by_side():
         if e[0] == "open":
             per_n[e[1]] = per_n.get(e[1], 0) + 1
     assert max(per_n.values()) == 3 and all(v <= 3 for v in per_n.values())
+
+
+def test_short_stream_holds_the_requested_n30_requests():
+    """A short sample of the serving mix (2 % at N = 30) that drew no N = 30
+    request has one moved there, a Lanczos request from the middle; the rest of
+    the stream is unchanged."""
+    base = serve.make_stream(40, rate=1.0, seed=20261203)
+    got = serve.make_stream(40, rate=1.0, seed=20261203, min_n30=1)
+    n30 = [q for q in got if q.n == 30]
+    assert len(n30) >= 1
+    moved = [(a, b) for a, b in zip(base, got) if a.n != b.n]
+    assert len(moved) == max(0, 1 - sum(1 for q in base if q.n == 30))
+    for a, b in moved:
+        assert b.kind == "lanczos" and b.n == 30 and (a.rid, a.arrival, a.seed) == (b.rid, b.arrival, b.seed)
+    assert serve.make_stream(40, rate=1.0, seed=20261203, min_n30=3)[20].n in (18, 20, 22, 24, 26, 30)
+    assert sum(1 for q in serve.make_stream(40, rate=1.0, seed=20261203, min_n30=3) if q.n == 30) >= 3
