@@ -610,12 +610,14 @@ __global__ void __launch_bounds__(kThreads) hv_radix_kernel(const __grid_constan
 }
 
 // Sums partials[nb][KR] in a fixed order into out[KR] (one block).
-__global__ void finish_sum_kernel(const double2 *__restrict__ partials, int nb, int KR, double2 *out)
+// Sums partials[b * stride][kr] over b < nb for each kr into out[kr] (one block,
+// fixed order).
+__global__ void finish_sum_kernel(const double2 *__restrict__ partials, int nb, int KR, double2 *out, int stride)
 {
     __shared__ double2 sm[kThreads];
     for (int kr = 0; kr < KR; ++kr) {
         double2 s = make_double2(0.0, 0.0);
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) s = cadd(s, partials[(size_t)b * KR + kr]);
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s = cadd(s, partials[(size_t)b * stride * KR + kr]);
         sm[threadIdx.x] = s;
         __syncthreads();
         for (int w = blockDim.x / 2; w > 0; w >>= 1) {
@@ -1027,9 +1029,40 @@ cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStr
     }
 }
 
+// First level of a long finish: block b sums rows [b * chunk, (b + 1) * chunk) of
+// partials ([row][KR]) in a fixed order and writes the sum over row b * chunk, the
+// first of its own rows, which no other block reads.
+__global__ void finish_chunks_kernel(double2 *partials, int nb, int KR, int chunk)
+{
+    __shared__ double2 sm[kThreads];
+    const int64_t lo = int64_t(blockIdx.x) * chunk, hi = min(int64_t(nb), lo + chunk);
+    for (int kr = 0; kr < KR; ++kr) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int64_t b = lo + threadIdx.x; b < hi; b += blockDim.x) s = cadd(s, partials[b * KR + kr]);
+        sm[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sm[threadIdx.x] = cadd(sm[threadIdx.x], sm[threadIdx.x + w]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partials[lo * KR + kr] = sm[0];
+        __syncthreads();
+    }
+}
+
 cudaError_t launch_finish(const double2 *partials, int nb, int KR, double2 *out, cudaStream_t st)
 {
-    finish_sum_kernel<<<1, kThreads, 0, st>>>(partials, nb, KR, out);
+    // long lists (per-tile sums of the tile kernels) in two levels: one block alone
+    // would read them at a single SM's bandwidth
+    constexpr int kLevel1Blocks = 512;
+    if (nb > 4 * kLevel1Blocks) {
+        const int chunk = (nb + kLevel1Blocks - 1) / kLevel1Blocks;
+        const int nb2 = (nb + chunk - 1) / chunk;
+        finish_chunks_kernel<<<nb2, kThreads, 0, st>>>(const_cast<double2 *>(partials), nb, KR, chunk);
+        finish_sum_kernel<<<1, kThreads, 0, st>>>(partials, nb2, KR, out, chunk);
+        return cudaGetLastError();
+    }
+    finish_sum_kernel<<<1, kThreads, 0, st>>>(partials, nb, KR, out, 1);
     return cudaGetLastError();
 }
 

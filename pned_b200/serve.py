@@ -303,7 +303,7 @@ class Server:
 
     def __init__(self, budget: int, lane_factory=None, lane_slots=default_lane_slots, max_steps: int = 512,
                  chunk_ms: float = 30.0, clock=time.perf_counter, sleep=time.sleep, max_lanes=default_max_lanes,
-                 exclusive_n: int = 20):
+                 exclusive_n: int = 24):
         self.budget = int(budget)
         # lanes of exclusive_n sites and more run their chunks one at a time: their H.V
         # holds a window of the vector in L2, which a second such kernel beside it evicts
@@ -345,6 +345,14 @@ class Server:
         stats.lanes_created += 1
         stats.peak_bytes = max(stats.peak_bytes, self.used)
         return True
+
+    def warm(self, sizes):
+        """Plans (autotunes) the lanes of these lattice sizes ahead of the requests,
+        as a server does at start-up: each lane is opened once and closed again,
+        so that requests do not wait for the tuner (its choice is cached)."""
+        for n in sorted(set(sizes)):
+            eng = self.lane_factory(n, self.lane_slots(n), self.max_steps)
+            eng.close()
 
     def _close_lane(self, ls):
         self.lanes.remove(ls)
@@ -473,15 +481,37 @@ def summarize(stats: ServeStats, requests) -> dict:
 
 # --------------------------------------------------------------------------- plain one-at-a-time path
 
+def warm_plain(requests):
+    """Tunes the plain path's plans for every (size, vector count) the requests
+    use, once (the autotuner caches per lattice, terms and R)."""
+    from .tune import autotune
+    seen = set()
+    for r in requests:
+        widths = {"lanczos": (1,), "tpq": (r.nvec,), "dsf": (1, r.nq)}[r.kind]
+        for R in widths:
+            key = (r.n, R, r.kind == "tpq")
+            if key in seen:
+                continue
+            seen.add(key)
+            cl = cluster_for_sites(r.n)
+            cpl, fld = r.couplings()
+            m = api.Model.from_couplings(cl, cpl, field=fld, tps_L=r.n * r.l if r.kind == "tpq" else None)
+            autotune(m, R)
+            m.close()
+
+
 def run_plain(req: Request) -> dict:
     """One request alone through the plain path (model, context and whole-run
-    driver per request, as a caller without the serving loop would)."""
+    driver per request, as a caller without the serving loop would), with the
+    autotuner's plan for its lattice and vector count (cached after the first)."""
     import torch
     cl = cluster_for_sites(req.n)
     cpl, fld = req.couplings()
     out = {"rid": req.rid, "kind": req.kind, "n": req.n}
+    from .tune import autotune
     if req.kind == "lanczos":
         m = api.Model.from_couplings(cl, cpl, field=fld)
+        autotune(m, 1)
         ctx = api.Context(m, R=1)
         v = torch.empty(m.dim, dtype=torch.complex128, device="cuda")
         ctx.fill_gaussian(req.seed, v)
@@ -490,6 +520,7 @@ def run_plain(req: Request) -> dict:
     elif req.kind == "tpq":
         L = req.n * req.l
         m = api.Model.from_couplings(cl, cpl, field=fld, tps_L=L)
+        autotune(m, req.nvec)
         ctx = api.Context(m, R=req.nvec)
         v = torch.empty(m.dim * req.nvec, dtype=torch.complex128, device="cuda")
         ctx.fill_gaussian(req.seed, v)
@@ -497,6 +528,8 @@ def run_plain(req: Request) -> dict:
         out["coef"] = r["coef"]
     else:
         m = api.Model.from_couplings(cl, cpl, field=fld)
+        autotune(m, 1)
+        autotune(m, req.nq)
         ctx = api.Context(m, R=1)
         v = torch.empty(m.dim, dtype=torch.complex128, device="cuda")
         ctx.fill_gaussian(req.seed, v)

@@ -5,10 +5,10 @@ Past a few dozen steps a Lanczos chain in finite precision is chaotic: its late
 coefficients depend on the rounding of every step.  The reference's own results
 move with its reduction order (OpenMP thread count, MPI ranks), its compiler's
 rounding and the order in which p_mltply_v3 sums its items.  So a GPU chain is
-compared with the oracle's in two parts: its coefficients within 1e-10 over the
-prefix where all oracle variants agree with one another within 1e-10, and its
-spectrum S(q, w) within 1e-10 or, where larger, ten times the largest spread
-among the oracle variants.  The variants: another OpenMP thread count (1), the
+compared with the oracle's in two parts: its coefficients over the prefix where
+all oracle variants agree with one another within 1e-10, and its spectrum
+S(q, w); each within 1e-10 or, where larger, ten times the largest spread among
+the oracle variants over the same part.  The variants: another OpenMP thread count (1), the
 start vector perturbed at the rounding level, the oracle built with fused
 multiply-adds (PNED_ORACLE_BUILD=fma) and each H.v's items summed in reverse
 order (PNED_ORACLE_ITEM_ORDER=reverse); the last two run as separate processes
@@ -60,8 +60,11 @@ def check_chain(got_a, got_b, ref, others, e0, steps, min_prefix=10, **spec):
     sa, sb = ref
     k = min(stable_prefix(sa, o[0]) for o in others)
     assert k >= min_prefix, k
-    assert rel(got_a[:k], sa[:k]) <= 1e-10, (k, rel(got_a[:k], sa[:k]))
-    assert rel(got_b[:k], sb[:k]) <= 1e-10
+    # over the prefix: 1e-10, or ten times the variants' own spread there where larger
+    sp_a = max(rel(o[0][:k], sa[:k]) for o in others)
+    sp_b = max(rel(o[1][:k], sb[:k]) for o in others)
+    assert rel(got_a[:k], sa[:k]) <= spread_bound(sp_a), (k, rel(got_a[:k], sa[:k]), sp_a)
+    assert rel(got_b[:k], sb[:k]) <= spread_bound(sp_b), (k, rel(got_b[:k], sb[:k]), sp_b)
     d_ref = spectra(sa, sb, e0, steps, lib=O, **spec)
     spread = max(rel(spectra(o[0], o[1], e0, steps, lib=O, **spec), d_ref) for o in others)
     d_gpu = spectra(got_a, got_b, e0, steps, **spec)
