@@ -30,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "lanczos_steps_per_s_N30"
+LOAD_FRACTION = 0.7   # the served latency run's arrival rate, as a fraction of the measured capacity
 UNIT = "steps/s"
 SEED = 20261203
 
@@ -122,7 +123,7 @@ def build_model(n_sites=30, R=1):
 
 
 # single-vector tile kernel by partner-tile staging mode of the plan
-TILE_KERNELS = {0: "hv_tile_kernel", 1: "hv_tile_stage_kernel", 2: "hv_tile_bulk_kernel"}
+TILE_KERNELS = {0: "hv_tile_kernel", 1: "hv_tile_stage_kernel", 2: "hv_tile_bulk_kernel", 3: "hv_tile_tma_kernel"}
 
 
 def cpu_step_timing(n_sites: int, threads: int, samples: int, warmup: int, full: int, slice_log2: int) -> dict:
@@ -739,10 +740,15 @@ def served_section(args, local_rank, n_requests, rate, sweep=()):
     """Serving stream (continuous batching) against the plain one-at-a-time path:
     capacity (all requests queued at once), p50/p99 latency at `rate` (and at
     each rate of `sweep`: the same requests with arrival times rescaled), and the
-    same requests run alone through the plain path."""
+    same requests run alone through the plain path.  rate None: a load the
+    server sustains, LOAD_FRACTION of the capacity just measured (above the
+    capacity the queue grows with the length of the stream and so does every
+    latency figure)."""
     import torch
     from pned_b200 import serve
-    reqs = serve.make_stream(n_requests, rate=rate, seed=SEED, p30=args.p30, min_n30=args.min_n30)
+    auto_rate = rate is None
+    reqs = serve.make_stream(n_requests, rate=1.0 if auto_rate else rate, seed=SEED, p30=args.p30,
+                             min_n30=args.min_n30)
     free, _ = torch.cuda.mem_get_info()
     budget = int(0.85 * free)
     cap_reqs = [serve.Request(**{**q.__dict__, "arrival": 0.0}) for q in reqs]
@@ -756,6 +762,9 @@ def served_section(args, local_rank, n_requests, rate, sweep=()):
     swept = []
     with ClockSampler(local_rank) as clk:
         cap = srv.run(cap_reqs, realtime=True)
+        if auto_rate:   # the stream was drawn at 1 request/s: rescale its arrival times
+            rate = LOAD_FRACTION * len(cap.results) / cap.makespan_s
+            reqs = [serve.Request(**{**q.__dict__, "arrival": q.arrival / rate}) for q in reqs]
         st = srv.run(reqs, realtime=True)
         for r in sweep:
             reqs_r = [serve.Request(**{**q.__dict__, "arrival": q.arrival * rate / r}) for q in reqs]
@@ -791,7 +800,8 @@ def served_section(args, local_rank, n_requests, rate, sweep=()):
                      "slot_occupancy": cap.occupied_slot_steps / max(1, cap.slot_steps), "peak_bytes": cap.peak_bytes,
                      "note": "all requests queued at t=0"},
         "latency": {"rate_per_s": rate, "solves_per_s": s["solves_per_s"], "p50_s": s["p50_latency_s"],
-                    "p99_s": s["p99_latency_s"], "makespan_s": s["makespan_s"]},
+                    "p99_s": s["p99_latency_s"], "makespan_s": s["makespan_s"],
+                    **({"rate_rule": f"{LOAD_FRACTION} x the measured capacity"} if auto_rate else {})},
         **({"latency_sweep": swept} if swept else {}),
         "plain": {"solves_per_s": plain, "sample": k, "mean_s": tp / k,
                   "max_rel_e0_diff_served_vs_plain": max(diffs) if diffs else None},
@@ -860,7 +870,8 @@ def main():
     ap.add_argument("--s1-sites", type=int, default=18)
     ap.add_argument("--s1-vectors", type=int, default=4)
     ap.add_argument("--served-requests", type=int, default=40)
-    ap.add_argument("--served-rate", type=float, default=1.0)
+    ap.add_argument("--served-rate", type=float, default=None,
+                    help="arrival rate of the served section's latency run (default: 0.7 x its measured capacity)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -152,7 +152,11 @@ typedef struct {
     int32_t stage_partner_tiles; /* R = 1, j_bits 3: 1 copies each partner tile into shared memory once
                                     (cp.async); 2 streams own and partner tiles with bulk copies (TMA engine)
                                     through a ring of 32 KB shared-memory stages, one block per SM; 2 needs
-                                    tile rows that keep >= 3 low global bits, else the plan uses 0 */
+                                    tile rows that keep >= 3 low global bits, else the plan uses 0; 3 gathers
+                                    the partners as 0 and brings the tile's own rows, epilogue rows and
+                                    diagonal in with tensor copies (TMA, no multicast); 3 needs every pass's
+                                    tile bits (starting at bit 0) in at most 5 copy dimensions and two
+                                    blocks per SM, else the plan uses 0 */
     int32_t blocks_per_sm; /* R = 1, j_bits 3: 3 builds the gather kernel for three resident blocks per SM
                               (85 registers, faster up to about 2^26 states); else two (the default) */
     int32_t objective;     /* how a pass picks its tile bits: 0 (default) the fewest partner tiles; 1 the

@@ -125,29 +125,6 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
     block_reduce_store<K, VPT>(red, G, VPT, R, a.partials);
 }
 
-// Block sum of one vector's K sums (lanes, then warps, in a fixed order) into
-// dst[0 .. K-1]; the thread's sums are reset.  All threads of the block call it.
-template <int K>
-__device__ __forceinline__ void tile_sums_store(double2 (&red)[K][1], double2 (*s_red)[K], double2 *dst)
-{
-    const uint32_t tid = threadIdx.x;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        for (int off = 16; off >= 1; off >>= 1) {
-            red[k][0].x += __shfl_xor_sync(0xffffffffu, red[k][0].x, off);
-            red[k][0].y += __shfl_xor_sync(0xffffffffu, red[k][0].y, off);
-        }
-        if ((tid & 31u) == 0) s_red[tid >> 5][k] = red[k][0];
-        red[k][0] = make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    if (tid < uint32_t(K)) {
-        double2 sum = make_double2(0.0, 0.0);
-        for (int w = 0; w < kThreads / 32; ++w) sum = cadd(sum, s_red[w][tid]);
-        dst[tid] = sum;
-    }
-}
-
 // Tiled single-vector (R = 1) H.v on the S = 1/2 full basis, one pass of a
 // multi-pass program (each pass owns a subset of the flip masks).  A block owns
 // a tile of 256 * 2^JB states: thread t holds the states of row t (its 8 bits
@@ -1012,6 +989,7 @@ cudaError_t launch_hv(const pned_model *m, const HvArgs &a, int nblocks, cudaStr
 {
     if (!m->tprogs.empty() && a.R == 1 && m->use_tile) {
         if (tile_staged(m)) return launch_tile_staged(m, a, nblocks, st);
+        if (m->tile_stage == 3 && tile_tma_usable(m, a)) return launch_tile_tma(m, a, nblocks, st);
         if (a.K == 1) return launch_tile<1>(m, a, nblocks, st);
         if (a.K == 4) return launch_tile<4>(m, a, nblocks, st);
     }
@@ -1176,7 +1154,20 @@ void build_tile_programs(pned_model *m)
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
         m->tile_bps = (jb == 3 && m->plan1.blocks_per_sm == 3) ? 3 : tile_blocks_per_sm(jb);
-        m->tile_stage = std::max(0, std::min(2, m->plan1.stage_partner_tiles));
+        m->tile_stage = std::max(0, std::min(3, m->plan1.stage_partner_tiles));
+        if (m->tile_stage == 3) {
+            // own rows, epilogue rows and diagonal by tensor copies: 8 rows a thread, every
+            // pass's tile within 5 copy dimensions, two blocks' shared memory per SM
+            m->tma_geom.assign(m->tprogs.size(), TmaGeom{});
+            bool ok = jb == 3 && tile_tma_encoder() != nullptr;
+            for (size_t p = 0; ok && p < m->tprogs.size(); ++p) ok = tile_tma_geometry(*m->tprogs[p], m->tma_geom[p]);
+            const size_t smem = tile_tma_smem(m);
+            int optin = 0;
+            if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerMultiprocessor, m->device) != cudaSuccess)
+                optin = 0;
+            ok = ok && 2 * (smem + 1024) <= size_t(optin);
+            if (!ok) m->tile_stage = 0;
+        }
         // own tile, and for up to 8 rows a thread the staged epilogue rows, then the table
         m->tile_smem = sizeof(double2) * ((jb <= 3 ? 2 : 1) * size_t(kThreads) * (1 << jb) + std::max(1, m->ntab));
         m->use_tile = true;

@@ -41,7 +41,10 @@ struct pned_model {
     int tile_bps = 2;                       // resident blocks per SM the single-vector tile kernel is built for
     bool carveout = true;                   // size the shared-memory carveout to the tiles (rest L1)
     int tile_stage = 0;                     // single-vector partner tiles: 0 gathered through L1/L2,
-                                            // 1 staged in shared memory (cp.async), 2 streamed by bulk copies
+                                            // 1 staged in shared memory (cp.async), 2 streamed by bulk copies,
+                                            // 3 gathered as 0 with the tile's own rows, epilogue rows and
+                                            // diagonal copied in by the tensor-copy engine
+    std::vector<pned::TmaGeom> tma_geom;    // stage 3: copy geometry of each pass's tile
     int bulk_stages = 0;                    // shared-memory stages of the bulk-copy pipeline
     int nsm = 148;
     double2 *d_table = nullptr;
@@ -179,6 +182,14 @@ int sector_grid(const pned_model *m, int nblocks);
 cudaError_t launch_sector(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
 // True when the plan runs a staged variant of the single-vector tile kernel.
 inline bool tile_staged(const pned_model *m) { return m->tile_stage == 2 || (m->tile_stage == 1 && m->tile_jb == 3); }
+// Stage 3 (tile kernel with tensor copies): the driver's tensor-map encoder (null: unavailable),
+// a pass's copy geometry, the kernel's dynamic shared memory, whether a call's vectors suit the
+// copies (16-byte aligned), and the launch.
+void *tile_tma_encoder();
+bool tile_tma_geometry(const TileProgram &p, TmaGeom &g);
+size_t tile_tma_smem(const pned_model *m);
+bool tile_tma_usable(const pned_model *m, const HvArgs &a);
+cudaError_t launch_tile_tma(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
 // All passes of the staged single-vector tile kernel (cp.async or bulk copies).
 cudaError_t launch_tile_staged(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st);
 // Number of partial-sum blocks launch_hv writes for this model, R and grid
@@ -243,6 +254,29 @@ __device__ __forceinline__ int digit_at(uint64_t digits, int j) { return int((di
 // Block-level reduction of red[K][VPT] (vector r = g*vpt + j, or g + j*G when
 // STRIDED; g = lane % G, G a power of two dividing 32) into
 // partials[slot][K][R] (slot < 0: blockIdx.x).
+// Block sum of one vector's K sums (lanes, then warps, in a fixed order) into
+// dst[0 .. K-1]; the thread's sums are reset.  All threads of the block call it.
+template <int K>
+__device__ __forceinline__ void tile_sums_store(double2 (&red)[K][1], double2 (*s_red)[K], double2 *dst)
+{
+    const uint32_t tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        for (int off = 16; off >= 1; off >>= 1) {
+            red[k][0].x += __shfl_xor_sync(0xffffffffu, red[k][0].x, off);
+            red[k][0].y += __shfl_xor_sync(0xffffffffu, red[k][0].y, off);
+        }
+        if ((tid & 31u) == 0) s_red[tid >> 5][k] = red[k][0];
+        red[k][0] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (tid < uint32_t(K)) {
+        double2 sum = make_double2(0.0, 0.0);
+        for (int w = 0; w < kThreads / 32; ++w) sum = cadd(sum, s_red[w][tid]);
+        dst[tid] = sum;
+    }
+}
+
 template <int K, int VPT, bool STRIDED = false>
 __device__ __forceinline__ void block_reduce_store(double2 (&red)[K][VPT], int G, int vpt, int R, double2 *partials,
                                                    int64_t slot = -1)

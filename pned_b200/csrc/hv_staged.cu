@@ -1,6 +1,10 @@
 // Staged variants of the single-vector S = 1/2 tile kernel, chosen by the
 // plan: partner tiles copied into shared memory with cp.async (stage 1) or
-// with cp.async.bulk under mbarriers by a producer warp (stage 2).
+// with cp.async.bulk under mbarriers by a producer warp (stage 2); or the
+// gather kernel with the tile's own rows, its epilogue rows and its diagonal
+// brought in by tensor copies (stage 3).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -562,6 +566,388 @@ cudaError_t launch_tile_staged(const pned_model *m, const HvArgs &a, int nblocks
     if (!tile_staged(m)) return cudaErrorInvalidValue;
     if (a.K == 1) return launch_staged_k<1>(m, a, nblocks, st);
     if (a.K == 4) return launch_staged_k<4>(m, a, nblocks, st);
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// Tile kernel with tensor copies of the tile's own rows (stage 3)
+// ---------------------------------------------------------------------------
+// Every flip term moves a 16-byte value through the SM's load/store data path
+// per state, from shared memory or from L1/L2, and that path bounds the gather
+// kernel.  Its own-row traffic rides the same path: the tile's rows of C are
+// loaded and stored into shared memory, and the epilogue rows of P or W are
+// copied in with cp.async and read back.  Here the tensor-copy engine writes
+// the tile's rows of C, of P or W and of the diagonal straight into shared
+// memory, outside that path; per state and pass that leaves the epilogue's two
+// shared reads (three in the first pass) and the store of W beside the terms.
+// The copies are issued by one thread when the tile starts and land while the
+// block gathers the out-of-tile terms through L1/L2; the in-tile terms follow
+// once the own rows have arrived, the diagonal term is added in the epilogue.
+// The same tiles, passes and terms as hv_tile_kernel with 8 rows a thread; W
+// agrees to rounding (the diagonal term is added last instead of first).
+
+// Tensor maps of one pass: C (own rows), P or W (epilogue rows), diagonal.
+struct TmaMaps {
+    CUtensorMap c, pw, d;
+    TmaGeom g;
+    uint32_t bytes_c, bytes_pw, bytes_d;   // bytes of each copy (0: not copied)
+};
+
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+
+// One box of a tensor map into shared memory (no multicast), counted in bytes
+// on the mbarrier.
+__device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *map, const int (&c)[kTmaMaxRank], int rank,
+                                        uint32_t bar)
+{
+    const uint64_t tm = reinterpret_cast<uint64_t>(map);
+    switch (rank) {
+    case 1:
+        asm volatile("cp.async.bulk.tensor.1d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2}], [%3];\n"
+                     ::"r"(dst), "l"(tm), "r"(c[0]), "r"(bar) : "memory");
+        break;
+    case 2:
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                     "[%4];\n" ::"r"(dst), "l"(tm), "r"(c[0]), "r"(c[1]), "r"(bar) : "memory");
+        break;
+    case 3:
+        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+                     "[%5];\n" ::"r"(dst), "l"(tm), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(bar) : "memory");
+        break;
+    case 4:
+        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+                     "%5}], [%6];\n" ::"r"(dst), "l"(tm), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(bar) : "memory");
+        break;
+    default:
+        asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+                     "%5, %6}], [%7];\n" ::"r"(dst), "l"(tm), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]),
+                     "r"(bar) : "memory");
+        break;
+    }
+}
+
+constexpr int kTmaSPT = 8;                          // rows a thread
+constexpr int kTmaTile = kThreads * kTmaSPT;        // 2048 states
+
+template <bool RC, bool RD, int K>
+__global__ void __launch_bounds__(kThreads, 2)
+    hv_tile_tma_kernel(const __grid_constant__ TileProgram prog, const HvArgs a, const __grid_constant__ TmaMaps tm)
+{
+    constexpr int SPT = kTmaSPT;
+    constexpr int TILE = kTmaTile;
+    extern __shared__ unsigned char tma_raw[];
+    // copies land at 128-byte aligned addresses
+    unsigned char *tma_smem = tma_raw + ((128u - (smem_addr(tma_raw) & 127u)) & 127u);
+    double2 *s_v = reinterpret_cast<double2 *>(tma_smem);   // own rows of C
+    double2 *s_pw = s_v + TILE;                             // rows of P (first pass) or W (later passes)
+    double2 *s_dc = s_pw + TILE;                            // diagonal (complex; real: the first half as doubles)
+    const double *s_dr = reinterpret_cast<const double *>(s_dc);
+    double2 *s_tab = s_dc + (RD ? TILE / 2 : TILE);
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_next[2];
+    __shared__ int s_abort;
+    __shared__ double2 s_red[kThreads / 32][K];
+    const uint32_t tid = threadIdx.x;
+    for (int i = tid; i < prog.ntab; i += blockDim.x) s_tab[i] = a.table[i];
+    const uint32_t bar_v = smem_addr(&s_bar[0]), bar_e = smem_addr(&s_bar[1]);
+    uint32_t *const ctr = a.tile_counter ? a.tile_counter + prog.pass : nullptr;
+    if (tid == 0) {
+        mbar_init(bar_v, 1);
+        mbar_init(bar_e, 1);
+        fence_mbar_init();
+        s_abort = 0;
+        s_next[0] = ctr ? atomicAdd(ctr, 1u) : 0u;
+    }
+    const int64_t ntiles = int64_t(1) << prog.nouter;
+    const bool pw_on = prog.first ? a.P != nullptr : true;
+    const double sc = a.sc[0], pc = a.pc ? a.pc[0] : 0.0, gs = a.gsc ? a.gsc[0] : 0.0;
+    const double hs = a.hsc ? a.hsc[0] : sc;
+    const double shift = a.shift + (a.shiftv ? a.shiftv[0] : 0.0);
+    uint32_t rowbase = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) rowbase |= ((tid >> k) & 1u) << prog.rowpos[k];
+    double2 red[K][1];
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k][0] = make_double2(0.0, 0.0);
+    uint32_t phase = 0;
+    int fail = 0;
+    bool gave_up = false;
+    for (uint32_t it = 0;; ++it) {
+        // the previous tile's shared reads are done and s_next[it & 1] is set; a wait
+        // that gave up anywhere in the block ends the loop for every thread
+        if (__syncthreads_or(fail)) {
+            gave_up = true;
+            break;
+        }
+        const int64_t tile = ctr ? int64_t(s_next[it & 1u]) : int64_t(blockIdx.x) + int64_t(it) * gridDim.x;
+        if (tile >= ntiles) break;
+        uint32_t tbase = 0;
+        for (int k = 0; k < prog.nouter; ++k) tbase |= uint32_t((tile >> k) & 1) << prog.outer[k];
+        const uint32_t base = rowbase | tbase;
+        if (tid == 0) {
+            if (ctr) s_next[(it + 1u) & 1u] = atomicAdd(ctr, 1u);
+            int c[kTmaMaxRank];
+#pragma unroll
+            for (int d = 0; d < kTmaMaxRank; ++d)
+                c[d] = (d < tm.g.rank && !tm.g.tile[d]) ? int((tbase >> tm.g.lo[d]) & ((1u << tm.g.nbits[d]) - 1u)) : 0;
+            fence_proxy_async_smem();   // the previous tile's reads of these buffers come first
+            mbar_arrive_expect_tx(bar_v, tm.bytes_c);
+            tma_box(smem_addr(s_v), &tm.c, c, tm.g.rank, bar_v);
+            mbar_arrive_expect_tx(bar_e, (pw_on ? tm.bytes_pw : 0u) + (prog.first ? tm.bytes_d : 0u));
+            if (pw_on) tma_box(smem_addr(s_pw), &tm.pw, c, tm.g.rank, bar_e);
+            if (prog.first) tma_box(smem_addr(s_dc), &tm.d, c, tm.g.rank, bar_e);
+        }
+        double2 acc[SPT];
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) acc[j] = make_double2(0.0, 0.0);
+        // flip masks leaving the tile first: partners through L1/L2 while the own rows arrive
+        for (int t = prog.nin; t < prog.nterms; ++t) {
+            const TileTerm T = prog.t[t];
+            const uint32_t pbx = base ^ T.mask;
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            double2 w0[SPT];
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + (pbx ^ prog.jexp[j]));
+            if (!T.hasj) {
+                const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
+                    else acc[j] = cfma(c, w0[j], acc[j]);
+                }
+                continue;
+            }
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const double2 c = s_tab[T.tab + (ib | uint32_t((T.jtab >> (4 * j)) & 15u))];
+                if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
+                else acc[j] = cfma(c, w0[j], acc[j]);
+            }
+        }
+        const bool okv = mbar_wait_or_abort(bar_v, phase, &s_abort);
+        // flip masks inside the tile: partners from shared memory
+        for (int t = 0; t < prog.nin; ++t) {
+            const TileTerm T = prog.t[t];
+            uint32_t ib = 0;
+#pragma unroll
+            for (int d = 0; d < kMaxDeps; ++d)
+                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+            const double2 *sv = s_v + (tid ^ (T.mask & 0xffu));
+            const uint32_t mhi = T.mask >> 8;
+            if (!T.hasj) {
+                const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) {
+                    const double2 w = sv[kThreads * (j ^ mhi)];
+                    if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                    else acc[j] = cfma(c, w, acc[j]);
+                }
+                continue;
+            }
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
+                const double2 w = sv[kThreads * (j ^ mhi)];
+                if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
+                else acc[j] = cfma(c, w, acc[j]);
+            }
+        }
+        const bool oke = mbar_wait_or_abort(bar_e, phase, &s_abort);
+        phase ^= 1u;
+        if (!(okv && oke)) {
+            fail = 1;
+            s_abort = 1;
+            if (a.err) atomicExch(a.err, 1);
+        }
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            const int sl = int(tid) + kThreads * j;
+            const int64_t e = base | prog.jexp[j];
+            const double2 v = s_v[sl];
+            double2 hsum = acc[j];
+            if (prog.first) {
+                if (RD) {
+                    const double dd = s_dr[sl] - shift;
+                    hsum.x = fma(dd, v.x, hsum.x);
+                    hsum.y = fma(dd, v.y, hsum.y);
+                } else {
+                    double2 dd = s_dc[sl];
+                    dd.x -= shift;
+                    hsum = cfma(dd, v, hsum);
+                }
+            }
+            const double2 hv = cscale(hs, hsum);
+            double2 out = hv;
+            if (!prog.first) {
+                const double2 w0 = s_pw[sl];
+                out.x += w0.x;
+                out.y += w0.y;
+            } else if (a.P) {
+                const double2 p = s_pw[sl];
+                out.x = fma(pc, p.x, out.x);
+                out.y = fma(pc, p.y, out.y);
+            }
+            if (!fail) __stcs(a.W + e, out);
+            const double2 vv = cscale(sc, v);
+            red[0][0] = cadd(red[0][0], cconjmul(vv, hv));
+            if (!prog.last) continue;
+            if (K >= 2) red[1][0].x += out.x * out.x + out.y * out.y;
+            if (K >= 4 && a.G) {
+                const double2 gv = cscale(gs, a.G[e]);
+                red[2][0] = cadd(red[2][0], cconjmul(gv, out));
+                red[3][0] = cadd(red[3][0], cconjmul(gv, vv));
+            }
+        }
+        // per-tile sums in a fixed order (dynamic order: independent of which block took the tile)
+        if (ctr) tile_sums_store<K>(red, s_red, a.partials + size_t(tile) * K);
+    }
+    if (!ctr) tile_sums_store<K>(red, s_red, a.partials + size_t(blockIdx.x) * K);
+    // after a wait gave up: wait (bounded) for the last tile's copies before the block's
+    // shared memory is released
+    if (gave_up && tid == 0) {
+        mbar_wait(bar_v, phase ^ 1u);
+        mbar_wait(bar_e, phase ^ 1u);
+    }
+}
+
+void *tile_tma_encoder()
+{
+    static void *fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = f;
+    });
+    return fn;
+}
+
+bool tile_tma_geometry(const TileProgram &p, TmaGeom &g)
+{
+    g = TmaGeom{};
+    if (p.tbits != 8 || p.jb != 3 || p.n > 32) return false;
+    uint32_t tmask = 0;
+    for (int k = 0; k < 8; ++k) tmask |= 1u << p.rowpos[k];
+    tmask |= p.jexp[7];
+    // shared memory holds the tile as [j][row]: its bits in ascending order must be
+    // the 8 row bits, then the 3 j bits, starting at bit 0
+    int bits[32], nb = 0;
+    for (int b = 0; b < p.n; ++b)
+        if ((tmask >> b) & 1u) bits[nb++] = b;
+    if (nb != 11 || bits[0] != 0) return false;
+    for (int k = 0; k < 8; ++k)
+        if (bits[k] != p.rowpos[k]) return false;
+    for (int k = 0; k < 3; ++k)
+        if ((1u << bits[8 + k]) != p.jexp[1u << k]) return false;
+    for (int b = 0; b < p.n;) {
+        const bool in = (tmask >> b) & 1u;
+        int e = b;
+        while (e < p.n && (((tmask >> e) & 1u) != 0) == in) ++e;
+        for (int s = b; s < e;) {
+            const int len = std::min(in ? (g.rank == 0 ? 7 : 8) : 31, e - s);
+            if (g.rank == kTmaMaxRank) return false;
+            g.lo[g.rank] = s;
+            g.nbits[g.rank] = len;
+            g.tile[g.rank] = in ? 1 : 0;
+            ++g.rank;
+            s += len;
+        }
+        b = e;
+    }
+    return true;
+}
+
+size_t tile_tma_smem(const pned_model *m)
+{
+    const size_t tile = size_t(kTmaTile);
+    return 128 + sizeof(double2) * (2 * tile + (m->real_diag ? tile / 2 : tile) + size_t(std::max(1, m->ntab)));
+}
+
+bool tile_tma_usable(const pned_model *m, const HvArgs &a)
+{
+    auto al = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    return a.R == 1 && m->tma_geom.size() == m->tprogs.size() && tile_tma_encoder() && al(a.C) && al(a.W) &&
+           al(a.P) && al(a.diag);
+}
+
+// Tensor map of one vector (complex: 16-byte states, or real doubles) over the
+// pass's copy dimensions, box = the tile.
+static bool encode_tile_map(CUtensorMap *map, const TmaGeom &g, const void *base, bool complex)
+{
+    auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(tile_tma_encoder());
+    if (!fn || g.rank < 1) return false;
+    cuuint64_t dims[kTmaMaxRank], strides[kTmaMaxRank];
+    cuuint32_t box[kTmaMaxRank], estr[kTmaMaxRank];
+    const cuuint64_t es = complex ? 16 : 8;
+    for (int d = 0; d < g.rank; ++d) {
+        dims[d] = cuuint64_t(1) << g.nbits[d];
+        if (d == 0 && complex) dims[0] *= 2;   // elements are doubles
+        box[d] = g.tile[d] ? cuuint32_t(dims[d]) : 1u;
+        estr[d] = 1;
+        if (d > 0) strides[d - 1] = (cuuint64_t(1) << g.lo[d]) * es;
+    }
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, cuuint32_t(g.rank), const_cast<void *>(base), dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <bool RC, bool RD, int K>
+static cudaError_t launch_tile_tma_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    auto kern = hv_tile_tma_kernel<RC, RD, K>;
+    const size_t smem = tile_tma_smem(m);
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
+    if (e == cudaSuccess && m->carveout) e = set_carveout(reinterpret_cast<const void *>(kern), m->device, smem, 2);
+    if (e != cudaSuccess) return e;
+    const int grid = tile_grid(m, nblocks);
+    const bool dyn = tile_dynamic(m, a, nblocks);
+    HvArgs b = a;
+    if (!dyn) b.tile_counter = nullptr;
+    else if ((e = cudaMemsetAsync(a.tile_counter, 0, sizeof(uint32_t) * kTileMaxPasses, st)) != cudaSuccess)
+        return e;
+    size_t off = 0;
+    for (size_t p = 0; p < m->tprogs.size(); ++p) {
+        const TileProgram &pg = *m->tprogs[p];
+        TmaMaps tm{};
+        tm.g = m->tma_geom[p];
+        const double2 *pw = pg.first ? a.P : a.W;
+        bool ok = encode_tile_map(&tm.c, tm.g, a.C, true);
+        if (pw) ok = ok && encode_tile_map(&tm.pw, tm.g, pw, true);
+        if (pg.first) ok = ok && encode_tile_map(&tm.d, tm.g, a.diag, !RD);
+        if (!ok) return cudaErrorInvalidValue;
+        tm.bytes_c = uint32_t(kTmaTile * sizeof(double2));
+        tm.bytes_pw = pw ? uint32_t(kTmaTile * sizeof(double2)) : 0u;
+        tm.bytes_d = pg.first ? uint32_t(kTmaTile * (RD ? sizeof(double) : sizeof(double2))) : 0u;
+        b.partials = a.partials + off;
+        off += dyn ? (size_t(1) << pg.nouter) * K : size_t(grid) * K;
+        kern<<<grid, kThreads, smem, st>>>(pg, b, tm);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <int K>
+static cudaError_t launch_tile_tma_k(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    if (m->real_coef && m->real_diag) return launch_tile_tma_t<true, true, K>(m, a, nblocks, st);
+    if (m->real_diag) return launch_tile_tma_t<false, true, K>(m, a, nblocks, st);
+    return launch_tile_tma_t<false, false, K>(m, a, nblocks, st);
+}
+
+cudaError_t launch_tile_tma(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
+{
+    if (a.K == 1) return launch_tile_tma_k<1>(m, a, nblocks, st);
+    if (a.K == 4) return launch_tile_tma_k<4>(m, a, nblocks, st);
     return cudaErrorInvalidValue;
 }
 

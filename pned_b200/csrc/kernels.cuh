@@ -77,6 +77,20 @@ struct TileProgram {
     TileTerm t[kMaxTerms];
 };
 
+// Tensor-copy geometry of a single-vector tile (a pass's rows and j bits, in
+// ascending global bit order, as the tile is laid out in shared memory): the
+// global bits split into up to 5 copy dimensions, each a run of bits, either
+// all tile bits (copied whole) or all outer bits (one position, the tile's).
+// Dimension 0 starts at bit 0 and holds at most 7 bits (a box row of at most
+// 256 doubles of complex data), the other tile runs at most 8.
+constexpr int kTmaMaxRank = 5;
+struct TmaGeom {
+    int rank = 0;
+    int lo[kTmaMaxRank] = {};      // lowest global bit of the dimension
+    int nbits[kTmaMaxRank] = {};   // its bits
+    int tile[kTmaMaxRank] = {};    // 1: tile bits (box spans it), 0: outer bits (box of 1)
+};
+
 // Per-call scalars: W = pc_r * P + sc_r * (H - shift) (sc_r * C); all from device memory.
 struct HvArgs {
     const double2 *C;       // input vectors (scaled by sc)

@@ -30,7 +30,12 @@ CANDIDATES_1 = [(8, 10, 4, 3), (8, 8, 2, 3), (8, 10, 1, 3), (5, 8, 1, 3), (5, 10
                 # objective 1: tiles that hold the most flip terms
                 (5, 10, 2, 3, 1, 0, -1, 1), (5, 8, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1),
                 (5, 9, 2, 4, 1, 0, -1, 1), (5, 11, 2, 4, 1, 0, -1, 1), (5, 10, 2, 3, 1, 0, 3, 1),
-                (8, 8, 2, 3, 1, 0, -1, 1), (5, 10, 3, 4, 1, 0, -1, 1)]
+                (8, 8, 2, 3, 1, 0, -1, 1), (5, 10, 3, 4, 1, 0, -1, 1),
+                # own rows, epilogue rows and diagonal by tensor copies (plans whose tiles
+                # fit the copy geometry; the others are skipped)
+                (5, 8, 2, 3, 1, 3, -1, 1), (5, 7, 2, 3, 1, 3, -1, 1), (5, 9, 2, 3, 1, 3, -1, 1),
+                (5, 10, 2, 3, 1, 3, -1, 1), (5, 6, 2, 3, 1, 3, -1, 1), (5, 4, 2, 3, 1, 3, -1, 1),
+                (5, 12, 2, 3, 1, 3, -1, 1), (5, 8, 3, 3, 1, 3, -1, 1)]
 CANDIDATES_R = [(-1, -1, -1), (0, 6, 2), (0, 8, 2), (0, 10, 2), (1, 10, 2), (3, 10, 2), (0, 10, 1),
                 # objective 1: tiles on the bits that hold the most flip terms (rows need no low
                 # bits: a state's R values are already a contiguous run)
@@ -87,6 +92,8 @@ def autotune(model, R: int = 1, reps: int = 2, candidates=None, cache_path: str 
         plan = model.set_plan(R, *c)
         if R == 1 and plan["tile_passes"] == 0:
             break                      # no tiled kernel for this model: nothing to tune
+        if R == 1 and len(c) > 5 and c[5] == 3 and plan.get("staging") != 3:
+            continue                   # tiles outside the tensor-copy geometry: the plan fell back
         tried.append({"plan": list(c), "ms": _time_hv(ctx, v1, v0, reps), "partner_tiles": plan["partner_tiles"],
                       "passes": plan["tile_passes"]})
     del v1, v0

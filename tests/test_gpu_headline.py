@@ -6,7 +6,8 @@ tiles keep a 12-bit L2 window and split the 45 flip masks over two passes,
 structure that the 16- and 24-site clusters of the other parity tests never
 reach.  Each plan the autotuner chooses between at these sizes (8- and 16-row
 tiles, two or three resident blocks per SM, partner tiles streamed by the
-bulk-copy engine, tiles that hold the most flip terms) and the plan it
+bulk-copy engine, own rows brought in by tensor copies, tiles that hold the
+most flip terms) and the plan it
 actually picks run one H.v through the C ABI on device vectors; the oracle (p_mltply_v3 of the reference's lnp = 1 path,
 S_one_half/Hybrid_TPS_parallel.f90:190-263, 415-440) gathers from the same
 full input vector and computes three output slices of 2^20 states -- the
@@ -39,9 +40,9 @@ EPERBD = 0.0625
 #  objective]); objective 1 picks tiles that hold the most flip terms
 PLANS = {
     30: [(5, 12, 2, 3), (5, 12, 2, 3, 1, 0, 3), (5, 11, 2, 4), (5, 10, 2, 3, 1, 2),
-         (5, 10, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1)],
+         (5, 10, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1)],
     28: [(5, 12, 2, 3), (5, 10, 2, 3, 1, 0, 3), (5, 11, 2, 4), (5, 10, 2, 3, 1, 2),
-         (5, 10, 2, 3, 1, 0, -1, 1), (5, 9, 2, 4, 1, 0, -1, 1)],
+         (5, 10, 2, 3, 1, 0, -1, 1), (5, 9, 2, 4, 1, 0, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1)],
 }
 
 
@@ -81,8 +82,8 @@ def test_headline_hv_slices_match_oracle(n_sites):
     for plan in plans:
         got = gm.set_plan(1, *plan)
         assert got["tile_passes"] >= 2, plan
-        if len(plan) > 5 and plan[5] == 2:
-            assert got["staging"] == 2, plan
+        if len(plan) > 5 and plan[5] in (2, 3):
+            assert got["staging"] == plan[5], plan
         ctx = P.Context(gm, R=1)
         w.zero_()
         torch.cuda.synchronize()

@@ -396,17 +396,20 @@ def test_session_checkpoint_resumes_exactly(kind, tmp_path):
                                   (5, 12, 2, 1, 0, 0), (8, 10, 4, 3, 1, 2), (5, 10, 2, 3, 1, 2), (3, 8, 1, 3, 1, 2),
                                   (5, 6, 3, 3, 1, 2), (8, 8, 2, 3, 1, 0, 3), (5, 10, 2, 3, 1, 0, 3),
                                   (5, 8, 2, 4, 1, 0), (8, 10, 4, 4, 1, 0), (3, 6, 1, 4, 0, 0),
-                                  (5, 6, 2, 3, 1, 0, -1, 1), (5, 4, 2, 4, 1, 0, -1, 1), (5, 6, 2, 3, 1, 0, 3, 1)])
+                                  (5, 6, 2, 3, 1, 0, -1, 1), (5, 4, 2, 4, 1, 0, -1, 1), (5, 6, 2, 3, 1, 0, 3, 1),
+                                  (5, 6, 2, 3, 1, 3, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1), (5, 6, 3, 3, 0, 3, -1, 1)])
 def test_tile_plans_agree_with_oracle(plan):
     """Every tile plan the autotuner may pick (rows kept, window, passes, rows per
-    thread, carveout, staged or bulk-streamed partner tiles, tiles that hold the
-    most terms) gives the oracle's H.v to 1e-12."""
+    thread, carveout, staged or bulk-streamed partner tiles, own rows by tensor
+    copies, tiles that hold the most terms) gives the oracle's H.v to 1e-12."""
     cl = honeycomb(2, 4)
     gm, om = models(cl, 2, 0, KHGH, FIELD)
     got = gm.set_plan(1, *plan)
     assert got["tile_passes"] >= 1
     if plan[5] == 2:
         assert got["staging"] == 2 and got["ring_stages"] >= 2
+    if plan[5] == 3:
+        assert got["staging"] == 3
     ctx = P.Context(gm, R=1)
     rng = np.random.default_rng(23)
     v1 = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
@@ -450,6 +453,52 @@ def test_bulk_streamed_tiles_match_gathered_tiles(plan):
     assert abs(out[0][1][0] - out[2][1][0]) <= 1e-12 * abs(out[0][1][0])
     assert rel(out[0][2], out[2][2]) <= 1e-12 and rel(out[0][3], out[2][3]) <= 1e-12
     gm.set_plan(1)
+
+
+@pytest.mark.parametrize("plan", [(5, 6, 2, 3, 1, 3, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1), (5, 4, 2, 3, 1, 3, -1, 1)])
+def test_tensor_copied_tiles_lanczos_tps_and_noalloc(plan):
+    """N = 24, two passes: the tile kernel whose own rows, epilogue rows and
+    diagonal arrive by tensor copies (stage 3) gives the oracle's H.v to 1e-12
+    (and the gather kernel's with the same tiles), the oracle's Lanczos and
+    one-vector TPS coefficients to 1e-10 (the TPS pass forms the K = 4 sums),
+    and the same H.v through the allocation-free entry point (static tile order)."""
+    cl = honeycomb(3, 4)
+    gm, om = models(cl, 2, 0, KHGH, FIELD)
+    got = gm.set_plan(1, *plan)
+    assert got["staging"] == 3 and got["tile_passes"] == 2
+    rng = np.random.default_rng(31)
+    v1 = rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim)
+    v0 = 0.1 * (rng.standard_normal(gm.dim) + 1j * rng.standard_normal(gm.dim))
+    ctx = P.Context(gm, R=1)
+    w = v0.copy()
+    pr = ctx.p_mltply_v3(v1, w, 0.0625)
+    ref = v0.copy()
+    prr = om.p_mltply_v3(v1, ref, 0.0625)
+    assert rel(w, ref) <= 1e-12 and abs(pr[0] - prr) <= 1e-12 * abs(prr)
+    t1 = torch.from_numpy(v1).cuda()
+    t0 = torch.from_numpy(v0).cuda()
+    prn = P.hv_noalloc(gm, 1, t1, t0, 0.0625)
+    torch.cuda.synchronize()
+    assert rel(t0.cpu().numpy(), ref) <= 1e-12 and abs(prn[0] - prr) <= 1e-12 * abs(prr)
+    v = O.gaussian(5, gm.dim)
+    v /= np.linalg.norm(v)
+    out = ctx.lanczos(v, 30)
+    refl = om.lanczos(v, 30)
+    assert rel(out["alpha"][:20, 0], refl["alpha"][:20]) <= 1e-10
+    assert abs(out["ene"][0] - refl["ene"][0]) <= 1e-10 * abs(refl["ene"][0])
+    ctx.close()
+    gm.set_plan(1, *plan[:5], 0, *plan[6:])   # the same tiles gathered through L1/L2
+    assert gm.plan(1)["staging"] == 0
+    w0 = v0.copy()
+    P.Context(gm, R=1).p_mltply_v3(v1, w0, 0.0625)
+    assert rel(w, w0) <= 1e-13
+    L = 2.0 * cl.n
+    gt, ot = models(cl, 2, 0, KHGH, FIELD, tps_L=L)
+    assert gt.set_plan(1, *plan)["staging"] == 3
+    out = P.Context(gt, R=1).tps(L, v, 25)
+    reft = ot.tps(L, v, 25)
+    assert rel(out["beta"][:, 0], reft["beta"]) <= 1e-10
+    assert rel(out["coef"][:, 0, :5], reft["coef"][:, :5]) <= 1e-10
 
 
 @pytest.mark.parametrize("plan", [(5, 11, 2, 4), (8, 10, 3, 4)])
