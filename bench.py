@@ -324,6 +324,7 @@ def run_ours(args, rank, world, local_rank):
                                           "j_bits": pl[3] if len(pl) > 3 else -1,
                                           "blocks_per_sm": pl[6] if len(pl) > 6 else -1,
                                           "objective": pl[7] if len(pl) > 7 else 0,
+                                          "terms_in_flight": pl[8] if len(pl) > 8 else -1,
                                           "plan_arg": ",".join(str(x) for x in pl),
                                           "candidates": len(tuning.get("tried", []))}
     if rank == 0 and args.dense_check:

@@ -162,6 +162,8 @@ typedef struct {
     int32_t objective;     /* how a pass picks its tile bits: 0 (default) the fewest partner tiles; 1 the
                               most flip terms inside the tile (each then gathers from shared memory instead
                               of through L1/L2) and window bits that take the most terms into the pass */
+    int32_t terms_in_flight; /* stage 3: the partner rows of 2 out-of-tile terms requested together
+                                (126 registers); else (0, 1, -1: default) one term at a time */
 } pned_tile_plan;
 int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
 /*

@@ -33,7 +33,8 @@ class ModelDesc(C.Structure):
 class TilePlan(C.Structure):
     _fields_ = [("row_fixed_bits", C.c_int32), ("window_bits", C.c_int32), ("max_passes", C.c_int32),
                 ("j_bits", C.c_int32), ("l1_carveout", C.c_int32), ("stage_partner_tiles", C.c_int32),
-                ("blocks_per_sm", C.c_int32), ("objective", C.c_int32)]
+                ("blocks_per_sm", C.c_int32), ("objective", C.c_int32),
+                ("terms_in_flight", C.c_int32)]
 
 
 class Observable(C.Structure):

@@ -300,7 +300,7 @@ def tile_plan_export(desc: "ModelInput", row_fixed_bits: int = -1, window_bits: 
     single-vector plan Model.set_plan builds), computed on the host
     (pned_tile_plan_export): the program's flip terms and, per pass, the tile
     bits, outer order, terms and partner-tile groups."""
-    tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1, int(objective))
+    tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1, int(objective), -1)
     n = C.c_int64(0)
     check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), C.byref(tp), None, 0, C.byref(n)))
     buf = np.zeros(n.value, dtype=np.int64)
@@ -379,10 +379,10 @@ class Model:
 
     def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
                  j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1,
-                 objective: int = -1):
+                 objective: int = -1, terms_in_flight: int = -1):
         """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""
         tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles), int(blocks_per_sm), int(objective))
+                            int(stage_partner_tiles), int(blocks_per_sm), int(objective), int(terms_in_flight))
         check(lib().pned_model_set_plan(self._h, int(R), C.byref(tp)))
         return self.plan(R)
 
@@ -764,9 +764,9 @@ class SlotBatch:
 
     def set_plan(self, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
                  j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1,
-                 objective: int = -1) -> dict:
+                 objective: int = -1, terms_in_flight: int = -1) -> dict:
         tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles), int(blocks_per_sm), int(objective))
+                            int(stage_partner_tiles), int(blocks_per_sm), int(objective), int(terms_in_flight))
         check(lib().pned_slots_set_plan(self._h, C.byref(tp)))
         return self.plan()
 

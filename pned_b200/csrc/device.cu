@@ -1154,6 +1154,7 @@ void build_tile_programs(pned_model *m)
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
         m->tile_bps = (jb == 3 && m->plan1.blocks_per_sm == 3) ? 3 : tile_blocks_per_sm(jb);
+        m->tma_deep = m->plan1.terms_in_flight == 2;
         m->tile_stage = std::max(0, std::min(3, m->plan1.stage_partner_tiles));
         if (m->tile_stage == 3) {
             // own rows, epilogue rows and diagonal by tensor copies: 8 rows a thread, every
@@ -1423,15 +1424,15 @@ extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *p
 {
     if (!m || pick_vpt(R) == 0) return fail(PNED_EINVAL, "pned_model_set_plan: bad arguments");
     if (plan && (plan->max_passes > kTileMaxPasses || plan->window_bits > 30 || plan->row_fixed_bits > 8 ||
-                 plan->j_bits > kTileMaxJB || plan->j_bits == 0 || plan->objective > 1))
+                 plan->j_bits > kTileMaxJB || plan->j_bits == 0 || plan->objective > 1 || plan->terms_in_flight > 2))
         return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
     if (R == 1) {
-        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1, -1, -1};
+        m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1, -1, -1, -1};
         m->carveout = m->plan1.l1_carveout != 0;
         build_tile_programs(m);
         return PNED_OK;
     }
-    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1, -1};
     if (plan) m->carveout = plan->l1_carveout != 0;
     ensure_rtiles(m, R, false, plan ? plan : &def);
     return PNED_OK;

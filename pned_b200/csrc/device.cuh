@@ -45,6 +45,7 @@ struct pned_model {
                                             // 3 gathered as 0 with the tile's own rows, epilogue rows and
                                             // diagonal copied in by the tensor-copy engine
     std::vector<pned::TmaGeom> tma_geom;    // stage 3: copy geometry of each pass's tile
+    bool tma_deep = false;                  // stage 3: partner rows of two out-of-tile terms in flight
     int bulk_stages = 0;                    // shared-memory stages of the bulk-copy pipeline
     int nsm = 148;
     double2 *d_table = nullptr;

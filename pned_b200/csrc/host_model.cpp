@@ -848,7 +848,7 @@ extern "C" int pned_tile_plan_export(const pned_model_desc *d, int row_bits, con
     int rc = compile_program(d, P);
     if (rc) return rc;
     if (P.q != 2 || P.sector) return fail(PNED_ENOTSUP, "pned_tile_plan_export: tiles are planned for the S = 1/2 full basis");
-    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1, -1};
     const pned_tile_plan &pl = plan ? *plan : def;
     if (pl.max_passes > kTileMaxPasses || pl.window_bits > 30 || pl.row_fixed_bits > 8 || pl.j_bits > kTileMaxJB ||
         pl.j_bits == 0 || pl.objective > 1)

@@ -631,9 +631,36 @@ __device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *map, co
 }
 
 constexpr int kTmaSPT = 8;                          // rows a thread
+
+// acc[j] += c_j w[j] for the thread's states, c_j the term's coefficient at the
+// thread's base (and, for terms with dependency bits among the j bits, at its j-th state).
+template <int SPT, bool RC>
+__device__ __forceinline__ void tma_term_apply(const TileTerm &T, uint32_t base, const double2 *s_tab,
+                                               const double2 (&w)[SPT], double2 (&acc)[SPT])
+{
+    uint32_t ib = 0;
+#pragma unroll
+    for (int d = 0; d < kMaxDeps; ++d)
+        if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
+    if (!T.hasj) {
+        const double2 c = s_tab[T.tab + ib];
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            if (RC) { acc[j].x = fma(c.x, w[j].x, acc[j].x); acc[j].y = fma(c.x, w[j].y, acc[j].y); }
+            else acc[j] = cfma(c, w[j], acc[j]);
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < SPT; ++j) {
+        const double2 c = s_tab[T.tab + (ib | uint32_t((T.jtab >> (4 * j)) & 15u))];
+        if (RC) { acc[j].x = fma(c.x, w[j].x, acc[j].x); acc[j].y = fma(c.x, w[j].y, acc[j].y); }
+        else acc[j] = cfma(c, w[j], acc[j]);
+    }
+}
 constexpr int kTmaTile = kThreads * kTmaSPT;        // 2048 states
 
-template <bool RC, bool RD, int K>
+template <bool RC, bool RD, int K, bool DEEP>
 __global__ void __launch_bounds__(kThreads, 2)
     hv_tile_tma_kernel(const __grid_constant__ TileProgram prog, const HvArgs a, const __grid_constant__ TmaMaps tm)
 {
@@ -704,32 +731,29 @@ __global__ void __launch_bounds__(kThreads, 2)
         double2 acc[SPT];
 #pragma unroll
         for (int j = 0; j < SPT; ++j) acc[j] = make_double2(0.0, 0.0);
-        // flip masks leaving the tile first: partners through L1/L2 while the own rows arrive
-        for (int t = prog.nin; t < prog.nterms; ++t) {
+        // flip masks leaving the tile first: partners through L1/L2 while the own rows
+        // arrive, DEEP: the partner rows of two terms in flight at a time
+        int t = prog.nin;
+        if (DEEP) {
+            for (; t + 1 < prog.nterms; t += 2) {
+                const TileTerm T0 = prog.t[t], T1 = prog.t[t + 1];
+                const uint32_t p0 = base ^ T0.mask, p1 = base ^ T1.mask;
+                double2 w0[SPT], w1[SPT];
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + (p0 ^ prog.jexp[j]));
+#pragma unroll
+                for (int j = 0; j < SPT; ++j) w1[j] = __ldg(a.C + (p1 ^ prog.jexp[j]));
+                tma_term_apply<SPT, RC>(T0, base, s_tab, w0, acc);
+                tma_term_apply<SPT, RC>(T1, base, s_tab, w1, acc);
+            }
+        }
+        for (; t < prog.nterms; ++t) {
             const TileTerm T = prog.t[t];
             const uint32_t pbx = base ^ T.mask;
-            uint32_t ib = 0;
-#pragma unroll
-            for (int d = 0; d < kMaxDeps; ++d)
-                if (d < T.nb) ib |= ((base >> ((T.pos4 >> (8 * d)) & 0xffu)) & 1u) << d;
             double2 w0[SPT];
 #pragma unroll
             for (int j = 0; j < SPT; ++j) w0[j] = __ldg(a.C + (pbx ^ prog.jexp[j]));
-            if (!T.hasj) {
-                const double2 c = s_tab[T.tab + ib];
-#pragma unroll
-                for (int j = 0; j < SPT; ++j) {
-                    if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
-                    else acc[j] = cfma(c, w0[j], acc[j]);
-                }
-                continue;
-            }
-#pragma unroll
-            for (int j = 0; j < SPT; ++j) {
-                const double2 c = s_tab[T.tab + (ib | uint32_t((T.jtab >> (4 * j)) & 15u))];
-                if (RC) { acc[j].x = fma(c.x, w0[j].x, acc[j].x); acc[j].y = fma(c.x, w0[j].y, acc[j].y); }
-                else acc[j] = cfma(c, w0[j], acc[j]);
-            }
+            tma_term_apply<SPT, RC>(T, base, s_tab, w0, acc);
         }
         const bool okv = mbar_wait_or_abort(bar_v, phase, &s_abort);
         // flip masks inside the tile: partners from shared memory
@@ -900,10 +924,10 @@ static bool encode_tile_map(CUtensorMap *map, const TmaGeom &g, const void *base
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <bool RC, bool RD, int K>
+template <bool RC, bool RD, int K, bool DEEP>
 static cudaError_t launch_tile_tma_t(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
-    auto kern = hv_tile_tma_kernel<RC, RD, K>;
+    auto kern = hv_tile_tma_kernel<RC, RD, K, DEEP>;
     const size_t smem = tile_tma_smem(m);
     cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void *>(kern), m->device);
     if (e == cudaSuccess && m->carveout) e = set_carveout(reinterpret_cast<const void *>(kern), m->device, smem, 2);
@@ -936,18 +960,19 @@ static cudaError_t launch_tile_tma_t(const pned_model *m, const HvArgs &a, int n
     return cudaSuccess;
 }
 
-template <int K>
+template <int K, bool DEEP>
 static cudaError_t launch_tile_tma_k(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
-    if (m->real_coef && m->real_diag) return launch_tile_tma_t<true, true, K>(m, a, nblocks, st);
-    if (m->real_diag) return launch_tile_tma_t<false, true, K>(m, a, nblocks, st);
-    return launch_tile_tma_t<false, false, K>(m, a, nblocks, st);
+    if (m->real_coef && m->real_diag) return launch_tile_tma_t<true, true, K, DEEP>(m, a, nblocks, st);
+    if (m->real_diag) return launch_tile_tma_t<false, true, K, DEEP>(m, a, nblocks, st);
+    return launch_tile_tma_t<false, false, K, DEEP>(m, a, nblocks, st);
 }
 
 cudaError_t launch_tile_tma(const pned_model *m, const HvArgs &a, int nblocks, cudaStream_t st)
 {
-    if (a.K == 1) return launch_tile_tma_k<1>(m, a, nblocks, st);
-    if (a.K == 4) return launch_tile_tma_k<4>(m, a, nblocks, st);
+    const bool deep = m->tma_deep;
+    if (a.K == 1) return deep ? launch_tile_tma_k<1, true>(m, a, nblocks, st) : launch_tile_tma_k<1, false>(m, a, nblocks, st);
+    if (a.K == 4) return deep ? launch_tile_tma_k<4, true>(m, a, nblocks, st) : launch_tile_tma_k<4, false>(m, a, nblocks, st);
     return cudaErrorInvalidValue;
 }
 

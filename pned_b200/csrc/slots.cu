@@ -847,7 +847,7 @@ extern "C" int pned_slots_set_plan(pned_slots *S, const pned_tile_plan *plan)
         cudaGraphExecDestroy(S->graph);
         S->graph = nullptr;
     }
-    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1};
+    const pned_tile_plan def{-1, -1, -1, -1, -1, -1, -1, -1, -1};
     if (plan) S->tm.carveout = plan->l1_carveout != 0;
     if (S->R == 1) {
         S->tm.plan1 = plan ? *plan : def;

@@ -18,7 +18,8 @@ import os
 
 from . import api
 
-# (row_fixed_bits, window_bits, max_passes[, j_bits[, l1_carveout, stage_partner_tiles, blocks_per_sm[, objective]]]);
+# (row_fixed_bits, window_bits, max_passes[, j_bits[, l1_carveout, stage_partner_tiles, blocks_per_sm[, objective[,
+#  terms_in_flight]]]]);
 # -1 = the library default.  Three resident blocks per SM pay up to about 2^26 states,
 # 16-row tiles (j_bits 4) about 2^28.
 CANDIDATES_1 = [(8, 10, 4, 3), (8, 8, 2, 3), (8, 10, 1, 3), (5, 8, 1, 3), (5, 10, 2, 3), (5, 12, 2, 3),
@@ -35,7 +36,11 @@ CANDIDATES_1 = [(8, 10, 4, 3), (8, 8, 2, 3), (8, 10, 1, 3), (5, 8, 1, 3), (5, 10
                 # fit the copy geometry; the others are skipped)
                 (5, 8, 2, 3, 1, 3, -1, 1), (5, 7, 2, 3, 1, 3, -1, 1), (5, 9, 2, 3, 1, 3, -1, 1),
                 (5, 10, 2, 3, 1, 3, -1, 1), (5, 6, 2, 3, 1, 3, -1, 1), (5, 4, 2, 3, 1, 3, -1, 1),
-                (5, 12, 2, 3, 1, 3, -1, 1), (5, 8, 3, 3, 1, 3, -1, 1)]
+                (5, 12, 2, 3, 1, 3, -1, 1), (5, 8, 3, 3, 1, 3, -1, 1),
+                # the same with the partner rows of two out-of-tile terms in flight
+                (5, 8, 2, 3, 1, 3, -1, 1, 2), (5, 7, 2, 3, 1, 3, -1, 1, 2), (5, 9, 2, 3, 1, 3, -1, 1, 2),
+                (5, 10, 2, 3, 1, 3, -1, 1, 2), (5, 6, 2, 3, 1, 3, -1, 1, 2), (5, 4, 2, 3, 1, 3, -1, 1, 2),
+                (5, 12, 2, 3, 1, 3, -1, 1, 2)]
 CANDIDATES_R = [(-1, -1, -1), (0, 6, 2), (0, 8, 2), (0, 10, 2), (1, 10, 2), (3, 10, 2), (0, 10, 1),
                 # objective 1: tiles on the bits that hold the most flip terms (rows need no low
                 # bits: a state's R values are already a contiguous run)

@@ -37,12 +37,14 @@ SLICE = 1 << 20
 EPERBD = 0.0625
 
 # (row_fixed_bits, window_bits, max_passes, j_bits[, l1_carveout, stage_partner_tiles, blocks_per_sm,
-#  objective]); objective 1 picks tiles that hold the most flip terms
+#  objective, terms_in_flight]); objective 1 picks tiles that hold the most flip terms
 PLANS = {
     30: [(5, 12, 2, 3), (5, 12, 2, 3, 1, 0, 3), (5, 11, 2, 4), (5, 10, 2, 3, 1, 2),
-         (5, 10, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1)],
+         (5, 10, 2, 3, 1, 0, -1, 1), (5, 10, 2, 4, 1, 0, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1),
+         (5, 8, 2, 3, 1, 3, -1, 1, 2)],
     28: [(5, 12, 2, 3), (5, 10, 2, 3, 1, 0, 3), (5, 11, 2, 4), (5, 10, 2, 3, 1, 2),
-         (5, 10, 2, 3, 1, 0, -1, 1), (5, 9, 2, 4, 1, 0, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1)],
+         (5, 10, 2, 3, 1, 0, -1, 1), (5, 9, 2, 4, 1, 0, -1, 1), (5, 8, 2, 3, 1, 3, -1, 1),
+         (5, 8, 2, 3, 1, 3, -1, 1, 2)],
 }
 
 

@@ -42,13 +42,16 @@ def inputs(cl, cpl, fld, tps_L=None):
     return slot_in, om
 
 
-@pytest.mark.parametrize("R", [1, 4])
-def test_slots_lanczos_tps_parity(R):
-    """Each slot carries its own couplings; Lanczos and TPS slots share one H.V."""
+@pytest.mark.parametrize("R,plan", [(1, None), (4, None), (1, (5, 0, 2, 3, 1, 3, -1, 1, 2))])
+def test_slots_lanczos_tps_parity(R, plan):
+    """Each slot carries its own couplings; Lanczos and TPS slots share one H.V
+    (also with a two-pass plan whose tile rows arrive by tensor copies)."""
     cl = honeycomb(3, 2)
     L = 2.0 * cl.n
     steps = 40
     sb = P.SlotBatch(P.ModelInput.structure(cl), R, steps)
+    if plan is not None:
+        assert sb.set_plan(*plan)["tile_passes"] == 2
     kinds = ["lanczos", "tps", "lanczos", "tps"][:max(R, 2)]
     runs = []
     for r, kind in enumerate(kinds):
