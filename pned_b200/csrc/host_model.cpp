@@ -680,6 +680,7 @@ int plan_tiles(const HostProgram &P, int tbits, int jb, int fixed, int window_bi
                     }
                 }
                 q.jtab |= uint64_t(bits) << (4 * j);
+                q.jdep = uint8_t(q.jdep | bits);
             }
             // in-tile terms: the local xor inside the tile; out-of-tile terms: the global xor
             if ((t.xmask & ~tilemask) == 0) {

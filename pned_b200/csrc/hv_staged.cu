@@ -632,6 +632,36 @@ __device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *map, co
 
 constexpr int kTmaSPT = 8;                          // rows a thread
 
+// acc[j] += c_j w[j] for a term with dependency bits among the j bits: c_j at the
+// thread's base ib and its j-th state.  With one such bit the two coefficients are
+// read once and chosen per state (two shared reads instead of one per state).
+template <int SPT, bool RC>
+__device__ __forceinline__ void tma_term_apply_j(const TileTerm &T, uint32_t ib, const double2 *s_tab,
+                                                 const double2 (&w)[SPT], double2 (&acc)[SPT])
+{
+    if (__popc(uint32_t(T.jdep)) == 1) {
+        const double2 c0 = s_tab[T.tab + ib], c1 = s_tab[T.tab + (ib | T.jdep)];
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            const bool on = ((T.jtab >> (4 * j)) & 15u) != 0;
+            if (RC) {
+                const double cx = on ? c1.x : c0.x;
+                acc[j].x = fma(cx, w[j].x, acc[j].x);
+                acc[j].y = fma(cx, w[j].y, acc[j].y);
+            } else {
+                acc[j] = cfma(on ? c1 : c0, w[j], acc[j]);
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < SPT; ++j) {
+        const double2 c = s_tab[T.tab + (ib | uint32_t((T.jtab >> (4 * j)) & 15u))];
+        if (RC) { acc[j].x = fma(c.x, w[j].x, acc[j].x); acc[j].y = fma(c.x, w[j].y, acc[j].y); }
+        else acc[j] = cfma(c, w[j], acc[j]);
+    }
+}
+
 // acc[j] += c_j w[j] for the thread's states, c_j the term's coefficient at the
 // thread's base (and, for terms with dependency bits among the j bits, at its j-th state).
 template <int SPT, bool RC>
@@ -651,12 +681,7 @@ __device__ __forceinline__ void tma_term_apply(const TileTerm &T, uint32_t base,
         }
         return;
     }
-#pragma unroll
-    for (int j = 0; j < SPT; ++j) {
-        const double2 c = s_tab[T.tab + (ib | uint32_t((T.jtab >> (4 * j)) & 15u))];
-        if (RC) { acc[j].x = fma(c.x, w[j].x, acc[j].x); acc[j].y = fma(c.x, w[j].y, acc[j].y); }
-        else acc[j] = cfma(c, w[j], acc[j]);
-    }
+    tma_term_apply_j<SPT, RC>(T, ib, s_tab, w, acc);
 }
 constexpr int kTmaTile = kThreads * kTmaSPT;        // 2048 states
 
@@ -775,13 +800,10 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
                 continue;
             }
+            double2 wi[SPT];
 #pragma unroll
-            for (int j = 0; j < SPT; ++j) {
-                const double2 c = s_tab[T.tab + (ib | ((T.jtab >> (4 * j)) & 15u))];
-                const double2 w = sv[kThreads * (j ^ mhi)];
-                if (RC) { acc[j].x = fma(c.x, w.x, acc[j].x); acc[j].y = fma(c.x, w.y, acc[j].y); }
-                else acc[j] = cfma(c, w, acc[j]);
-            }
+            for (int j = 0; j < SPT; ++j) wi[j] = sv[kThreads * (j ^ mhi)];
+            tma_term_apply_j<SPT, RC>(T, ib, s_tab, wi, acc);
         }
         const bool oke = mbar_wait_or_abort(bar_e, phase, &s_abort);
         phase ^= 1u;

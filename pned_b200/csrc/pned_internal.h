@@ -57,6 +57,7 @@ struct TileTerm {
     uint8_t nb;      // number of dependency bits
     uint8_t hasj;    // 1 if a dependency bit is a j-bit
     uint32_t lmask;  // out-of-tile: local xor of the mask's in-tile part (the offset inside the partner tile)
+    uint8_t jdep;    // the coefficient-index bits that j sets (OR of the jtab nibbles)
 };
 // Tiled mixed-radix (q > 2) pass: the states that agree on all digits but
 // those of the k tile sites form a tile of q^k states, staged in shared

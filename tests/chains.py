@@ -92,10 +92,10 @@ def variant_oracle_chains(cl, X, skip, pt, x, qrs, steps, threads, env):
         return [(r["salpha"][k], r["sbeta"][k]) for k in range(len(qrs))]
 
 
-def oracle_chain_variants(cl, cpl, x, qrs, steps):
+def oracle_chain_variants(cl, cpl, x, qrs, steps, fld=None):
     """The oracle's DSF chains for each momentum (all threads) and its variant runs:
     returns [(ref, [variants...])] per momentum."""
-    X = O.xlocal(2, 0, cpl)
+    X = O.xlocal(2, 0, cpl, field=fld)
     skip, _, pt = O.parity_skip(2, 0, X)
     om = O.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
     nth = O.num_threads()

@@ -13,13 +13,15 @@ import pytest
 import pned_b200 as P
 from oracle import oracle as O
 from pned_b200 import couplings as CP
-from pned_b200.lattice import honeycomb
+from pned_b200.lattice import cluster_for_sites, honeycomb
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 if not torch.cuda.is_available():  # pragma: no cover
     pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from tests.chains import check_chain, oracle_chain_variants  # noqa: E402
 
 
 def rel(a, b):
@@ -195,13 +197,35 @@ def test_gaussian_column_matches_interleaved_fill():
     assert np.max(np.abs(full.view(m.dim, R).cpu().numpy() - ref)) <= 1e-14
 
 
+def oracle_dsf(q):
+    """The oracle's run of a DSF request: the ground state from its seeded start
+    vector (gs_steps Lanczos steps, vec12, the eigenvector pass), then the
+    momentum chains with the variant runs that measure the oracle's own spread
+    (tests/chains.py); returns (E0, [(ref, [variants])] per momentum)."""
+    cl = cluster_for_sites(q.n)
+    cpl, fld = q.couplings()
+    X = O.xlocal(2, 0, cpl, field=fld)
+    skip, _, pt = O.parity_skip(2, 0, X)
+    om = O.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    v = O.gaussian(q.seed, om.ldim)
+    v /= np.linalg.norm(v)
+    run = om.lanczos(v, q.gs_steps)
+    E = O.bisec(run["alpha"], run["beta"], q.gs_steps, 1)
+    c = O.vec12(run["alpha"], run["beta"], E, q.gs_steps, 1)[0]
+    x = om.lanczos_vector(v, run["alpha"], run["beta"], c)
+    qrs = np.stack([cl.qr(k) for k in range(q.nq)])
+    return E[0], oracle_chain_variants(cl, cpl, x, qrs, q.steps, fld=fld)
+
+
 def test_serving_results_alone_and_in_the_mix():
     """Requests served in a mixed stream (lanes of N = 10, 12, 14, co-batched,
     joining while others run) give the same results as each request served
-    alone (bit for bit) and as the plain path (E0 and TPQ coefficients 1e-10;
-    DSF spectra 1e-6: both take the ground state from a 40-step Lanczos
-    eigenvector pass, through different H.V kernels; chains run on past
-    convergence amplify rounding, so the pass stops short of it)."""
+    alone (bit for bit) and as the plain path (E0 and TPQ coefficients 1e-10).
+    DSF: both take the ground state from a 40-step Lanczos eigenvector pass,
+    through different H.V kernels, so their chains are compared with the
+    oracle's run of the same request instead, each within 1e-10 or ten times
+    the oracle's own spread (coefficients over the prefix the oracle's variant
+    runs agree on, and S(q, w)), as the configuration tests do."""
     from pned_b200 import serve
     reqs = serve.make_stream(14, rate=1e6, seed=11, sizes=(10, 12, 14), p30=0.0, mix=(0.5, 0.3, 0.2),
                              lanczos_steps=60, tpq_steps=40, dsf_steps=20, dsf_gs_steps=40)
@@ -230,5 +254,9 @@ def test_serving_results_alone_and_in_the_mix():
             for k in range(q.nq):
                 assert np.array_equal(r["salpha"][k], a["salpha"][k])
             assert abs(r["e0"] - p["e0"]) <= 1e-10 * abs(p["e0"])
-            sr, sp = serve.dsf_spectra(r, 400), serve.dsf_spectra(p, 400)
-            assert rel(sr, sp) <= 1e-6
+            e0, chains = oracle_dsf(q)
+            assert abs(r["e0"] - e0) <= 1e-10 * abs(e0)
+            for k, (ref, others) in enumerate(chains):
+                for got in (r, p):
+                    check_chain(np.asarray(got["salpha"][k]), np.asarray(got["sbeta"][k]), ref, others, e0, q.steps,
+                                min_prefix=10)
