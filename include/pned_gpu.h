@@ -411,6 +411,25 @@ int pned_session_save(pned_ctx *c, const char *path);
 int pned_session_load(pned_ctx *c, const char *path, int max_steps);
 /* The context's session: kind (0 = none), steps enqueued, max_steps, TPS coefficients per step. */
 int pned_session_info(const pned_ctx *c, int *kind, int *steps_done, int *max_steps, int *n_coef);
+/*
+ * A Lanczos session (R = 1) in the reference's checkpoint terms: the state
+ * parallelized_lnc1z holds at the top of its next iteration (S1/2 Lanczos.f90:
+ * 97-122), where interval_dump writes it (vec1 = v0, vec2 = v1; pned_write_
+ * interval_dump).  After k >= 1 steps: w_out = v0 = H v_k - beta_{k-1} v_{k-1}
+ * (the last product, before its alpha is taken off), v_out = v1 = v_k (the
+ * normalised vector whose alpha is alpha[k-1]); dim states each, host or
+ * device memory per flags (PNED_PTR_DEVICE).  Waits for the session's steps.
+ */
+int pned_session_lanczos_state(pned_ctx *c, pned_c128 *w_out, pned_c128 *v_out, int flags);
+/*
+ * Starts a Lanczos session (R = 1) from that state, as interval_dump_read
+ * resumes parallelized_lnc1z (:87-93): k >= 1 steps done, alpha[0..k-1],
+ * beta[0..k-1] (beta[k-1] > 0), w = v0 and v = v1 above; room for max_steps
+ * steps in all.  The next step forms (v0 - alpha[k-1] v1) / beta[k-1] and
+ * continues the chain.
+ */
+int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                                  const double *beta, int k, int max_steps, int flags);
 
 /* ------------------------------------------------------------------------ */
 /* slot batches: continuous batching of chains with different couplings      */
@@ -548,6 +567,46 @@ int pned_append_sq(const char *path, int iq, double q1, double q2, double norm_r
  * records indx (int32), v1 [ll], v2 [ll]; long records in subrecords as pned_write_vec_data. */
 int pned_write_dsf_vectors(const char *path, int indx, const pned_c128 *v1, const pned_c128 *v2, int64_t ll);
 int pned_read_dsf_vectors(const char *path, int *indx, pned_c128 *v1, pned_c128 *v2, int64_t ll);
+/*
+ * The reference's checkpoint of a long run (interval_dump / interval_dump_read /
+ * check_interval_dump, S1/2 output.f90:50-211; files DUMP_NAME = vecdump_me%05d
+ * and DUMP_NAME.info).  The .info file holds one record each of DUMP_NAME
+ * (character(128), blank padded), lnp, progress(7) (logicals, 4 bytes, 1 =
+ * .true.), max_itr, dsf_comp (character(2)), s_maxitr, n, ibond, nvec,
+ * total_sz, then itr_counter(1..12) one record each.  The data file holds
+ * data_size, vec_size (int32 records), then the arrays the calling loop
+ * passes, in this order and only those present: sa, sb, sc (column-major),
+ * se (doubles), vec0, vec1, vec2, vec3, vec4 (data_size complex states each;
+ * vec1 and vec2 always).  Long records are split into subrecords as
+ * pned_write_vec_data does.  parallelized_lnc1z passes sa = alpha, sb = beta
+ * (itr_counter(2) each), sc = coef (itr_counter(2) x 9), se = ene (max_itr),
+ * vec1 = v0, vec2 = v1 (pned_session_lanczos_state).
+ */
+typedef struct {
+    char dump_name[128];       /* DUMP_NAME as stored: blank padded, no terminator needed */
+    int32_t np;                /* lnp, the run's MPI ranks */
+    int32_t position[7];       /* progress(1..7): 0 or 1 */
+    int32_t max_itr;
+    char dsf_comp[2];
+    int32_t s_maxitr, n, ibond, nvec, total_sz;
+    int32_t itr_counter[12];
+} pned_dump_info;
+typedef struct {
+    int32_t data_size;         /* states of each vector */
+    int32_t vec_size;          /* length of the iteration arrays (itr_counter(2) or (12)) */
+    double *sa, *sb, *sc, *se; /* null: not in the file */
+    int64_t n_sa, n_sb, n_sc, n_se;
+    pned_c128 *vec[5];         /* vec0 .. vec4; null: not in the file (vec1, vec2 required) */
+} pned_dump_data;
+/* Writes `path` and `path`.info. */
+int pned_write_interval_dump(const char *path, const pned_dump_info *info, const pned_dump_data *d);
+/* Reads `path`.info. */
+int pned_read_interval_dump_info(const char *path, pned_dump_info *info);
+/* Byte lengths of the data file's records (*count of them; the first `cap` into bytes). */
+int pned_interval_dump_records(const char *path, int64_t *bytes, int cap, int *count);
+/* Reads the data file into the arrays present in d (their lengths must match the
+ * records; vectors data_size states); sets d->data_size and d->vec_size. */
+int pned_read_interval_dump(const char *path, pned_dump_data *d);
 /*
  * Largest payload of one subrecord for the writers above (no counterpart in the
  * reference; gfortran's -fmax-subrecord-length): 1 .. 2147483639 bytes, default

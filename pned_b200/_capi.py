@@ -30,6 +30,22 @@ class ModelDesc(C.Structure):
     ]
 
 
+class DumpInfo(C.Structure):
+    """pned_dump_info: the .info file of interval_dump."""
+    _fields_ = [("dump_name", C.c_char * 128), ("np", C.c_int32), ("position", C.c_int32 * 7),
+                ("max_itr", C.c_int32), ("dsf_comp", C.c_char * 2), ("s_maxitr", C.c_int32), ("n", C.c_int32),
+                ("ibond", C.c_int32), ("nvec", C.c_int32), ("total_sz", C.c_int32),
+                ("itr_counter", C.c_int32 * 12)]
+
+
+class DumpData(C.Structure):
+    """pned_dump_data: the arrays of interval_dump's data file (null pointers: absent)."""
+    _fields_ = [("data_size", C.c_int32), ("vec_size", C.c_int32),
+                ("sa", C.POINTER(C.c_double)), ("sb", C.POINTER(C.c_double)), ("sc", C.POINTER(C.c_double)),
+                ("se", C.POINTER(C.c_double)), ("n_sa", C.c_int64), ("n_sb", C.c_int64), ("n_sc", C.c_int64),
+                ("n_se", C.c_int64), ("vec", C.c_void_p * 5)]
+
+
 class TilePlan(C.Structure):
     _fields_ = [("row_fixed_bits", C.c_int32), ("window_bits", C.c_int32), ("max_passes", C.c_int32),
                 ("j_bits", C.c_int32), ("l1_carveout", C.c_int32), ("stage_partner_tiles", C.c_int32),
@@ -67,6 +83,8 @@ EXPORTS = [
     "pned_session_load", "pned_session_info", "pned_write_vec_data", "pned_read_vec_data",
     "pned_write_dsf_alpha_beta", "pned_read_dsf_alpha_beta", "pned_append_dsf_res", "pned_append_sq",
     "pned_write_dsf_vectors", "pned_read_dsf_vectors", "pned_set_max_subrecord",
+    "pned_session_lanczos_state", "pned_session_begin_lanczos_at", "pned_write_interval_dump",
+    "pned_read_interval_dump_info", "pned_interval_dump_records", "pned_read_interval_dump",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -155,6 +173,12 @@ def lib() -> C.CDLL:
     L.pned_append_sq.argtypes = [C.c_char_p, i32, dbl, dbl, dbl]
     L.pned_write_dsf_vectors.argtypes = [C.c_char_p, i32, vp, vp, i64]
     L.pned_read_dsf_vectors.argtypes = [C.c_char_p, ip, vp, vp, i64]
+    L.pned_session_lanczos_state.argtypes = [vp, vp, vp, i32]
+    L.pned_session_begin_lanczos_at.argtypes = [vp, vp, vp, dp, dp, i32, i32, i32]
+    L.pned_write_interval_dump.argtypes = [C.c_char_p, C.POINTER(DumpInfo), C.POINTER(DumpData)]
+    L.pned_read_interval_dump_info.argtypes = [C.c_char_p, C.POINTER(DumpInfo)]
+    L.pned_interval_dump_records.argtypes = [C.c_char_p, C.POINTER(i64), i32, ip]
+    L.pned_read_interval_dump.argtypes = [C.c_char_p, C.POINTER(DumpData)]
     L.pned_set_max_subrecord.argtypes = [i64]
     _lib = L
     return L

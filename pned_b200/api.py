@@ -238,6 +238,106 @@ def read_dsf_vectors(path: str, ll: int):
     return i.value, a, b
 
 
+# --------------------------------------------------------------------------- interval_dump checkpoints
+
+REF_MAX_ITR = 1024     # max_itr of the reference (S_one_half/Hybrid_TPS_params.f90:39)
+REF_S_MAXITR = 4096    # s_maxitr (:42)
+REF_NVEC = 8           # nvec (:31)
+DUMP_ARRAYS = ("sa", "sb", "sc", "se", "vec0", "vec1", "vec2", "vec3", "vec4")
+# what each loop of the reference passes to interval_dump (S1/2 Lanczos.f90:101, 275; TPS.f90:370; DSF.f90:236)
+DUMP_LAYOUTS = {"lnc1z": ("sa", "sb", "sc", "se", "vec1", "vec2"),
+                "lncv1z": ("sa", "sb", "sc", "se", "vec0", "vec1", "vec2"),
+                "tpsz": ("sa", "sb", "sc", "se", "vec1", "vec2", "vec3"),
+                "dsflnc": ("sa", "sb", "vec1", "vec2")}
+
+
+def dump_info(n_sites: int, n_bonds: int, itr_counter, dump_name: str = "vecdump_me00000",
+              position=(1, 0, 1, 0, 0, 0, 0), dsf_comp: str = "ee", np_ranks: int = 1, max_itr: int = REF_MAX_ITR,
+              s_maxitr: int = REF_S_MAXITR, nvec: int = REF_NVEC, total_sz=None) -> "_capi.DumpInfo":
+    """The .info record set of interval_dump (S1/2 output.f90:176-191); total_sz
+    defaults to n/2 as the reference sets it (params.f90:149)."""
+    info = _capi.DumpInfo()
+    info.dump_name = dump_name.encode().ljust(128, b" ")[:128]
+    info.np = int(np_ranks)
+    for i, p in enumerate(position):
+        info.position[i] = 1 if p else 0
+    info.max_itr = int(max_itr)
+    info.dsf_comp = dsf_comp.encode()[:2].ljust(2, b" ")
+    info.s_maxitr, info.n, info.ibond, info.nvec = int(s_maxitr), int(n_sites), int(n_bonds), int(nvec)
+    info.total_sz = int(n_sites // 2 if total_sz is None else total_sz)
+    for i, k in enumerate(itr_counter):
+        info.itr_counter[i] = int(k)
+    return info
+
+
+def info_dict(info: "_capi.DumpInfo") -> dict:
+    return {"dump_name": bytes(info.dump_name).decode(errors="replace").rstrip(" \x00"), "np": info.np,
+            "position": tuple(bool(x) for x in info.position), "max_itr": info.max_itr,
+            "dsf_comp": bytes(info.dsf_comp).decode(errors="replace"), "s_maxitr": info.s_maxitr, "n": info.n,
+            "ibond": info.ibond, "nvec": info.nvec, "total_sz": info.total_sz,
+            "itr_counter": tuple(info.itr_counter)}
+
+
+def write_interval_dump(path: str, info: "_capi.DumpInfo", vec_size: int, **arrays):
+    """interval_dump's files `path` and `path`.info: arrays by name (DUMP_ARRAYS;
+    sa .. se real, sc column-major as given in Fortran order; vec0 .. vec4
+    complex, vec1 and vec2 required, all of one length)."""
+    d = _capi.DumpData()
+    keep = []
+    vl = None
+    for name in DUMP_ARRAYS:
+        x = arrays.get(name)
+        if x is None:
+            continue
+        if name.startswith("vec"):
+            a = np.ascontiguousarray(x, dtype=np.complex128)
+            if vl is not None and a.size != vl:
+                raise ValueError("the dump's vectors need one length")
+            vl = a.size
+            d.vec[int(name[3])] = a.ctypes.data
+        else:
+            a = np.asfortranarray(x, dtype=np.float64).reshape(-1, order="F")
+            setattr(d, name, _dp(a))
+            setattr(d, "n_" + name, a.size)
+        keep.append(a)
+    if arrays.get("vec1") is None or arrays.get("vec2") is None:
+        raise ValueError("interval_dump always writes vec1 and vec2")
+    d.data_size, d.vec_size = int(vl), int(vec_size)
+    check(lib().pned_write_interval_dump(os.fsencode(path), C.byref(info), C.byref(d)))
+
+
+def read_interval_dump_info(path: str) -> dict:
+    info = _capi.DumpInfo()
+    check(lib().pned_read_interval_dump_info(os.fsencode(path), C.byref(info)))
+    return info_dict(info)
+
+
+def read_interval_dump(path: str, layout) -> dict:
+    """interval_dump's data file read with the arrays `layout` names (in file order,
+    e.g. DUMP_LAYOUTS['lnc1z']), sized from the records themselves."""
+    names = DUMP_LAYOUTS[layout] if isinstance(layout, str) else tuple(layout)
+    cap = 16
+    lens = (C.c_int64 * cap)()
+    cnt = C.c_int(0)
+    check(lib().pned_interval_dump_records(os.fsencode(path), lens, cap, C.byref(cnt)))
+    if cnt.value != 2 + len(names):
+        raise ValueError(f"{path}: {cnt.value} records, the layout {names} needs {2 + len(names)}")
+    d = _capi.DumpData()
+    out = {}
+    for name, nb in zip(names, list(lens)[2:cnt.value]):
+        if name.startswith("vec"):
+            a = np.zeros(nb // 16, dtype=np.complex128)
+            d.vec[int(name[3])] = a.ctypes.data
+        else:
+            a = np.zeros(nb // 8)
+            setattr(d, name, _dp(a))
+            setattr(d, "n_" + name, a.size)
+        out[name] = a
+    check(lib().pned_read_interval_dump(os.fsencode(path), C.byref(d)))
+    out["data_size"], out["vec_size"] = d.data_size, d.vec_size
+    return out
+
+
 # --------------------------------------------------------------------------- model / context
 
 
@@ -673,6 +773,57 @@ class Context:
     def session_end(self):
         check(lib().pned_session_end(self._h))
         self._sess = None
+
+    def lanczos_state(self):
+        """The running Lanczos session (R = 1) as the reference's loop holds it at the
+        top of its next iteration: (v0, v1) = (H v_k - beta v_{k-1}, v_k) on the host."""
+        w = np.zeros(self.model.dim, dtype=np.complex128)
+        v = np.zeros(self.model.dim, dtype=np.complex128)
+        check(lib().pned_session_lanczos_state(self._h, C.c_void_p(w.ctypes.data), C.c_void_p(v.ctypes.data),
+                                               PTR_HOST))
+        return w, v
+
+    def lanczos_dump_reference(self, path: str, vec_size: int = REF_MAX_ITR, ene_size: int = REF_MAX_ITR, **info_kw):
+        """Writes the running Lanczos session (R = 1) as parallelized_lnc1z's
+        interval_dump does (S1/2 Lanczos.f90:99-103; files `path`, `path`.info):
+        alpha, beta (vec_size each, zero past the steps done), coef (vec_size x
+        9, zero: lnc1z keeps none), ene (the 8 lowest Ritz values so far, then
+        zeros), vec1 = v0, vec2 = v1, and itr_counter(1) = steps done + 1."""
+        r = self.session_read()
+        k = r["steps"]
+        if k < 1 or k > vec_size:
+            raise ValueError("the session needs 1..vec_size steps done")
+        a = np.zeros(vec_size)
+        b = np.zeros(vec_size)
+        a[:k], b[:k] = r["alpha"][:, 0], r["beta"][:, 0]
+        ene = np.zeros(ene_size)
+        ne = min(k, REF_NVEC)
+        ene[:ne] = bisec(a[:k], b[:k], k, ne)
+        w, v = self.lanczos_state()
+        m = self.model
+        itr = (k + 1, vec_size, 2, vec_size, 1, 5000, 1, 500, 1, REF_NVEC, 2, REF_S_MAXITR)
+        info = dump_info(m.n, m.n_bonds, itr, **info_kw)
+        write_interval_dump(path, info, vec_size, sa=a, sb=b, sc=np.zeros((vec_size, REF_NVEC + 1), order="F"),
+                            se=ene, vec1=w, vec2=v)
+
+    def lanczos_resume_reference(self, path: str, max_steps: int):
+        """Starts a Lanczos session (R = 1) from parallelized_lnc1z's interval_dump
+        files, as interval_dump_read resumes the loop (S1/2 Lanczos.f90:87-93):
+        itr_counter(1) - 1 steps done; returns that count."""
+        info = read_interval_dump_info(path)
+        k = info["itr_counter"][0] - 1
+        if info["n"] != self.model.n:
+            raise ValueError(f"{path}: dump of {info['n']} sites, the model has {self.model.n}")
+        d = read_interval_dump(path, "lnc1z")
+        if d["data_size"] != self.model.dim or k < 1 or k > d["sa"].size:
+            raise ValueError(f"{path}: not a Lanczos dump of this basis")
+        a = np.ascontiguousarray(d["sa"][:k])
+        b = np.ascontiguousarray(d["sb"][:k])
+        check(lib().pned_session_begin_lanczos_at(self._h, C.c_void_p(d["vec1"].ctypes.data),
+                                                  C.c_void_p(d["vec2"].ctypes.data), _dp(a), _dp(b), int(k),
+                                                  int(max_steps), PTR_HOST))
+        self._sess = dict(kind="lanczos", nobs=0, max_steps=int(max_steps))
+        return k
 
 
 # --------------------------------------------------------------------------- slot batches

@@ -337,3 +337,96 @@ extern "C" int pned_read_dsf_vectors(const char *path, int *indx, pned_c128 *v1,
     *indx = i4;
     return PNED_OK;
 }
+
+// ---------------------------------------------------------------------------
+// interval_dump / interval_dump_read / check_interval_dump (S1/2 output.f90:50-211)
+// ---------------------------------------------------------------------------
+extern "C" int pned_write_interval_dump(const char *path, const pned_dump_info *info, const pned_dump_data *d)
+{
+    if (!path || !info || !d || !d->vec[1] || !d->vec[2] || d->data_size < 1 || d->vec_size < 0)
+        return fail(PNED_EINVAL, "pned_write_interval_dump: bad arguments");
+    const std::string ipath = std::string(path) + ".info";
+    FILE *f = std::fopen(ipath.c_str(), "wb");
+    if (!f) return fail(PNED_EINVAL, "pned_write_interval_dump: cannot open " + ipath);
+    bool ok = put_record(f, info->dump_name, 128) && put_record(f, &info->np, 4) &&
+              put_record(f, info->position, 28) && put_record(f, &info->max_itr, 4) &&
+              put_record(f, info->dsf_comp, 2) && put_record(f, &info->s_maxitr, 4) && put_record(f, &info->n, 4) &&
+              put_record(f, &info->ibond, 4) && put_record(f, &info->nvec, 4) && put_record(f, &info->total_sz, 4);
+    for (int i = 0; i < 12 && ok; ++i) ok = put_record(f, &info->itr_counter[i], 4);
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(PNED_EINVAL, "pned_write_interval_dump: write failed");
+    f = std::fopen(path, "wb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_write_interval_dump: cannot open ") + path);
+    ok = put_record(f, &d->data_size, 4) && put_record(f, &d->vec_size, 4);
+    const double *arr[4] = {d->sa, d->sb, d->sc, d->se};
+    const int64_t len[4] = {d->n_sa, d->n_sb, d->n_sc, d->n_se};
+    for (int i = 0; i < 4 && ok; ++i)
+        if (arr[i]) ok = len[i] >= 0 && put_record(f, arr[i], size_t(len[i]) * 8);
+    const size_t vb = size_t(d->data_size) * 16;
+    for (int i = 0; i < 5 && ok; ++i)
+        if (d->vec[i]) ok = put_record(f, d->vec[i], vb);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? PNED_OK : fail(PNED_EINVAL, "pned_write_interval_dump: write failed");
+}
+
+extern "C" int pned_read_interval_dump_info(const char *path, pned_dump_info *info)
+{
+    if (!path || !info) return fail(PNED_EINVAL, "pned_read_interval_dump_info: bad arguments");
+    const std::string ipath = std::string(path) + ".info";
+    FILE *f = std::fopen(ipath.c_str(), "rb");
+    if (!f) return fail(PNED_EINVAL, "pned_read_interval_dump_info: cannot open " + ipath);
+    pned_dump_info t{};
+    bool ok = get_record_exact(f, t.dump_name, 128) && get_record_exact(f, &t.np, 4) &&
+              get_record_exact(f, t.position, 28) && get_record_exact(f, &t.max_itr, 4) &&
+              get_record_exact(f, t.dsf_comp, 2) && get_record_exact(f, &t.s_maxitr, 4) &&
+              get_record_exact(f, &t.n, 4) && get_record_exact(f, &t.ibond, 4) && get_record_exact(f, &t.nvec, 4) &&
+              get_record_exact(f, &t.total_sz, 4);
+    for (int i = 0; i < 12 && ok; ++i) ok = get_record_exact(f, &t.itr_counter[i], 4);
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_read_interval_dump_info: not an interval_dump .info file");
+    *info = t;
+    return PNED_OK;
+}
+
+extern "C" int pned_interval_dump_records(const char *path, int64_t *bytes, int cap, int *count)
+{
+    if (!path || !count || cap < 0 || (cap && !bytes)) return fail(PNED_EINVAL, "pned_interval_dump_records: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_interval_dump_records: cannot open ") + path);
+    int n = 0;
+    bool ok = true;
+    for (;;) {
+        const int c = std::fgetc(f);
+        if (c == EOF) break;
+        std::ungetc(c, f);
+        size_t len = 0;
+        if (!read_record(f, nullptr, 0, &len)) { ok = false; break; }
+        if (n < cap) bytes[n] = int64_t(len);
+        ++n;
+    }
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_interval_dump_records: malformed record");
+    *count = n;
+    return PNED_OK;
+}
+
+extern "C" int pned_read_interval_dump(const char *path, pned_dump_data *d)
+{
+    if (!path || !d || !d->vec[1] || !d->vec[2]) return fail(PNED_EINVAL, "pned_read_interval_dump: bad arguments");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(PNED_EINVAL, std::string("pned_read_interval_dump: cannot open ") + path);
+    int32_t ds = 0, vs = 0;
+    bool ok = get_record_exact(f, &ds, 4) && get_record_exact(f, &vs, 4) && ds >= 1 &&
+              (d->data_size <= 0 || ds == d->data_size);
+    double *arr[4] = {d->sa, d->sb, d->sc, d->se};
+    const int64_t len[4] = {d->n_sa, d->n_sb, d->n_sc, d->n_se};
+    for (int i = 0; i < 4 && ok; ++i)
+        if (arr[i]) ok = len[i] >= 0 && get_record_exact(f, arr[i], size_t(len[i]) * 8);
+    for (int i = 0; i < 5 && ok; ++i)
+        if (d->vec[i]) ok = get_record_exact(f, d->vec[i], size_t(ds) * 16);
+    std::fclose(f);
+    if (!ok) return fail(PNED_EINVAL, "pned_read_interval_dump: records do not match the expected arrays");
+    d->data_size = ds;
+    d->vec_size = vs;
+    return PNED_OK;
+}

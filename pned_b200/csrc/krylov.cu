@@ -254,6 +254,16 @@ __global__ void __launch_bounds__(kThreads) lncv_kernel(const double2 *__restric
     }
 }
 
+// Resuming a Lanczos chain from the reference's loop state: Rn = W - a V.
+__global__ void __launch_bounds__(kThreads) resume_kernel(const double2 *__restrict__ W, const double2 *__restrict__ V,
+                                                          double2 *Rn, double a, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 w = W[i], v = V[i];
+        Rn[i] = make_double2(w.x - a * v.x, w.y - a * v.y);
+    }
+}
+
 // sc <- 1/b, pc <- -b sc_old
 __global__ void lncv_scal_kernel(double *sc, double *pc, double b)
 {
@@ -1067,6 +1077,85 @@ extern "C" int pned_session_load(pned_ctx *c, const char *path, int max_steps)
     if (!ok || e != cudaSuccess) {
         session_release(c);
         return e != cudaSuccess ? cuda_fail(e, "pned_session_load") : fail(PNED_EINVAL, "pned_session_load: short file");
+    }
+    S.enqueued = k;
+    return PNED_OK;
+}
+
+extern "C" int pned_session_lanczos_state(pned_ctx *c, pned_c128 *w_out, pned_c128 *v_out, int flags)
+{
+    if (!c || !w_out || !v_out) return fail(PNED_EINVAL, "pned_session_lanczos_state: bad arguments");
+    Session &S = c->sess;
+    if (S.kind != PNED_SESSION_LANCZOS || c->R != 1 || S.enqueued < 1)
+        return fail(PNED_EINVAL, "pned_session_lanczos_state: needs a Lanczos session (R = 1) with steps done");
+    cudaSetDevice(c->m->device);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_lanczos_state");
+    // after step k: b0 = W_k - alpha_k v_k (the next vector times beta_k), b1 = v_k / sc_old,
+    // b2 = W_k; sc = 1 / beta_k, pc = -beta_k sc_old
+    const int k = S.enqueued;
+    double sc = 0.0, pc = 0.0, be = 0.0;
+    e = cudaMemcpy(&sc, slot(c, kSlotSc), sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&pc, slot(c, kSlotPc), sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&be, S.d_beta + (k - 1), sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_lanczos_state: scalars");
+    if (!(be > 0.0)) return fail(PNED_EBREAKDOWN, "pned_session_lanczos_state: beta of the last step is zero");
+    const double sc_old = -pc / be;
+    const int64_t n = c->m->dim;
+    const size_t bytes = sizeof(double2) * size_t(n);
+    const bool dev = (flags & PNED_PTR_DEVICE) != 0;
+    const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    e = cudaMemcpyAsync(w_out, c->buf[S.b2], bytes, kind, c->stream);
+    if (e == cudaSuccess && dev) {
+        e = cudaMemcpyAsync(v_out, c->buf[S.b1], bytes, kind, c->stream);
+        if (e == cudaSuccess) {
+            scale_real_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(reinterpret_cast<double2 *>(v_out), sc_old, n);
+            e = cudaGetLastError();
+        }
+    } else if (e == cudaSuccess) {
+        // copied out, then scaled on the host (no device memory beyond the session's)
+        e = cudaMemcpyAsync(v_out, c->buf[S.b1], bytes, kind, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_lanczos_state");
+    if (!dev) {
+        double *p = reinterpret_cast<double *>(v_out);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < 2 * n; ++i) p[i] *= sc_old;
+    }
+    return PNED_OK;
+}
+
+extern "C" int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                                             const double *beta, int k, int max_steps, int flags)
+{
+    if (!c || !w || !v || !alpha || !beta || k < 1 || max_steps < k)
+        return fail(PNED_EINVAL, "pned_session_begin_lanczos_at: bad arguments");
+    if (c->R != 1) return fail(PNED_EINVAL, "pned_session_begin_lanczos_at: needs a context with R = 1");
+    if (!(beta[k - 1] > 0.0)) return fail(PNED_EINVAL, "pned_session_begin_lanczos_at: beta[k-1] must be positive");
+    cudaSetDevice(c->m->device);
+    int rc = session_common_begin(c, PNED_SESSION_LANCZOS, max_steps);
+    if (rc) return rc;
+    Session &S = c->sess;
+    const int64_t n = c->m->dim;
+    const size_t bytes = sizeof(double2) * size_t(n);
+    const cudaMemcpyKind kind = (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    // b2 = W, b1 = v (the previous vector, scale 1), b0 = W - alpha v (the next vector times beta)
+    cudaError_t e = cudaMemcpyAsync(c->buf[S.b2], w, bytes, kind, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->buf[S.b1], v, bytes, kind, c->stream);
+    if (e == cudaSuccess) {
+        resume_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(c->buf[S.b2], c->buf[S.b1], c->buf[S.b0], alpha[k - 1], n);
+        e = cudaGetLastError();
+    }
+    const int32_t counters[2] = {k, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_alpha, alpha, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_beta, beta, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_counter, counters, sizeof(counters), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);   // host sources may go away after the call
+    if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "pned_session_begin_lanczos_at"); }
+    if ((rc = set_slot(c, kSlotSc, 1.0 / beta[k - 1])) || (rc = set_slot(c, kSlotPc, -beta[k - 1]))) {
+        session_release(c);
+        return rc;
     }
     S.enqueued = k;
     return PNED_OK;
