@@ -430,6 +430,19 @@ int pned_session_lanczos_state(pned_ctx *c, pned_c128 *w_out, pned_c128 *v_out, 
  */
 int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
                                   const double *beta, int k, int max_steps, int flags);
+/*
+ * The same for a TPS session (R = 1, model built for L - H), in the terms of
+ * parallelized_TPSz (S1/2 TPS.f90:366-395), whose interval_dump passes vec1 =
+ * v0, vec2 = v1, vec3 = vg: after k >= 1 steps w_out = v0 = (L - H) v_k (not
+ * normalised), v_out = v1 = v_k, g_out = vg = v_{k-1} (zero after one step).
+ * begin_tps_at resumes from w and v (vg is overwritten by the loop's first
+ * assignment), alpha/beta and the first five coefficient columns per step
+ * (coef [k][5]: 2i/alpha1, L, beta, L - alpha1, <k-1|H|k>; a session without
+ * observables).
+ */
+int pned_session_tps_state(pned_ctx *c, pned_c128 *w_out, pned_c128 *v_out, pned_c128 *g_out, int flags);
+int pned_session_begin_tps_at(pned_ctx *c, double L, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                              const double *beta, const double *coef, int k, int max_steps, int flags);
 
 /* ------------------------------------------------------------------------ */
 /* slot batches: continuous batching of chains with different couplings      */

@@ -806,6 +806,60 @@ class Context:
         write_interval_dump(path, info, vec_size, sa=a, sb=b, sc=np.zeros((vec_size, REF_NVEC + 1), order="F"),
                             se=ene, vec1=w, vec2=v)
 
+    def tps_dump_reference(self, path: str, vec_size: int | None = None, ene_size: int = REF_MAX_ITR, **info_kw):
+        """Writes the running TPS session (R = 1) as parallelized_TPSz's interval_dump
+        does (S1/2 TPS.f90:368-372): alpha, beta (vec_size each), coef (vec_size x
+        the session's coefficients per step, column-major: the reference's first
+        five columns, then two per observable), ene (zeros: TPS keeps none), vec1
+        = v0, vec2 = v1, vec3 = vg, and itr_counter(1) = steps done + 1."""
+        r = self.session_read()
+        k = r["steps"]
+        vec_size = int(vec_size or self._sess["max_steps"])
+        if k < 1 or k > vec_size:
+            raise ValueError("the session needs 1..vec_size steps done")
+        a = np.zeros(vec_size)
+        b = np.zeros(vec_size)
+        a[:k], b[:k] = r["alpha"][:, 0], r["beta"][:, 0]
+        nc = r["coef"].shape[-1]
+        coef = np.zeros((vec_size, nc), order="F")
+        coef[:k] = r["coef"][:, 0, :]
+        w = np.zeros(self.model.dim, dtype=np.complex128)
+        v = np.zeros_like(w)
+        g = np.zeros_like(w)
+        check(lib().pned_session_tps_state(self._h, C.c_void_p(w.ctypes.data), C.c_void_p(v.ctypes.data),
+                                           C.c_void_p(g.ctypes.data), PTR_HOST))
+        m = self.model
+        itr = (k + 1, vec_size, 2, vec_size, 1, 5000, 1, 500, 1, REF_NVEC, 2, REF_S_MAXITR)
+        info_kw = {"position": (0, 0, 0, 0, 0, 0, 1), "dsf_comp": "tp", **info_kw}
+        info = dump_info(m.n, m.n_bonds, itr, **info_kw)
+        write_interval_dump(path, info, vec_size, sa=a, sb=b, sc=coef, se=np.zeros(ene_size), vec1=w, vec2=v, vec3=g)
+
+    def tps_resume_reference(self, path: str, max_steps: int):
+        """Starts a TPS session (R = 1, this context's model built for L - H) from
+        parallelized_TPSz's interval_dump files (S1/2 TPS.f90:359-363), carrying
+        alpha, beta and the first five coefficient columns (observable columns are
+        not resumed); L is the dump's coef(1, 2).  Returns the steps done."""
+        info = read_interval_dump_info(path)
+        k = info["itr_counter"][0] - 1
+        if info["n"] != self.model.n:
+            raise ValueError(f"{path}: dump of {info['n']} sites, the model has {self.model.n}")
+        d = read_interval_dump(path, "tpsz")
+        vs = d["sa"].size
+        if d["data_size"] != self.model.dim or k < 1 or k > vs or d["sc"].size % vs:
+            raise ValueError(f"{path}: not a TPS dump of this basis")
+        coef = d["sc"].reshape(vs, -1, order="F")
+        if coef.shape[1] < 5:
+            raise ValueError(f"{path}: fewer than five coefficient columns")
+        L = float(coef[0, 1])
+        a = np.ascontiguousarray(d["sa"][:k])
+        b = np.ascontiguousarray(d["sb"][:k])
+        cf = np.ascontiguousarray(coef[:k, :5])
+        check(lib().pned_session_begin_tps_at(self._h, L, C.c_void_p(d["vec1"].ctypes.data),
+                                              C.c_void_p(d["vec2"].ctypes.data), _dp(a), _dp(b), _dp(cf), int(k),
+                                              int(max_steps), PTR_HOST))
+        self._sess = dict(kind="tps", nobs=0, max_steps=int(max_steps))
+        return k
+
     def lanczos_resume_reference(self, path: str, max_steps: int):
         """Starts a Lanczos session (R = 1) from parallelized_lnc1z's interval_dump
         files, as interval_dump_read resumes the loop (S1/2 Lanczos.f90:87-93):

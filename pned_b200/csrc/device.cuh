@@ -70,7 +70,7 @@ enum : int {
     kSlotSc,        // scale of the current vector C
     kSlotPc,        // coefficient of the previous vector P in W
     kSlotGsc,       // scale of the vector G (TPS: previous vector)
-    kSlotTmp,
+    kSlotGscPrev,   // TPS: the scale G had before the last step (the W buffer holds that vector then)
     kScalSlots
 };
 

@@ -44,8 +44,8 @@ __global__ void lanczos_epilogue(const double2 *__restrict__ sa, const double2 *
 
 // TPS: alpha1 = Re<v|(L-H)v>, beta = ||(L-H)v||, coef as eval_phys_val.
 __global__ void tps_epilogue(const double2 *__restrict__ s, int R, int nobs, const double2 *__restrict__ so, double L,
-                             double *sc, double *gsc, double *d_alpha, double *d_beta, double *d_coef, int ncoef,
-                             int *counter)
+                             double *sc, double *gsc, double *gscp, double *d_alpha, double *d_beta, double *d_coef,
+                             int ncoef, int *counter)
 {
     __shared__ int k;
     if (threadIdx.x == 0) k = *counter;
@@ -67,6 +67,7 @@ __global__ void tps_epilogue(const double2 *__restrict__ s, int R, int nobs, con
             cf[5 + 2 * o] = so[(2 * o) * R + r].x;
             cf[6 + 2 * o] = so[(2 * o + 1) * R + r].x;
         }
+        gscp[r] = gsc[r];
         gsc[r] = sc[r];
         sc[r] = 1.0 / be;
     }
@@ -349,8 +350,8 @@ static cudaError_t tps_step(pned_ctx *c, Session &S, bool first)
     }
     if (e == cudaSuccess) {
         tps_epilogue<<<1, 32 * ((R + 31) / 32), 0, c->stream>>>(c->sums, R, S.nobs, S.d_osum, S.L, slot(c, kSlotSc),
-                                                               slot(c, kSlotGsc), S.d_alpha, S.d_beta, S.d_coef,
-                                                               S.ncoef, S.d_counter);
+                                                               slot(c, kSlotGsc), slot(c, kSlotGscPrev), S.d_alpha,
+                                                               S.d_beta, S.d_coef, S.ncoef, S.d_counter);
         e = cudaGetLastError();
     }
     const int og = S.b2;
@@ -1154,6 +1155,95 @@ extern "C" int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, co
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);   // host sources may go away after the call
     if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "pned_session_begin_lanczos_at"); }
     if ((rc = set_slot(c, kSlotSc, 1.0 / beta[k - 1])) || (rc = set_slot(c, kSlotPc, -beta[k - 1]))) {
+        session_release(c);
+        return rc;
+    }
+    S.enqueued = k;
+    return PNED_OK;
+}
+
+// Copies `src` (scaled by f) into a caller's host or device vector of n states.
+static cudaError_t scaled_out(pned_ctx *c, const double2 *src, double f, pned_c128 *out, bool dev, int64_t n)
+{
+    const size_t bytes = sizeof(double2) * size_t(n);
+    cudaError_t e = cudaMemcpyAsync(out, src, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && dev && f != 1.0) {
+        scale_real_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(reinterpret_cast<double2 *>(out), f, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess && !dev && f != 1.0) {
+        double *p = reinterpret_cast<double *>(out);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < 2 * n; ++i) p[i] *= f;
+    }
+    return e;
+}
+
+extern "C" int pned_session_tps_state(pned_ctx *c, pned_c128 *w_out, pned_c128 *v_out, pned_c128 *g_out, int flags)
+{
+    if (!c || !w_out || !v_out || !g_out) return fail(PNED_EINVAL, "pned_session_tps_state: bad arguments");
+    Session &S = c->sess;
+    if (S.kind != PNED_SESSION_TPS || c->R != 1 || S.enqueued < 1)
+        return fail(PNED_EINVAL, "pned_session_tps_state: needs a TPS session (R = 1) with steps done");
+    cudaSetDevice(c->m->device);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_tps_state");
+    // after step k: b0 = (L - H) v_k, b2 = v_k / gsc, b1 = v_{k-1} / gsc_prev (the next step's W)
+    double gsc = 0.0, gscp = 0.0;
+    e = cudaMemcpy(&gsc, slot(c, kSlotGsc), sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&gscp, slot(c, kSlotGscPrev), sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "pned_session_tps_state: scalars");
+    const bool dev = (flags & PNED_PTR_DEVICE) != 0;
+    const int64_t n = c->m->dim;
+    e = scaled_out(c, c->buf[S.b0], 1.0, w_out, dev, n);
+    if (e == cudaSuccess) e = scaled_out(c, c->buf[S.b2], gsc, v_out, dev, n);
+    if (e == cudaSuccess) {
+        if (S.enqueued >= 2) {
+            e = scaled_out(c, c->buf[S.b1], gscp, g_out, dev, n);
+        } else {   // no vector before the first
+            e = dev ? cudaMemsetAsync(g_out, 0, sizeof(double2) * size_t(n), c->stream) : cudaSuccess;
+            if (!dev) std::memset(static_cast<void *>(g_out), 0, sizeof(double2) * size_t(n));
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        }
+    }
+    return e == cudaSuccess ? PNED_OK : cuda_fail(e, "pned_session_tps_state");
+}
+
+extern "C" int pned_session_begin_tps_at(pned_ctx *c, double L, const pned_c128 *w, const pned_c128 *v,
+                                         const double *alpha, const double *beta, const double *coef, int k,
+                                         int max_steps, int flags)
+{
+    if (!c || !w || !v || !alpha || !beta || !coef || k < 1 || max_steps < k)
+        return fail(PNED_EINVAL, "pned_session_begin_tps_at: bad arguments");
+    if (c->R != 1) return fail(PNED_EINVAL, "pned_session_begin_tps_at: needs a context with R = 1");
+    if (!(beta[k - 1] > 0.0)) return fail(PNED_EINVAL, "pned_session_begin_tps_at: beta[k-1] must be positive");
+    cudaSetDevice(c->m->device);
+    int rc = session_common_begin(c, PNED_SESSION_TPS, max_steps);
+    if (rc) return rc;
+    Session &S = c->sess;
+    S.L = L;
+    S.nobs = 0;
+    S.ncoef = 5;
+    S.d_coef = sess_alloc<double>(S, size_t(max_steps) * S.ncoef);
+    S.d_osum = sess_alloc<double2>(S, 2);
+    if (!S.d_coef || !S.d_osum) { session_release(c); return fail(PNED_ENOMEM, "session scratch"); }
+    const int64_t n = c->m->dim;
+    const size_t bytes = sizeof(double2) * size_t(n);
+    const cudaMemcpyKind kind = (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    // b0 = C = (L - H) v_k with scale 1/beta_k, b2 = G = v_k with scale 1 (the step rotates them)
+    cudaError_t e = cudaMemcpyAsync(c->buf[S.b0], w, bytes, kind, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->buf[S.b2], v, bytes, kind, c->stream);
+    const int32_t counters[2] = {k, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_alpha, alpha, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_beta, beta, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(S.d_coef, coef, sizeof(double) * size_t(k) * S.ncoef, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_counter, counters, sizeof(counters), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { session_release(c); return cuda_fail(e, "pned_session_begin_tps_at"); }
+    if ((rc = set_slot(c, kSlotSc, 1.0 / beta[k - 1])) || (rc = set_slot(c, kSlotGsc, 1.0)) ||
+        (rc = set_slot(c, kSlotGscPrev, 1.0))) {
         session_release(c);
         return rc;
     }

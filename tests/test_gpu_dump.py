@@ -111,3 +111,51 @@ def test_gpu_dump_resumes_on_the_oracle(tmp_path):
     assert rel(got_a, al) <= 1e-10 and rel(got_b, be) <= 1e-10
     ene = d["se"][:8]
     assert abs(ene[0] - P.bisec(al[:STOP], be[:STOP], STOP, 1)[0]) <= 1e-10 * abs(ene[0])
+
+
+def tps_models(cl, L):
+    cpl = CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi), gamma=0.1)
+    fld = CP.field_111(0.05)
+    gm = P.Model.from_couplings(cl, cpl, field=fld, tps_L=L)
+    X = O.xlocal(2, 0, cpl, field=fld)
+    skip, _, pt = O.parity_skip(2, 0, X)
+    X = O.tps_explicit(2, cl.nbond, L, X)
+    om = O.Model(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    return gm, om
+
+
+def test_tps_run_resumes_through_its_dump(tmp_path):
+    """An mTPQ vector's run (parallelized_TPSz, S1/2 TPS.f90:325-409) stopped after
+    9 steps, written as interval_dump writes it (vec1 = v0, vec2 = v1, vec3 = vg,
+    coef with L in its second column) and resumed on a fresh context follows the
+    uninterrupted run (alpha, beta, coefficients) to 1e-12 and the oracle's run to
+    1e-10."""
+    cl = honeycomb(2, 4)
+    L = 2.0 * cl.n
+    gm, om = tps_models(cl, L)
+    v = start(gm.dim)
+    full = P.Context(gm, R=1).tps(L, v, STEPS)
+    ctx = P.Context(gm, R=1)
+    ctx.session_begin("tps", v, STEPS, L=L)
+    ctx.session_step(STOP)
+    path = str(tmp_path / "vecdump_me00000")
+    ctx.tps_dump_reference(path)
+    info = P.api.read_interval_dump_info(path)
+    assert info["itr_counter"][0] == STOP + 1 and info["dsf_comp"] == "tp"
+    d = P.api.read_interval_dump(path, "tpsz")
+    w, vk, vg = d["vec1"], d["vec2"], d["vec3"]
+    # the loop's state: v1 normalised, v0 = (L - H) v1 with norm beta, vg the vector before v1
+    assert abs(np.linalg.norm(vk) - 1.0) <= 1e-13
+    assert abs(np.linalg.norm(w) - full["beta"][STOP - 1, 0]) <= 1e-12 * np.linalg.norm(w)
+    assert abs(np.linalg.norm(vg) - 1.0) <= 1e-13
+    ctx.session_end()
+    c2 = P.Context(gm, R=1)
+    assert c2.tps_resume_reference(path, STEPS) == STOP
+    c2.session_step(STEPS - STOP)
+    r = c2.session_read()
+    assert rel(r["beta"][:, 0], full["beta"][:, 0]) <= 1e-12
+    assert rel(r["alpha"][:, 0], full["alpha"][:, 0]) <= 1e-12
+    assert rel(r["coef"][:, 0, :5], full["coef"][:, 0, :5]) <= 1e-12
+    ref = om.tps(L, v, STEPS)
+    assert rel(r["beta"][:, 0], ref["beta"]) <= 1e-10
+    assert rel(r["coef"][:, 0, :5], ref["coef"][:, :5]) <= 1e-10

@@ -123,3 +123,21 @@ def resumed(om, v, cl, tmp_path):
         a, b = om.lanczos_step(v1, v0, a, b)
         rest.append((a, b))
     return al, be, states, rest
+
+
+def test_tps_dump_layout_reads_back(tmp_path):
+    """parallelized_TPSz's dump (S1/2 TPS.f90:368-372) adds vec3 = vg after vec1, vec2."""
+    rng = np.random.default_rng(8)
+    vs, ds = 4, 6
+    vec = [rng.standard_normal(ds) + 1j * rng.standard_normal(ds) for _ in range(3)]
+    coef = np.asfortranarray(rng.standard_normal((vs, 5)))
+    info = P.api.dump_info(12, 18, (3, vs, 2, vs, 1, 5000, 1, 500, 1, 8, 2, 4096), dsf_comp="tp",
+                           position=(0, 0, 0, 0, 0, 0, 1))
+    path = str(tmp_path / "vecdump_me00003")
+    P.api.write_interval_dump(path, info, vs, sa=np.arange(vs, dtype=float), sb=np.ones(vs), sc=coef,
+                              se=np.zeros(9), vec1=vec[0], vec2=vec[1], vec3=vec[2])
+    d = P.api.read_interval_dump(path, "tpsz")
+    assert np.array_equal(d["sc"].reshape(vs, 5, order="F"), coef) and d["se"].size == 9
+    for i in range(3):
+        assert np.array_equal(d[f"vec{i + 1}"], vec[i])
+    assert P.api.read_interval_dump_info(path)["position"][6]
