@@ -421,6 +421,12 @@ int pned_session_info(const pned_ctx *c, int *kind, int *steps_done, int *max_st
  * device memory per flags (PNED_PTR_DEVICE).  Waits for the session's steps.
  */
 int pned_session_lanczos_state(pned_ctx *c, pned_c128 *w_out, pned_c128 *v_out, int flags);
+/* A DSF chain session (R = 1) has the same state in parallelized_dsflnc1z's terms
+ * (S1/2 DSF.f90:234-257; its interval_dump passes vec1 = v1, vec2 = v0, sa = salpha,
+ * sb = sbeta with sbeta(1) = cnorm): pned_session_lanczos_state exports it and
+ * pned_session_begin_dsf_at resumes it (alpha = salpha[0..k-1], beta = sbeta[1..k]). */
+int pned_session_begin_dsf_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                              const double *beta, int k, int max_steps, int flags);
 /*
  * Starts a Lanczos session (R = 1) from that state, as interval_dump_read
  * resumes parallelized_lnc1z (:87-93): k >= 1 steps done, alpha[0..k-1],

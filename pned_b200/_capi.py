@@ -85,7 +85,7 @@ EXPORTS = [
     "pned_write_dsf_vectors", "pned_read_dsf_vectors", "pned_set_max_subrecord",
     "pned_session_lanczos_state", "pned_session_begin_lanczos_at", "pned_write_interval_dump",
     "pned_read_interval_dump_info", "pned_interval_dump_records", "pned_read_interval_dump",
-    "pned_session_tps_state", "pned_session_begin_tps_at",
+    "pned_session_tps_state", "pned_session_begin_tps_at", "pned_session_begin_dsf_at",
 ]
 SESSION_LANCZOS, SESSION_TPS, SESSION_DSF = 1, 2, 3
 
@@ -177,6 +177,7 @@ def lib() -> C.CDLL:
     L.pned_session_lanczos_state.argtypes = [vp, vp, vp, i32]
     L.pned_session_begin_lanczos_at.argtypes = [vp, vp, vp, dp, dp, i32, i32, i32]
     L.pned_session_tps_state.argtypes = [vp, vp, vp, vp, i32]
+    L.pned_session_begin_dsf_at.argtypes = [vp, vp, vp, dp, dp, i32, i32, i32]
     L.pned_session_begin_tps_at.argtypes = [vp, dbl, vp, vp, dp, dp, dp, i32, i32, i32]
     L.pned_write_interval_dump.argtypes = [C.c_char_p, C.POINTER(DumpInfo), C.POINTER(DumpData)]
     L.pned_read_interval_dump_info.argtypes = [C.c_char_p, C.POINTER(DumpInfo)]

@@ -806,6 +806,43 @@ class Context:
         write_interval_dump(path, info, vec_size, sa=a, sb=b, sc=np.zeros((vec_size, REF_NVEC + 1), order="F"),
                             se=ene, vec1=w, vec2=v)
 
+    def dsf_dump_reference(self, path: str, cnorm: float, vec_size: int = REF_S_MAXITR, iq: int = 1, **info_kw):
+        """Writes the running DSF chain session (R = 1) as parallelized_dsflnc1z's
+        interval_dump does (S1/2 DSF.f90:234-238): salpha, sbeta (vec_size each;
+        sbeta(1) = cnorm, sbeta(i+1) = beta_i), vec1 = v1, vec2 = v0, with
+        itr_counter(9) = iq and itr_counter(11) = steps done + 1."""
+        r = self.session_read()
+        k = r["steps"]
+        if k < 1 or k + 1 > vec_size:
+            raise ValueError("the session needs 1..vec_size-1 steps done")
+        a = np.zeros(vec_size)
+        b = np.zeros(vec_size)
+        a[:k] = r["alpha"][:, 0]
+        b[0] = float(np.real(cnorm))
+        b[1:k + 1] = r["beta"][:, 0]
+        w, v = self.lanczos_state()
+        m = self.model
+        itr = (2, REF_MAX_ITR, 2, REF_MAX_ITR, 1, 5000, 1, 500, int(iq), REF_NVEC, k + 1, vec_size)
+        info_kw = {"position": (0, 0, 0, 1, 1, 0, 0), "dsf_comp": "zz", **info_kw}
+        info = dump_info(m.n, m.n_bonds, itr, s_maxitr=vec_size, **info_kw)
+        write_interval_dump(path, info, vec_size, sa=a, sb=b, vec1=v, vec2=w)
+
+    def dsf_resume_reference(self, path: str, max_steps: int):
+        """Starts a DSF chain session (R = 1) from parallelized_dsflnc1z's dump files;
+        returns (steps done, cnorm)."""
+        info = read_interval_dump_info(path)
+        k = info["itr_counter"][10] - 1
+        d = read_interval_dump(path, "dsflnc")
+        if d["data_size"] != self.model.dim or k < 1 or k + 1 > d["sa"].size:
+            raise ValueError(f"{path}: not a DSF dump of this basis")
+        a = np.ascontiguousarray(d["sa"][:k])
+        b = np.ascontiguousarray(d["sb"][1:k + 1])
+        check(lib().pned_session_begin_dsf_at(self._h, C.c_void_p(d["vec2"].ctypes.data),
+                                              C.c_void_p(d["vec1"].ctypes.data), _dp(a), _dp(b), int(k),
+                                              int(max_steps), PTR_HOST))
+        self._sess = dict(kind="dsf", nobs=0, max_steps=int(max_steps))
+        return k, float(d["sb"][0])
+
     def tps_dump_reference(self, path: str, vec_size: int | None = None, ene_size: int = REF_MAX_ITR, **info_kw):
         """Writes the running TPS session (R = 1) as parallelized_TPSz's interval_dump
         does (S1/2 TPS.f90:368-372): alpha, beta (vec_size each), coef (vec_size x

@@ -1087,8 +1087,8 @@ extern "C" int pned_session_lanczos_state(pned_ctx *c, pned_c128 *w_out, pned_c1
 {
     if (!c || !w_out || !v_out) return fail(PNED_EINVAL, "pned_session_lanczos_state: bad arguments");
     Session &S = c->sess;
-    if (S.kind != PNED_SESSION_LANCZOS || c->R != 1 || S.enqueued < 1)
-        return fail(PNED_EINVAL, "pned_session_lanczos_state: needs a Lanczos session (R = 1) with steps done");
+    if ((S.kind != PNED_SESSION_LANCZOS && S.kind != PNED_SESSION_DSF) || c->R != 1 || S.enqueued < 1)
+        return fail(PNED_EINVAL, "pned_session_lanczos_state: needs a Lanczos or DSF session (R = 1) with steps done");
     cudaSetDevice(c->m->device);
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "pned_session_lanczos_state");
@@ -1127,23 +1127,23 @@ extern "C" int pned_session_lanczos_state(pned_ctx *c, pned_c128 *w_out, pned_c1
     return PNED_OK;
 }
 
-extern "C" int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
-                                             const double *beta, int k, int max_steps, int flags)
+static int begin_chain_at(pned_ctx *c, int kind, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                          const double *beta, int k, int max_steps, int flags)
 {
     if (!c || !w || !v || !alpha || !beta || k < 1 || max_steps < k)
         return fail(PNED_EINVAL, "pned_session_begin_lanczos_at: bad arguments");
     if (c->R != 1) return fail(PNED_EINVAL, "pned_session_begin_lanczos_at: needs a context with R = 1");
     if (!(beta[k - 1] > 0.0)) return fail(PNED_EINVAL, "pned_session_begin_lanczos_at: beta[k-1] must be positive");
     cudaSetDevice(c->m->device);
-    int rc = session_common_begin(c, PNED_SESSION_LANCZOS, max_steps);
+    int rc = session_common_begin(c, kind, max_steps);
     if (rc) return rc;
     Session &S = c->sess;
     const int64_t n = c->m->dim;
     const size_t bytes = sizeof(double2) * size_t(n);
-    const cudaMemcpyKind kind = (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind ck = (flags & PNED_PTR_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     // b2 = W, b1 = v (the previous vector, scale 1), b0 = W - alpha v (the next vector times beta)
-    cudaError_t e = cudaMemcpyAsync(c->buf[S.b2], w, bytes, kind, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c->buf[S.b1], v, bytes, kind, c->stream);
+    cudaError_t e = cudaMemcpyAsync(c->buf[S.b2], w, bytes, ck, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->buf[S.b1], v, bytes, ck, c->stream);
     if (e == cudaSuccess) {
         resume_kernel<<<c->nblocks, kThreads, 0, c->stream>>>(c->buf[S.b2], c->buf[S.b1], c->buf[S.b0], alpha[k - 1], n);
         e = cudaGetLastError();
@@ -1160,6 +1160,18 @@ extern "C" int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, co
     }
     S.enqueued = k;
     return PNED_OK;
+}
+
+extern "C" int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                                             const double *beta, int k, int max_steps, int flags)
+{
+    return begin_chain_at(c, PNED_SESSION_LANCZOS, w, v, alpha, beta, k, max_steps, flags);
+}
+
+extern "C" int pned_session_begin_dsf_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
+                                         const double *beta, int k, int max_steps, int flags)
+{
+    return begin_chain_at(c, PNED_SESSION_DSF, w, v, alpha, beta, k, max_steps, flags);
 }
 
 // Copies `src` (scaled by f) into a caller's host or device vector of n states.

@@ -159,3 +159,30 @@ def test_tps_run_resumes_through_its_dump(tmp_path):
     ref = om.tps(L, v, STEPS)
     assert rel(r["beta"][:, 0], ref["beta"]) <= 1e-10
     assert rel(r["coef"][:, 0, :5], ref["coef"][:, :5]) <= 1e-10
+
+
+def test_dsf_chain_resumes_through_its_dump(tmp_path):
+    """A DSF chain (parallelized_dsflnc1z, S1/2 DSF.f90:195-261) stopped after 9
+    steps and resumed from its interval_dump files (sbeta(1) = cnorm, vec1 = v1,
+    vec2 = v0) follows the uninterrupted chain to 1e-12 and the oracle's first 20
+    coefficients to 1e-10."""
+    cl, gm, om = models()
+    x = start(gm.dim)
+    qr = np.ascontiguousarray(cl.qr(1)).reshape(1, -1)
+    full = P.Context(gm, R=1).dsf(x, qr, STEPS)
+    ctx = P.Context(gm, R=1)
+    cn = ctx.session_begin_dsf(x, qr, STEPS)
+    ctx.session_step(STOP)
+    path = str(tmp_path / "vecdump_me00000")
+    ctx.dsf_dump_reference(path, cn[0])
+    ctx.session_end()
+    assert P.api.read_interval_dump_info(path)["itr_counter"][10] == STOP + 1
+    c2 = P.Context(gm, R=1)
+    k, cnorm = c2.dsf_resume_reference(path, STEPS)
+    assert k == STOP and cnorm == cn[0]
+    c2.session_step(STEPS - STOP)
+    r = c2.session_read()
+    assert rel(r["alpha"][:, 0], full["salpha"][:, 0]) <= 1e-12
+    assert rel(r["beta"][:, 0], full["sbeta"][1:, 0]) <= 1e-12
+    ra, rb = om.dsf_chain(*om.intalv_zz(qr[0], x), STEPS)
+    assert rel(r["alpha"][:20, 0], ra[:20]) <= 1e-10 and rel(r["beta"][:19, 0], rb[1:20]) <= 1e-10
