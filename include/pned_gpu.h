@@ -430,8 +430,8 @@ int pned_session_begin_dsf_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *
 /*
  * Starts a Lanczos session (R = 1) from that state, as interval_dump_read
  * resumes parallelized_lnc1z (:87-93): k >= 1 steps done, alpha[0..k-1],
- * beta[0..k-1] (beta[k-1] > 0), w = v0 and v = v1 above; room for max_steps
- * steps in all.  The next step forms (v0 - alpha[k-1] v1) / beta[k-1] and
+ * beta[0..k-1] (host arrays; beta[k-1] > 0), w = v0 and v = v1 above (host or
+ * device memory per flags); room for max_steps steps in all.  The next step forms (v0 - alpha[k-1] v1) / beta[k-1] and
  * continues the chain.
  */
 int pned_session_begin_lanczos_at(pned_ctx *c, const pned_c128 *w, const pned_c128 *v, const double *alpha,
