@@ -11,6 +11,7 @@ module pned_gpu
   public :: pned_lncv1_f, pned_inv1_f, pned_tps_run_f, pned_dump_alpha_beta_coef_f
   public :: pned_lanczos_begin_f, pned_steps_f, pned_lanczos_read_f, pned_interval_dump_f, pned_interval_dump_read_f
   public :: pned_gpu_init_target, pned_dsf_zz_f, pned_dsf_xy_f, pned_append_sq_f, pned_dump_alpha_beta_f
+  public :: pned_lanczos_state_f, pned_lanczos_resume_f
 
   type, bind(C) :: pned_model_desc
     integer(c_int32_t) :: n_sites, q_spin, tree, n_bonds
@@ -119,6 +120,20 @@ module pned_gpu
       type(c_ptr), value :: c
       character(kind=c_char), intent(in) :: path(*)
       integer(c_int), value :: max_steps
+    end function
+    integer(c_int) function pned_session_lanczos_state(c, w, v, flags) bind(C, name="pned_session_lanczos_state")
+      import :: c_int, c_ptr, c_double_complex
+      type(c_ptr), value :: c
+      complex(c_double_complex), intent(out) :: w(*), v(*)
+      integer(c_int), value :: flags
+    end function
+    integer(c_int) function pned_session_begin_lanczos_at(c, w, v, alpha, beta, k, max_steps, flags) &
+        bind(C, name="pned_session_begin_lanczos_at")
+      import :: c_int, c_ptr, c_double, c_double_complex
+      type(c_ptr), value :: c
+      complex(c_double_complex), intent(in) :: w(*), v(*)
+      real(c_double), intent(in) :: alpha(*), beta(*)
+      integer(c_int), value :: k, max_steps, flags
     end function
     integer(c_int) function pned_dsf_run(c, x, qr, nsteps, cnorm, salpha, sbeta, flags) bind(C, name="pned_dsf_run")
       import :: c_int, c_ptr, c_double, c_double_complex
@@ -378,6 +393,24 @@ contains
     if (pned_session_load(g_ctx, trim(filename) // c_null_char, int(max_steps, c_int)) /= 0) &
         stop 'pned_session_load failed'
   end subroutine pned_interval_dump_read_f
+
+  !! The GPU Lanczos run's state in parallelized_lnc1z's own variables at the top
+  !! of its next iteration (v0 = H v_k - beta v_{k-1}, v1 = v_k), so that the
+  !! reference's interval_dump writes its vecdump files unchanged (S1/2 Lanczos.f90:99-103).
+  subroutine pned_lanczos_state_f(v0, v1)
+    complex(kind(0d0)), intent(out) :: v0(:), v1(:)
+    if (pned_session_lanczos_state(g_ctx, v0, v1, 0_c_int) /= 0) stop 'pned_session_lanczos_state failed'
+  end subroutine pned_lanczos_state_f
+
+  !! Resumes the GPU run from what interval_dump_read has read back (:87-93):
+  !! alpha/beta of the done = itr_counter(1) - 1 steps, v0 and v1.
+  subroutine pned_lanczos_resume_f(v0, v1, alpha, beta, done, max_steps)
+    complex(kind(0d0)), intent(in) :: v0(:), v1(:)
+    double precision, intent(in) :: alpha(:), beta(:)
+    integer, intent(in) :: done, max_steps
+    if (pned_session_begin_lanczos_at(g_ctx, v0, v1, alpha, beta, int(done, c_int), int(max_steps, c_int), &
+                                      0_c_int) /= 0) stop 'pned_session_begin_lanczos_at failed'
+  end subroutine pned_lanczos_resume_f
 
   subroutine pned_gpu_finalize()
     integer(c_int) :: rc
