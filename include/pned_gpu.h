@@ -140,8 +140,12 @@ int pned_model_plan(const pned_model *m, int R, int *tile_passes, int *partner_t
  * pass expects in L2; max_passes: 1..4; j_bits (R = 1 only): 1..4, states
  * per thread 2^j_bits (fewer: fewer registers, more resident blocks; 4: tiles
  * of 4096 states, more flips inside the tile).  Re-plans at
- * once (plan NULL: defaults); call it between launches, not while other
- * threads launch on the model.  Used by the autotuner (pned_b200.tune).
+ * once; call it between launches, not while other threads launch on the
+ * model.  Used by the autotuner (pned_b200.tune).  plan NULL (and a model
+ * whose plan was never set) takes the size's default: for R = 1 from 26
+ * sites on, row_fixed_bits 5, window_bits 7, two passes, objective 1, stage
+ * 3, two terms in flight (the plan the autotuner picks on B200 at 26-30
+ * sites); otherwise every field at its own default as described here.
  */
 typedef struct {
     int32_t row_fixed_bits;

@@ -480,9 +480,14 @@ class Model:
     def set_plan(self, R: int = 1, row_fixed_bits: int = -1, window_bits: int = -1, max_passes: int = -1,
                  j_bits: int = -1, l1_carveout: int = 1, stage_partner_tiles: int = 0, blocks_per_sm: int = -1,
                  objective: int = -1, terms_in_flight: int = -1):
-        """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan."""
-        tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), int(l1_carveout),
-                            int(stage_partner_tiles), int(blocks_per_sm), int(objective), int(terms_in_flight))
+        """Re-plans the tiled H.v for R vectors (-1: default); returns the new plan.
+        With no plan argument the library's default plan for the size is restored."""
+        args = (row_fixed_bits, window_bits, max_passes, j_bits, l1_carveout, stage_partner_tiles, blocks_per_sm,
+                objective, terms_in_flight)
+        if args == (-1, -1, -1, -1, 1, 0, -1, -1, -1):
+            check(lib().pned_model_set_plan(self._h, int(R), None))
+            return self.plan(R)
+        tp = _capi.TilePlan(*(int(x) for x in args))
         check(lib().pned_model_set_plan(self._h, int(R), C.byref(tp)))
         return self.plan(R)
 

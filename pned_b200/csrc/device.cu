@@ -1145,17 +1145,25 @@ void build_tile_programs(pned_model *m)
     m->tprogs.clear();
     const HostProgram &hp = m->hp;
     std::vector<HostProgram::TilePass> passes;
-    const int fixed = m->plan1.row_fixed_bits >= 0 ? m->plan1.row_fixed_bits : 8;
-    const int window = m->plan1.window_bits >= 0 ? m->plan1.window_bits : kTileWindowBits;
-    const int mp = m->plan1.max_passes > 0 ? m->plan1.max_passes : kTileMaxPasses;
+    // Without a plan set (pned_model_set_plan with NULL, or never called): from 26
+    // sites on, the plan the autotuner picks on B200 at 26-30 sites (tile bits that
+    // hold the most flip terms, 7 window bits, two passes, own rows by tensor copies,
+    // two out-of-tile terms in flight); below, and for the fields a set plan leaves
+    // at -1, the fewest partner tiles with a 10-bit window through the gather kernel.
+    const bool big = hp.n >= kTileBigSites && !m->plan1_set;
+    const int fixed = m->plan1.row_fixed_bits >= 0 ? m->plan1.row_fixed_bits : (big ? 5 : 8);
+    const int window = m->plan1.window_bits >= 0 ? m->plan1.window_bits : (big ? 7 : kTileWindowBits);
+    const int mp = m->plan1.max_passes > 0 ? m->plan1.max_passes : (big ? 2 : kTileMaxPasses);
     const int jb = m->plan1.j_bits > 0 ? m->plan1.j_bits : 3;
-    const int obj = m->plan1.objective > 0 ? m->plan1.objective : 0;
+    const int obj = big ? 1 : (m->plan1.objective > 0 ? m->plan1.objective : 0);
+    const int stage = big ? 3 : m->plan1.stage_partner_tiles;
+    const int tif = big ? 2 : m->plan1.terms_in_flight;
     if (hp.q == 2 && !hp.sector && hp.n >= 12 && plan_tiles(hp, 8, jb, fixed, window, mp, passes, obj) == PNED_OK) {
         m->tprogs = tile_programs(hp, passes, m->ntab);
         m->tile_jb = jb;
         m->tile_bps = (jb == 3 && m->plan1.blocks_per_sm == 3) ? 3 : tile_blocks_per_sm(jb);
-        m->tma_deep = m->plan1.terms_in_flight == 2;
-        m->tile_stage = std::max(0, std::min(3, m->plan1.stage_partner_tiles));
+        m->tma_deep = tif == 2;
+        m->tile_stage = std::max(0, std::min(3, stage));
         if (m->tile_stage == 3) {
             // own rows, epilogue rows and diagonal by tensor copies: 8 rows a thread, every
             // pass's tile within 5 copy dimensions, two blocks' shared memory per SM
@@ -1428,6 +1436,7 @@ extern "C" int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *p
         return fail(PNED_EINVAL, "pned_model_set_plan: plan out of range");
     if (R == 1) {
         m->plan1 = plan ? *plan : pned_tile_plan{-1, -1, -1, -1, -1, -1, -1, -1, -1};
+        m->plan1_set = plan != nullptr;
         m->carveout = m->plan1.l1_carveout != 0;
         build_tile_programs(m);
         return PNED_OK;

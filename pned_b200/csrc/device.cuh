@@ -46,6 +46,7 @@ struct pned_model {
                                             // diagonal copied in by the tensor-copy engine
     std::vector<pned::TmaGeom> tma_geom;    // stage 3: copy geometry of each pass's tile
     bool tma_deep = false;                  // stage 3: partner rows of two out-of-tile terms in flight
+    bool plan1_set = false;                 // plan1 was set by the caller (else the size's default plan)
     int bulk_stages = 0;                    // shared-memory stages of the bulk-copy pipeline
     int nsm = 148;
     double2 *d_table = nullptr;

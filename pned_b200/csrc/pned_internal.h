@@ -71,6 +71,7 @@ struct QTileTerm {
 };
 constexpr int kTileMaxJB = 4;
 constexpr int kTileWindowBits = 10;   // outer bits whose partner tiles stay in L2 during a sweep
+constexpr int kTileBigSites = 26;     // from here on the single-vector plan defaults to the tensor-copy kernel
 constexpr int kTileMaxPasses = 4;
 constexpr int kTileMaxGroups = 64;    // partner tiles per pass
 

@@ -851,6 +851,7 @@ extern "C" int pned_slots_set_plan(pned_slots *S, const pned_tile_plan *plan)
     if (plan) S->tm.carveout = plan->l1_carveout != 0;
     if (S->R == 1) {
         S->tm.plan1 = plan ? *plan : def;
+        S->tm.plan1_set = plan != nullptr;
         build_tile_programs(&S->tm);
         S->tile = S->tm.use_tile;
     } else {

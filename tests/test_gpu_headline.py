@@ -76,14 +76,19 @@ def test_headline_hv_slices_match_oracle(n_sites):
         om.p_mltply_v3_slice(v1h, w, lo, lo + SLICE, EPERBD)
         ref.append(w)
     del v1h
+    # the default plan of this size first (no plan set: the tensor-copy kernel), then
+    # the candidates and the plan the autotuner picks
+    assert gm.plan(1)["staging"] == 3
     tuned = tune.autotune(gm, 1)
-    plans = list(PLANS[n_sites])
+    plans = [()] + list(PLANS[n_sites])
     if tuple(tuned["plan"]) not in plans:
         plans.append(tuple(tuned["plan"]))
     w = torch.empty_like(v1)
     for plan in plans:
         got = gm.set_plan(1, *plan)
         assert got["tile_passes"] >= 2, plan
+        if not plan:
+            assert got["staging"] == 3
         if len(plan) > 5 and plan[5] in (2, 3):
             assert got["staging"] == plan[5], plan
         ctx = P.Context(gm, R=1)
