@@ -141,3 +141,22 @@ def test_tps_dump_layout_reads_back(tmp_path):
     for i in range(3):
         assert np.array_equal(d[f"vec{i + 1}"], vec[i])
     assert P.api.read_interval_dump_info(path)["position"][6]
+
+
+def test_interval_dump_rejects_mismatched_files(tmp_path):
+    """A dump read with another loop's layout, a truncated data file and a missing
+    .info file are refused with an error, not misread."""
+    import pytest
+    rng = np.random.default_rng(9)
+    v = [rng.standard_normal(4) + 1j * rng.standard_normal(4) for _ in range(2)]
+    info = P.api.dump_info(8, 12, (2, 3, 2, 3, 1, 5000, 1, 500, 1, 8, 2, 4096))
+    path = str(tmp_path / "vecdump_me00000")
+    P.api.write_interval_dump(path, info, 3, sa=np.ones(3), sb=np.ones(3), vec1=v[0], vec2=v[1])
+    with pytest.raises(ValueError):
+        P.api.read_interval_dump(path, "lnc1z")          # six arrays expected, four in the file
+    raw = open(path, "rb").read()
+    open(path, "wb").write(raw[:-20])
+    with pytest.raises(P.PnedError):
+        P.api.read_interval_dump(path, "dsflnc")
+    with pytest.raises(P.PnedError):
+        P.api.read_interval_dump_info(str(tmp_path / "missing"))
