@@ -318,6 +318,21 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "e2e": e2e,
     }
+    # the bound that holds this gather in practice: every flip term moves a 16-byte
+    # operand per state through the SM's load/store data path (128 B per clock per
+    # SM), whether it comes from shared memory or from L1/L2; the own-row and
+    # epilogue accesses come on top, so the fraction is a lower bound
+    clk_sum = line["clocks"]
+    if plan["tile_passes"] and clk_sum.get("sm_mhz"):
+        nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+        lsu_bytes = 16 * model.n_terms * D
+        lsu_peak = 128 * nsm * clk_sum["sm_mhz"] * 1e6 / 1e12
+        lsu_ach = lsu_bytes / (hv_ms * 1e-3) / 1e12
+        line["roofline"]["data_path"] = {
+            "bound": "l1_data_path", "unit": "TB/s", "flip_terms": model.n_terms,
+            "bytes_per_hv": lsu_bytes, "achieved": lsu_ach, "peak": lsu_peak, "frac": lsu_ach / lsu_peak,
+            "note": "flip-term operands only (16 B per term and state) against 128 B per clock per SM at the "
+                    "median SM clock of the timed region; own-row and epilogue accesses are not counted"}
     if tuning is not None:
         pl = list(tuning["plan"]) + [-1] * (4 - len(tuning["plan"]))
         line["roofline"]["tuned_plan"] = {"row_fixed_bits": pl[0], "window_bits": pl[1], "max_passes": pl[2],
