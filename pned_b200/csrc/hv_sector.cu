@@ -21,8 +21,10 @@
 
 namespace pned {
 
+constexpr int kSegUnroll = 4;   // terms whose loads the segment kernel keeps in flight together
+
 template <bool RC, bool RD, int K>
-__global__ void __launch_bounds__(kThreads, 5)   // 48 registers, as the flat gather
+__global__ void __launch_bounds__(kThreads, 4)
     hv_sector_kernel(const __grid_constant__ XorProgram prog, const HvArgs a, const int64_t *__restrict__ seg_start,
                      const int32_t *__restrict__ seg_hi, const int32_t *__restrict__ rank_lo, int nseg)
 {
@@ -61,7 +63,38 @@ __global__ void __launch_bounds__(kThreads, 5)   // 48 registers, as the flat ga
                 dd.x -= a.shift;
                 acc[0] = cmul(dd, v[0]);
             }
-            for (int t = 0; t < prog.nterms; ++t) {
+            // four terms at a time: their rank reads, then their partner reads, are in
+            // flight together; the products are added in term order as below
+            int t = 0;
+            for (; t + kSegUnroll <= prog.nterms; t += kSegUnroll) {
+                double2 c[kSegUnroll], w[kSegUnroll];
+                int64_t pi[kSegUnroll];
+#pragma unroll
+                for (int u = 0; u < kSegUnroll; ++u) {
+                    const XorTerm T = prog.t[t + u];
+                    uint32_t idx = 0;
+#pragma unroll
+                    for (int k = 0; k < kMaxDeps; ++k)
+                        if (k < T.nb) idx |= ((su >> ((T.pos4 >> (8 * k)) & 0xffu)) & 1u) << k;
+                    c[u] = s_tab[T.tab + idx];
+                    const uint32_t ml = T.xmask & lomask;
+                    const bool zero = c[u].x == 0.0 && c[u].y == 0.0;
+                    const int64_t rk = ml == 0 ? r : __ldg(rank_lo + (lo ^ ml));
+                    pi[u] = zero ? s : s_base[t + u] + rk;
+                }
+#pragma unroll
+                for (int u = 0; u < kSegUnroll; ++u) w[u] = __ldg(a.C + pi[u]);
+#pragma unroll
+                for (int u = 0; u < kSegUnroll; ++u) {
+                    if (RC) {
+                        acc[0].x = fma(c[u].x, w[u].x, acc[0].x);
+                        acc[0].y = fma(c[u].x, w[u].y, acc[0].y);
+                    } else {
+                        acc[0] = cfma(c[u], w[u], acc[0]);
+                    }
+                }
+            }
+            for (; t < prog.nterms; ++t) {
                 const XorTerm T = prog.t[t];
                 uint32_t idx = 0;
 #pragma unroll
