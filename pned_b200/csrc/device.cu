@@ -96,7 +96,36 @@ __global__ void __launch_bounds__(kThreads) hv_xor_kernel(const __grid_constant_
 #pragma unroll
             for (int j = 0; j < VPT; ++j) acc[j] = cmul(dd, v[j]);
         }
-        for (int t = 0; t < prog.nterms; ++t) {
+        int t = 0;
+        if (SECTOR && VPT == 1) {
+            // sector, one vector a thread: four terms' table and partner reads in flight
+            // together, the products added in term order as below
+            for (; t + 4 <= prog.nterms; t += 4) {
+                double2 c[4], w[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const XorTerm T = prog.t[t + u];
+                    uint32_t idx = 0;
+#pragma unroll
+                    for (int k = 0; k < kMaxDeps; ++k)
+                        if (k < T.nb) idx |= ((su >> ((T.pos4 >> (8 * k)) & 0xffu)) & 1u) << k;
+                    c[u] = s_tab[T.tab + idx];
+                    int64_t pi = lin_index(a, su ^ T.xmask);
+                    if (c[u].x == 0.0 && c[u].y == 0.0) pi = s;
+                    w[u] = __ldg(a.C + pi * R + r0);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (RC) {
+                        acc[0].x = fma(c[u].x, w[u].x, acc[0].x);
+                        acc[0].y = fma(c[u].x, w[u].y, acc[0].y);
+                    } else {
+                        acc[0] = cfma(c[u], w[u], acc[0]);
+                    }
+                }
+            }
+        }
+        for (; t < prog.nterms; ++t) {
             const XorTerm T = prog.t[t];
             uint32_t idx = 0;
 #pragma unroll
