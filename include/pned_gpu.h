@@ -249,8 +249,7 @@ int pned_hv(pned_ctx *c, const pned_c128 *v1, pned_c128 *v0, double eperbd, pned
  * library (4096 complex values, 64 KB, held by every GPU that loads the
  * library until exit); R may be 1, 2, 3, 4, 6, 8, 12 or 16, and anything else
  * is rejected with PNED_EINVAL.  The first call on a device resolves the
- * array's device address (set-up), so make that first call before any stream
- * capture.  The address is kept for the life of the process: after a
+ * array's device address (set-up).  The address is kept for the life of the process: after a
  * cudaDeviceReset of that device it is stale, so do not call this again on a
  * device that was reset.  Every call shares the array: calls that overlap on the GPU race and
  * must be ordered by the caller (one stream, or events).  v1, v0 are device
