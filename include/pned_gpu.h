@@ -175,7 +175,9 @@ int pned_model_set_plan(pned_model *m, int R, const pned_tile_plan *plan);
  * (S = 1/2 full basis) that the planner builds for this model with row_bits row
  * bits a tile (8: the single-vector kernel, as pned_model_set_plan; fewer: the
  * multi-vector kernel's 256 / G rows), computed on the host without device
- * work; the default fixed row bits are min(row_bits, 8).  out[0..cap)
+ * work; the default fixed row bits are min(row_bits, 8), and plan NULL with
+ * row_bits 8 gives the model's default plan (from 26 sites on fixed 5, window
+ * 7, 2 passes, objective 1).  out[0..cap)
  * receives int64 values, *len the full count: the number of flip terms X, X
  * records (xmask, pos4, tab, nb), the number of passes, and per pass (tbits, jb,
  * nouter, nterms, nin, ngroups), rowpos[tbits], jpos[jb], outer[nouter], nterms

@@ -401,10 +401,12 @@ def tile_plan_export(desc: "ModelInput", row_fixed_bits: int = -1, window_bits: 
     (pned_tile_plan_export): the program's flip terms and, per pass, the tile
     bits, outer order, terms and partner-tile groups."""
     tp = _capi.TilePlan(int(row_fixed_bits), int(window_bits), int(max_passes), int(j_bits), 1, 0, -1, int(objective), -1)
+    # all defaults: no plan, the model's own default (as Model.set_plan)
+    ptp = None if (row_fixed_bits, window_bits, max_passes, j_bits, objective) == (-1,) * 5 else C.byref(tp)
     n = C.c_int64(0)
-    check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), C.byref(tp), None, 0, C.byref(n)))
+    check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), ptp, None, 0, C.byref(n)))
     buf = np.zeros(n.value, dtype=np.int64)
-    check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), C.byref(tp),
+    check(lib().pned_tile_plan_export(C.byref(desc.c), int(row_bits), ptp,
                                       buf.ctypes.data_as(C.POINTER(C.c_int64)), n.value, C.byref(n)))
     it = iter(buf.tolist())
     nx = next(it)

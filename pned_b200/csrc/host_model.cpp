@@ -854,13 +854,16 @@ extern "C" int pned_tile_plan_export(const pned_model_desc *d, int row_bits, con
     if (pl.max_passes > kTileMaxPasses || pl.window_bits > 30 || pl.row_fixed_bits > 8 || pl.j_bits > kTileMaxJB ||
         pl.j_bits == 0 || pl.objective > 1)
         return fail(PNED_EINVAL, "pned_tile_plan_export: plan out of range");
-    // the defaults of the model's own single-vector plan
-    const int fixed = std::min(row_bits, pl.row_fixed_bits >= 0 ? pl.row_fixed_bits : 8);
-    const int window = pl.window_bits >= 0 ? pl.window_bits : kTileWindowBits;
-    const int mp = pl.max_passes > 0 ? pl.max_passes : kTileMaxPasses;
+    // the defaults of the model's own single-vector plan: with no plan, from
+    // kTileBigSites sites on, the tuned tensor-copy plan (5 fixed row bits,
+    // window 7, 2 passes, most terms inside the tile)
+    const bool big = !plan && row_bits == 8 && P.n >= kTileBigSites;
+    const int fixed = big ? 5 : std::min(row_bits, pl.row_fixed_bits >= 0 ? pl.row_fixed_bits : 8);
+    const int window = big ? 7 : (pl.window_bits >= 0 ? pl.window_bits : kTileWindowBits);
+    const int mp = big ? 2 : (pl.max_passes > 0 ? pl.max_passes : kTileMaxPasses);
     const int jb = pl.j_bits > 0 ? pl.j_bits : 3;
     std::vector<HostProgram::TilePass> passes;
-    rc = plan_tiles(P, row_bits, jb, fixed, window, mp, passes, pl.objective > 0 ? pl.objective : 0);
+    rc = plan_tiles(P, row_bits, jb, fixed, window, mp, passes, big ? 1 : (pl.objective > 0 ? pl.objective : 0));
     if (rc) return fail(rc, "pned_tile_plan_export: no tile plan for this model and plan");
     std::vector<int64_t> v;
     v.push_back(int64_t(P.xterms.size()));

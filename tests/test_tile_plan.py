@@ -257,3 +257,63 @@ def test_most_terms_objective_n30():
     c18 = cluster_for_sites(18)
     d18 = P.ModelInput(c18.n, 2, 0, c18.ipair, c18.ibond_type, X, skip, pt)
     check_plan(c18.n, api.tile_plan_export(d18, 5, 6, 2, 3, objective=1), 5)
+
+
+def tma_copy_dims(n, ps):
+    """Copy dimensions of one pass's tile for the tensor-copy kernel
+    (pned_b200/csrc/hv_staged.cu, tile_tma_geometry): the tile's bits in
+    ascending order must be the 8 row bits, then the 3 j bits, from bit 0; runs
+    of tile bits (the first at most 7 bits, later ones 8) and runs of outer bits
+    (at most 31) each take one dimension.  None where the tile does not qualify."""
+    tb = sorted(ps["rowpos"] + ps["jpos"])
+    if len(ps["rowpos"]) != 8 or len(ps["jpos"]) != 3 or tb != ps["rowpos"] + ps["jpos"] or tb[0] != 0:
+        return None
+    tset, dims, b = set(tb), 0, 0
+    while b < n:
+        inside = b in tset
+        e = b
+        while e < n and (e in tset) == inside:
+            e += 1
+        s = b
+        while s < e:
+            s += min((7 if dims == 0 else 8) if inside else 31, e - s)
+            dims += 1
+        b = e
+    return dims
+
+
+@pytest.mark.parametrize("n", [26, 28, 30])
+def test_default_plan_from_26_sites_is_the_tensor_copy_plan(n):
+    """With no plan set, from 26 sites on the model plans 5 fixed row bits, a
+    7-bit window, 2 passes and the most-terms objective (the autotuned plan of
+    the tensor-copy kernel): the exporter gives the same plan, every pass's
+    tile maps onto at most 5 copy dimensions (else the kernel would fall back
+    to the gather), and every flip term is in exactly one pass.  At N = 30 the
+    passes have 10 + 12 partner tiles and 13 + 9 terms inside the tile."""
+    import math
+    from pned_b200.lattice import cluster_for_sites
+    cl = cluster_for_sites(n)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(math.cos(0.3 * math.pi), 2 * math.sin(0.3 * math.pi)))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    r = api.tile_plan_export(d)
+    assert r == api.tile_plan_export(d, 5, 7, 2, 3, objective=1)
+    assert len(r["passes"]) == 2
+    assert sorted(t["tab"] for ps in r["passes"] for t in ps["terms"]) == sorted(x["tab"] for x in r["xterms"])
+    assert len(r["xterms"]) == 3 * n // 2
+    for ps in r["passes"]:
+        dims = tma_copy_dims(n, ps)
+        assert dims is not None and dims <= 5
+    if n == 30:
+        assert [len(ps["gxor"]) for ps in r["passes"]] == [10, 12]
+        assert [ps["nin"] for ps in r["passes"]] == [13, 9]
+
+
+def test_default_plan_below_26_sites_is_the_gather_plan():
+    """Below 26 sites the default stays the fewest-partner-tile plan with a
+    10-bit window (the gather kernel's): the exporter without a plan gives the
+    plan of explicit defaults."""
+    from pned_b200.lattice import cluster_for_sites
+    cl = cluster_for_sites(24)
+    X, skip, pt = P.build_xlocal(2, 0, CP.kitaev_heisenberg(0.6, 1.6))
+    d = P.ModelInput(cl.n, 2, 0, cl.ipair, cl.ibond_type, X, skip, pt)
+    assert api.tile_plan_export(d) == api.tile_plan_export(d, 8, 10, -1, 3, objective=0)
