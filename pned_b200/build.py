@@ -38,8 +38,16 @@ def _stale() -> bool:
     return False
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile every CUDA/C++ source into pned_b200/libpned_gpu.so."""
+def build(force: bool = False, verbose: bool = False, sanitize: str = "") -> str:
+    """Compile every CUDA/C++ source into pned_b200/libpned_gpu.so.
+
+    sanitize ("address" or "undefined") instruments the host-only sources
+    (model compiler, planners, file formats) with that gcc sanitizer, for the
+    CPU tests; an address-sanitized library needs libasan preloaded
+    (LD_PRELOAD=$(gcc -print-file-name=libasan.so), ASAN_OPTIONS=detect_leaks=0).
+    Rebuild without it (force=True) afterwards."""
+    if sanitize not in ("", "address", "undefined"):
+        raise ValueError("sanitize: 'address' or 'undefined'")
     if not force and not _stale():
         return LIB
     nvcc = _nvcc()
@@ -51,6 +59,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc, *common, *ARCH, "-c", os.path.join(CSRC, src), "-o", obj]
+        if sanitize and src.endswith(".cpp"):
+            cmd += ["-Xcompiler", f"-fsanitize={sanitize},-fno-omit-frame-pointer,-g"]
         if src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if verbose else []
         if verbose:
@@ -59,11 +69,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc, "-shared", *ARCH, "-o", tmp, *objs, "-Xcompiler", "-fopenmp", "-lcudart"]
+    if sanitize:
+        cmd += ["-Xcompiler", f"-fsanitize={sanitize}"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    san = next((a.split("=", 1)[1] for a in sys.argv if a.startswith("--sanitize=")), "")
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv, sanitize=san)
     print(LIB)
